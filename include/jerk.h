@@ -1,0 +1,153 @@
+/*
+ * libjerk: B200 (sm_100a) Fourier-domain jerk search -- the C ABI.
+ *
+ * Drop-in for the search loop of PrestoZL's accelsearch_cu: everything
+ * between the reference's accelsearch_CPU1 (command line, accelobs, kernel
+ * bank) and accelsearch_CPU2 (sort, harmonic elimination, optimisation,
+ * ACCEL output) runs here on the GPU.  Plain pointers and sizes only.
+ *
+ * Reference interfaces each entry point replaces (paths inside the
+ * reference project):
+ *   jerk_plan_create   accelsearch_GPU set-up: init_constant_device,
+ *                      fkern_host_to_dev, buffer sizing
+ *                      (src/accelsearch_lib.c:473-645,
+ *                       src/accel_kernels.cu:73-79,
+ *                       src/accel_utils_cu.c:378-429)
+ *   jerk_search        accelsearch_GPU's batch loop + insert_to_cands
+ *                      (src/accelsearch_lib.c:660-878,
+ *                       src/accel_utils_cu.c:432-612 do_fft_batch /
+ *                       fuse_add_search_batch / sort_search_results,
+ *                       src/accel_utils_cu.c:857-929)
+ *   jerk_plan_destroy  accelsearch_GPU tear-down (cudaFree*, clear_cache;
+ *                      src/accelsearch_lib.c:866-878)
+ *   jerk_obs_from_params / jerk_subharm_sizes
+ *                      the sizing part of create_accelobs and
+ *                      init_subharminfo (src/accel_utils.c:1795-2004,
+ *                      199-234, 137-149)
+ *   jerk_candidate_sigma / jerk_power_for_sigma
+ *                      candidate_sigma / power_for_sigma
+ *                      (src/characteristics.c:647-705)
+ *   jerk_bank_generate the kernel bank of create_subharminfos
+ *                      (src/accel_utils.c:151-282, src/responses.c:333-418)
+ *
+ * Return codes: JERK_OK, > 0 recoverable, < 0 fatal (no exit() anywhere).
+ */
+#ifndef JERK_H
+#define JERK_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JERK_OK 0
+#define JERK_OVERFLOW 1          /* more hits than the hit buffer holds; retried internally */
+#define JERK_TIMEOUT 2           /* a bounded wait gave up */
+#define JERK_EINVAL (-1)         /* bad argument */
+#define JERK_ECUDA (-2)          /* CUDA runtime error */
+#define JERK_ENOMEM (-3)         /* device or host allocation failed */
+#define JERK_EUNSUPPORTED (-4)   /* a configuration the engine does not handle */
+
+#define JERK_MAX_STAGES 6
+
+/* The search geometry of one spectrum: the fields of the reference's
+ * accelobs (include/accel.h:37-82) that the search loop reads. */
+typedef struct jerk_obs {
+    long long numbins;        /* complex bins in the spectrum */
+    long long lobin;          /* bin number of spectrum[0] */
+    long long highestbin;     /* the search stops before this bin */
+    double rlo;               /* first fundamental Fourier bin searched */
+    double zlo;               /* -zmax */
+    double wlo;               /* -wmax */
+    int corr_uselen;          /* good interbins per rstep */
+    int numz;                 /* fundamental f-dot count */
+    int numw;                 /* accelobs.numw (0 when -wmax 0) */
+    int numharmstages;        /* log2(numharm) + 1 */
+    int norm_type;            /* 0: block median (the only one supported) */
+    float nph;                /* > 0: photon normalisation */
+    float powcut[JERK_MAX_STAGES];
+    long long numindep[JERK_MAX_STAGES];
+} jerk_obs;
+
+/* One subharmonic's kernel set (the reference's subharminfo,
+ * include/accel.h:110-122). */
+typedef struct jerk_subharm {
+    int numharm, harmnum;     /* harmonic fraction harmnum/numharm */
+    int zmax, wmax;           /* this subharmonic's own maxima */
+    int numz, numw;           /* numkern_zdim, numkern_wdim */
+    int fftlen;
+    int halfwidth;            /* kern[0][0].kern_half_width */
+    const void *kernels;      /* host complex64 [numw][numz][fftlen], or NULL
+                                 with a device bank (jerk_config.device_bank) */
+} jerk_subharm;
+
+/* A candidate: the leading fields of the reference's accelcand
+ * (include/accel.h:84-97). */
+typedef struct jerk_cand {
+    float power;
+    float sigma;
+    int numharm;
+    double r, z, w;
+} jerk_cand;
+
+typedef struct jerk_config {
+    int batch_rsteps;         /* rsteps per batch (the reference's -batchsize); 0 = auto */
+    long long max_hits;       /* initial hit-buffer capacity; 0 = auto */
+    void *stream;             /* cudaStream_t to run on; NULL = a private stream */
+    const void *device_bank;  /* optional resident bank (jerk_bank_generate) */
+} jerk_config;
+
+typedef struct jerk_plan jerk_plan;
+
+/* Raw threshold crossings of one search, in the reference's insertion order
+ * (rstep, stage, w, z, r). */
+typedef struct jerk_hits {
+    long long count;
+    unsigned long long *keys; /* encoded (rstep, stage, w, z, r) */
+    float *powers;
+} jerk_hits;
+
+int jerk_obs_from_params(long long numbins, long long N, double dt, int zmax, int wmax,
+                         int wmax_given, int numharm, float sigma, double flo, double fhi,
+                         jerk_obs *obs, int *fftlen, int *maxkernlen);
+int jerk_subharm_count(int numharmstages);
+int jerk_subharm_sizes(const jerk_obs *obs, int fftlen, int index, jerk_subharm *out);
+
+int jerk_plan_create(jerk_plan **plan, const jerk_obs *obs, const jerk_subharm *subs,
+                     int nsubs, const jerk_config *cfg);
+void jerk_plan_destroy(jerk_plan *plan);
+
+/* Search rsteps [first_rstep, first_rstep + num_rsteps) (num_rsteps <= 0:
+ * to the end).  spectrum: numbins complex64, on the host (copied in) or on
+ * the device (spectrum_on_device != 0).  The final candidate list (the
+ * reference's GSList contents, in list order) is written to *cands, which the
+ * caller frees with jerk_free; hits (optional) receives the raw crossings. */
+int jerk_search(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
+                long long first_rstep, long long num_rsteps, jerk_cand **cands,
+                long long *ncands, jerk_hits *hits);
+
+/* Number of rsteps of the full search. */
+long long jerk_num_rsteps(const jerk_plan *plan);
+
+/* Debug/test: the ffdot volume of subharmonic 'sub' at rstep 'rstep'
+ * ([numw][numz][numrs] floats, numrs written to *numrs). */
+int jerk_debug_volume(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
+                      long long rstep, int sub, float *out, int *numrs, long long *rlo);
+
+/* Statistics (host, double precision). */
+double jerk_candidate_sigma(double power, int numsum, double numtrials);
+double jerk_power_for_sigma(double sigma, int numsum, double numtrials);
+
+/* Candidate insertion with the reference's 15-bin rule over a decoded hit
+ * sequence; used by jerk_search, exported for tests. */
+long long jerk_insert_hits(const jerk_cand *hits, long long nhits, jerk_cand **cands);
+
+void jerk_free(void *p);
+const char *jerk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -94,6 +94,9 @@ def _ref():
                                            C.c_int, C.c_void_p]
         lib.ref_close.argtypes = [C.c_void_p]
         lib.ref_set_threads.argtypes = [C.c_int]
+        lib.ref_insert_sequence.restype = C.c_long
+        lib.ref_insert_sequence.argtypes = [C.c_void_p, C.c_long, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_long]
         lib.ref_set_threads(1)
         _reflib = lib
     return _reflib
@@ -168,6 +171,17 @@ class RefSearch:
                            pw.ctypes.data, rinds.ctypes.data, zinds.ctypes.data)
         return h, pw, rinds, zinds
 
+    def insert_sequence(self, pows, rlo, numharm, max_out: int = 1 << 20):
+        """The reference's own list insertion over a crafted hit sequence
+        (one 1x1x1 volume per hit through search_ffdotpows)."""
+        pows = np.ascontiguousarray(pows, dtype=np.float32)
+        rlo = np.ascontiguousarray(rlo, dtype=np.int64)
+        numharm = np.ascontiguousarray(numharm, dtype=np.int32)
+        out = np.zeros(max_out, dtype=CAND_DTYPE)
+        n = _ref().ref_insert_sequence(self.ctx, len(pows), pows.ctypes.data, rlo.ctypes.data,
+                                       numharm.ctypes.data, out.ctypes.data, max_out)
+        return out[: min(n, max_out)].copy()
+
     def search(self, max_steps: int = 0, max_out: int = 1 << 20):
         out = np.zeros(max_out, dtype=CAND_DTYPE)
         done = C.c_long(0)
@@ -225,6 +239,11 @@ def _orc():
         lib.orc_search.argtypes = [C.POINTER(OrcGeom), C.POINTER(OrcSub), C.c_void_p,
                                    C.c_long, C.c_long, C.c_void_p, C.c_long,
                                    C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        lib.orc_search_hits.restype = C.c_long
+        lib.orc_search_hits.argtypes = [C.POINTER(OrcGeom), C.POINTER(OrcSub), C.c_void_p,
+                                        C.c_long, C.c_long, C.c_void_p, C.c_long,
+                                        C.POINTER(C.c_long), C.POINTER(C.c_long),
+                                        C.c_void_p, C.c_void_p, C.c_long]
         lib.orc_insert_hits.restype = C.c_long
         lib.orc_insert_hits.argtypes = [C.c_void_p, C.c_long, C.POINTER(C.c_longlong),
                                         C.c_void_p, C.c_long]
@@ -304,6 +323,22 @@ class Oracle:
                               first_step, max_steps, out.ctypes.data, max_out,
                               C.byref(done), C.byref(nh))
         return out[: min(n, max_out)].copy(), done.value, nh.value
+
+
+    def search_hits(self, first_step: int = 0, max_steps: int = 0, max_out: int = 1 << 20,
+                    hit_cap: int = 1 << 22):
+        """(cands, steps, hit keys, hit powers): every threshold crossing in
+        insertion order, keyed as the product keys its hits."""
+        out = np.zeros(max_out, dtype=CAND_DTYPE)
+        keys = np.zeros(hit_cap, dtype=np.uint64)
+        pows = np.zeros(hit_cap, dtype=np.float32)
+        done, nh = C.c_long(0), C.c_long(0)
+        n = _orc().orc_search_hits(C.byref(self.geom), self.subs, self.spec.ctypes.data,
+                                   first_step, max_steps, out.ctypes.data, max_out,
+                                   C.byref(done), C.byref(nh), keys.ctypes.data,
+                                   pows.ctypes.data, hit_cap)
+        m = min(nh.value, hit_cap)
+        return out[: min(n, max_out)].copy(), done.value, keys[:m].copy(), pows[:m].copy()
 
 
 def insert_hits(hits: np.ndarray, numindep: Sequence[int], max_out: int = 1 << 20):

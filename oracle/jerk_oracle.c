@@ -311,8 +311,12 @@ static double equivalent_gaussian_sigma2(double logp)
     if (logp < -600.0) {
         x = extended_equiv_gaussian_sigma(logp);
     } else {
-        double q = exp(logp);
-        if (q >= 1.0)
+        const double q = exp(logp);
+        /* p = 1 - q < 0 has no normal quantile: the reference's cdfnor2 gives
+           NaN there, and -inf (clamped to 0) at q == 1 */
+        if (q > 1.0)
+            return NAN;
+        if (q == 1.0)
             return 0.0;
         x = norm_quantile_upper(q);
     }
@@ -526,8 +530,11 @@ static void add_vol(orc_vol *fund, const orc_vol *sub, int numharm, int harmnum)
 }
 
 /* ------------------------------------------------------------------ */
-/* Candidate list: insert_new_accelcand, src/accel_utils.c:382-480,     */
-/* on a sorted array (the linked list there is always sorted by r).    */
+/* Candidate list: insert_new_accelcand, src/accel_utils.c:382-480.       */
+/* The list is an array in list order; the walk is the reference's linear   */
+/* walk ("first node with r >= rr, else the last node").  The list is NOT   */
+/* always sorted: when the walk ends at the last node (r < rr) and only the */
+/* node before it is overwritten, the new r lands before a smaller one.     */
 
 typedef struct cand_list {
     orc_cand *c;
@@ -553,24 +560,16 @@ static void list_remove_at(cand_list *L, long pos)
 
 static int insert_cand(cand_list *L, orc_cand v)
 {
-    long lo, hi, tmp, prev;
+    long tmp, prev;
     double prev_diff_r = ACCEL_CLOSEST_R + 1.0, next_diff_r;
     int added = 0;
     if (L->n == 0) {
         list_insert_at(L, 0, v);
         return 1;
     }
-    /* the walk stops at the first node with r >= rr, or at the last node */
-    lo = 0;
-    hi = L->n - 1;
-    while (lo < hi) {
-        long mid = (lo + hi) / 2;
-        if (L->c[mid].r < v.r)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    tmp = lo;
+    tmp = 0;
+    while (tmp < L->n - 1 && L->c[tmp].r < v.r)
+        tmp++;
     prev = tmp - 1;
     next_diff_r = fabs(v.r - L->c[tmp].r);
     if (prev >= 0)
@@ -605,9 +604,31 @@ static int insert_cand(cand_list *L, orc_cand v)
     return added;
 }
 
+/* Optional record of every threshold crossing, keyed like the product's
+ * hits: ((((rstep * numharmstages + stage) * numw + ii) * numz + jj) * numrs + kk */
+typedef struct hit_rec {
+    unsigned long long *keys;
+    float *pows;
+    long n, cap;
+    long long rstep;
+} hit_rec;
+
+static void rec_hit(hit_rec *h, const orc_geom *g, const orc_vol *f, int stage, int ii, int jj,
+                    int kk, float pw)
+{
+    if (!h)
+        return;
+    if (h->n < h->cap) {
+        h->keys[h->n] = ((((unsigned long long)h->rstep * g->numharmstages + stage) * f->numws +
+                          ii) * f->numzs + jj) * f->numrs + kk;
+        h->pows[h->n] = pw;
+    }
+    h->n++;
+}
+
 /* search_ffdotpows, src/accel_utils.c:1507-1555 (single thread order) */
 static void search_vol(const orc_geom *g, const orc_vol *f, int numharm, cand_list *L,
-                       long *nhits)
+                       long *nhits, hit_rec *hr)
 {
     int stage = 0;
     while ((1 << stage) < numharm)
@@ -627,6 +648,7 @@ static void search_vol(const orc_geom *g, const orc_vol *f, int numharm, cand_li
                     c.z = (f->zlo + jj * (double)ACCEL_DZ) / (double)numharm;
                     c.w = (f->wlo + ii * (double)ACCEL_DW) / (double)numharm;
                     insert_cand(L, c);
+                    rec_hit(hr, g, f, stage, ii, jj, kk, pw);
                     (*nhits)++;
                 }
             }
@@ -687,10 +709,13 @@ int orc_summed(const orc_geom *g, const orc_sub *subs, const float *fft, double 
  * (1/1), (1/2), (1/4), (3/4), (1/8), ...  Returns the number of candidates
  * in the final list; up to max_out are copied to out.  *nhits receives the
  * number of threshold crossings (every call to insert). */
-long orc_search(const orc_geom *g, const orc_sub *subs, const float *fft, long first_step,
-                long max_steps, orc_cand *out, long max_out, long *steps_done, long *nhits)
+long orc_search_hits(const orc_geom *g, const orc_sub *subs, const float *fft, long first_step,
+                     long max_steps, orc_cand *out, long max_out, long *steps_done, long *nhits,
+                     unsigned long long *hit_keys, float *hit_pows, long hit_cap)
 {
     cand_list L = {NULL, 0, 0};
+    hit_rec hr = {hit_keys, hit_pows, 0, hit_keys ? hit_cap : 0, 0};
+    hit_rec *hp = hit_keys ? &hr : NULL;
     const int rstep = g->corr_uselen * ACCEL_DR;
     double startr = g->rlo + (double)first_step * rstep;
     long nsteps = 0, n;
@@ -700,8 +725,9 @@ long orc_search(const orc_geom *g, const orc_sub *subs, const float *fft, long f
         const double lastr = nextr - ACCEL_DR;
         orc_vol fund;
         int idx = 1;
+        hr.rstep = first_step + nsteps;
         fderivs(g, &subs[0], fft, startr, lastr, &fund);
-        search_vol(g, &fund, 1, &L, nhits);
+        search_vol(g, &fund, 1, &L, nhits, hp);
         for (int stage = 1; stage < g->numharmstages; stage++) {
             int harmtosum = 1 << stage;
             for (int harm = 1; harm < harmtosum; harm += 2, idx++) {
@@ -710,7 +736,7 @@ long orc_search(const orc_geom *g, const orc_sub *subs, const float *fft, long f
                 add_vol(&fund, &sub, harmtosum, harm);
                 free_vol(&sub);
             }
-            search_vol(g, &fund, harmtosum, &L, nhits);
+            search_vol(g, &fund, harmtosum, &L, nhits, hp);
         }
         free_vol(&fund);
         startr = nextr;
@@ -723,6 +749,13 @@ long orc_search(const orc_geom *g, const orc_sub *subs, const float *fft, long f
     if (steps_done)
         *steps_done = nsteps;
     return n;
+}
+
+long orc_search(const orc_geom *g, const orc_sub *subs, const float *fft, long first_step,
+                long max_steps, orc_cand *out, long max_out, long *steps_done, long *nhits)
+{
+    return orc_search_hits(g, subs, fft, first_step, max_steps, out, max_out, steps_done, nhits,
+                           NULL, NULL, 0);
 }
 
 /* Apply insert_new_accelcand to a given hit sequence (power, numharm, r, z,

@@ -217,6 +217,47 @@ long ref_search(refctx *c, long max_steps, ref_cand *out, long max_out, long *st
     return ncand;
 }
 
+/* Feed a hit sequence, one hit per call, through the reference's own
+ * search_ffdotpows (and so its static insert_new_accelcand): each hit is a
+ * 1x1x1 volume at fundamental bin rlo[i] with power pows[i], searched as
+ * numharm[i] summed harmonics.  Powers must exceed obs.powcut of their stage.
+ * Returns the final list like ref_search. */
+long ref_insert_sequence(refctx *c, long n, const float *pows, const long long *rlo,
+                         const int *numharm, ref_cand *out, long max_out)
+{
+    GSList *cands = NULL, *lp;
+    long ncand = 0;
+    float *cell = gen_fvect(1);
+    float *rows[1] = {cell};
+    float **planes[1] = {rows};
+    for (long i = 0; i < n; i++) {
+        ffdotpows f;
+        memset(&f, 0, sizeof(f));
+        f.rlo = rlo[i];
+        f.zlo = 0;
+        f.wlo = 0;
+        f.numrs = f.numzs = f.numws = 1;
+        f.powers = planes;
+        cell[0] = pows[i];
+        cands = search_ffdotpows(&f, numharm[i], &c->obs, cands);
+    }
+    vect_free(cell);
+    for (lp = cands; lp; lp = lp->next, ncand++) {
+        if (ncand < max_out && out) {
+            accelcand *a = (accelcand *)lp->data;
+            out[ncand].power = a->power;
+            out[ncand].sigma = a->sigma;
+            out[ncand].numharm = a->numharm;
+            out[ncand].r = a->r;
+            out[ncand].z = a->z;
+            out[ncand].w = a->w;
+        }
+    }
+    g_slist_foreach(cands, free_accelcand, NULL);
+    g_slist_free(cands);
+    return ncand;
+}
+
 double ref_candidate_sigma(double power, int numsum, double numtrials)
 {
     return candidate_sigma(power, numsum, numtrials);

@@ -1,0 +1,283 @@
+// Shared-memory mixed-radix Stockham FFT for one CTA (sm_100a, FP32).
+//
+// One CTA of T threads transforms one N-point complex sequence.  The first
+// stage takes its inputs from a functor (so the caller can fuse a load and a
+// multiply into it, and keep per-thread operands such as a kernel row in
+// registers across many transforms), the middle stages run in place in a
+// shared buffer of N float2, and the last stage hands every output to a
+// second functor (so the caller can fuse |.|^2 and the store into it).
+//
+// Stage s with radix R and Ns = product of the earlier radices (Stockham
+// autosort, decimation in time):
+//   butterfly j in [0, N/R):  v[r] = x[j + r*N/R] * W^(r * (j % Ns) * N/(Ns*R))
+//                             y = DFT_R(v)
+//                             out[(j/Ns)*Ns*R + j%Ns + r*Ns] = y[r]
+// with W = exp(SIGN * 2*pi*i / N).  Twiddles come from a table of the N
+// forward roots exp(-2*pi*i*m/N) (computed in double on the host), conjugated
+// for SIGN = +1.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace jerk {
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b): the correlation product of the reference, (ar*br + ai*bi, ai*br - ar*bi)
+__device__ __forceinline__ float2 cmulconj(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by SIGN * i
+template <int SIGN>
+__device__ __forceinline__ float2 mul_si(float2 a)
+{
+    return SIGN > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// In-register DFT of radix R with exponent sign SIGN (unnormalised).
+template <int R, int SIGN> struct Dft;
+
+template <int SIGN> struct Dft<2, SIGN> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <int SIGN> struct Dft<4, SIGN> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+        float2 c = cadd(v[1], v[3]), d = mul_si<SIGN>(csub(v[1], v[3]));
+        v[0] = cadd(a, c);
+        v[1] = cadd(b, d);
+        v[2] = csub(a, c);
+        v[3] = csub(b, d);
+    }
+};
+
+template <int SIGN> struct Dft<8, SIGN> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<4, SIGN>::run(e);
+        Dft<4, SIGN>::run(o);
+        const float h = 0.70710678118654752440f;
+        // W8^1 = h(1 + SIGN i), W8^2 = SIGN i, W8^3 = h(-1 + SIGN i)
+        float2 o1 = make_float2(h * (o[1].x - SIGN * o[1].y), h * (o[1].y + SIGN * o[1].x));
+        float2 o2 = mul_si<SIGN>(o[2]);
+        float2 o3 = make_float2(h * (-o[3].x - SIGN * o[3].y), h * (-o[3].y + SIGN * o[3].x));
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);
+        v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);
+        v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);
+        v[7] = csub(e[3], o3);
+    }
+};
+
+template <int SIGN> struct Dft<3, SIGN> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        const float s3 = 0.86602540378443864676f;  // sin(2 pi / 3)
+        float2 t = cadd(v[1], v[2]);
+        float2 d = mul_si<SIGN>(cscale(csub(v[1], v[2]), s3));
+        float2 m = make_float2(v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y);
+        v[0] = cadd(v[0], t);
+        v[1] = cadd(m, d);
+        v[2] = csub(m, d);
+    }
+};
+
+template <int SIGN> struct Dft<5, SIGN> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        const float c1 = 0.30901699437494742410f;   // cos(2 pi/5)
+        const float c2 = -0.80901699437494742410f;  // cos(4 pi/5)
+        const float s1 = 0.95105651629515357212f;   // sin(2 pi/5)
+        const float s2 = 0.58778525229247312917f;   // sin(4 pi/5)
+        float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+        float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+        float2 x0 = v[0];
+        float2 p1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+        float2 p2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+        float2 q1 = mul_si<SIGN>(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
+        float2 q2 = mul_si<SIGN>(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
+        v[0] = make_float2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+        v[1] = cadd(p1, q1);
+        v[4] = csub(p1, q1);
+        v[2] = cadd(p2, q2);
+        v[3] = csub(p2, q2);
+    }
+};
+
+// Radix plans: the first radix fixes the thread count T = N / R0.
+template <int N> struct FftPlan;
+#define JERK_FFT_PLAN(NN, ...)                                                  \
+    template <> struct FftPlan<NN> {                                            \
+        static constexpr int radices[] = {__VA_ARGS__};                         \
+        static constexpr int nstages = sizeof(radices) / sizeof(int);           \
+        static constexpr int R0 = radices[0];                                   \
+        static constexpr int T = NN / R0;                                       \
+    };
+JERK_FFT_PLAN(128, 4, 8, 4)
+JERK_FFT_PLAN(192, 4, 4, 4, 3)
+JERK_FFT_PLAN(256, 8, 8, 4)
+JERK_FFT_PLAN(384, 8, 4, 4, 3)
+JERK_FFT_PLAN(512, 8, 8, 8)
+JERK_FFT_PLAN(768, 8, 8, 4, 3)
+JERK_FFT_PLAN(1024, 8, 8, 4, 4)
+JERK_FFT_PLAN(1280, 8, 8, 4, 5)
+JERK_FFT_PLAN(2048, 8, 8, 8, 4)
+JERK_FFT_PLAN(4096, 8, 8, 8, 8)
+JERK_FFT_PLAN(5120, 8, 8, 8, 2, 5)
+JERK_FFT_PLAN(7680, 8, 8, 8, 3, 5)
+#undef JERK_FFT_PLAN
+
+template <int SIGN>
+__device__ __forceinline__ float2 twiddle(const float2 *tw, int m)
+{
+    float2 w = tw[m];
+    return SIGN > 0 ? make_float2(w.x, -w.y) : w;
+}
+
+// One middle stage, in place in buf.  Every thread of the block must call it
+// (it holds two barriers); only threads with act == true (tid < T) work.
+template <int N, int SIGN, int T, int Ns, int R>
+__device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw, int tid, bool act)
+{
+    constexpr int NB = N / R;
+    constexpr int PER = (NB + T - 1) / T;
+    float2 v[PER][R];
+    if (act) {
+#pragma unroll
+        for (int p = 0; p < PER; p++) {
+            const int j = tid + p * T;
+            if (NB % T == 0 || j < NB) {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    v[p][r] = buf[j + r * NB];
+            }
+        }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int p = 0; p < PER; p++) {
+            const int j = tid + p * T;
+            if (NB % T == 0 || j < NB) {
+                const int k = j % Ns;
+                if (Ns > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; r++)
+                        v[p][r] = cmul(v[p][r], twiddle<SIGN>(tw, r * k * (N / (Ns * R))));
+                }
+                Dft<R, SIGN>::run(v[p]);
+                const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    buf[idxD + r * Ns] = v[p][r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Last stage: Ns * R == N, so the output index of (j, r) is j + r * Ns.
+// No barrier inside; the caller must sync before buf is written again.
+template <int N, int SIGN, int T, int Ns, int R, class Out>
+__device__ __forceinline__ void fft_stage_last(const float2 *buf, const float2 *tw, int tid,
+                                               bool act, Out &out)
+{
+    constexpr int NB = N / R;
+    constexpr int PER = (NB + T - 1) / T;
+    static_assert(Ns * R == N, "last stage");
+    if (!act)
+        return;
+#pragma unroll
+    for (int p = 0; p < PER; p++) {
+        const int j = tid + p * T;
+        if (NB % T == 0 || j < NB) {
+            float2 v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                v[r] = buf[j + r * NB];
+#pragma unroll
+            for (int r = 1; r < R; r++)
+                v[r] = cmul(v[r], twiddle<SIGN>(tw, r * j * (N / (Ns * R))));
+            Dft<R, SIGN>::run(v);
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                out(j + r * Ns, v[r]);
+        }
+    }
+}
+
+// Stages I..end (I == nstages - 1 is the last one).
+template <int N, int SIGN, int T, int I, int Ns, bool LAST = (I == FftPlan<N>::nstages - 1)>
+struct FftTail;
+
+template <int N, int SIGN, int T, int I, int Ns>
+struct FftTail<N, SIGN, T, I, Ns, true> {
+    template <class Out>
+    __device__ __forceinline__ static void run(float2 *buf, const float2 *tw, int tid, bool act,
+                                               Out &out)
+    {
+        constexpr int R = FftPlan<N>::radices[I];
+        fft_stage_last<N, SIGN, T, Ns, R>(buf, tw, tid, act, out);
+    }
+};
+
+template <int N, int SIGN, int T, int I, int Ns>
+struct FftTail<N, SIGN, T, I, Ns, false> {
+    template <class Out>
+    __device__ __forceinline__ static void run(float2 *buf, const float2 *tw, int tid, bool act,
+                                               Out &out)
+    {
+        constexpr int R = FftPlan<N>::radices[I];
+        fft_stage_inplace<N, SIGN, T, Ns, R>(buf, tw, tid, act);
+        FftTail<N, SIGN, T, I + 1, Ns * R>::run(buf, tw, tid, act, out);
+    }
+};
+
+// Full transform by the whole block.  Threads with tid < T = N / R0 own
+// first-stage butterfly j = tid, whose inputs are in(r) for the element
+// index m = tid + r * (N / R0), r in [0, R0).  Every thread of the block
+// must call it (barriers); threads with tid >= T do no work.  buf[N] is
+// shared memory.  When it returns, outputs have been handed to out(m, y) by
+// the threads that computed them; the caller must __syncthreads() before
+// buf is written again.
+template <int N, int SIGN, class In, class Out>
+__device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid, In &in,
+                                          Out &out)
+{
+    using P = FftPlan<N>;
+    constexpr int R0 = P::R0;
+    constexpr int T = P::T;
+    const bool act = tid < T;
+    if (act) {
+        float2 v[R0];
+#pragma unroll
+        for (int r = 0; r < R0; r++)
+            v[r] = in(r);
+        Dft<R0, SIGN>::run(v);
+#pragma unroll
+        for (int r = 0; r < R0; r++)
+            buf[tid * R0 + r] = v[r];
+    }
+    __syncthreads();
+    FftTail<N, SIGN, T, 1, R0>::run(buf, tw, tid, act, out);
+}
+
+}  // namespace jerk

@@ -1,0 +1,391 @@
+// Jerk-search kernels for sm_100a (FP32 SIMT; the method is spectral, not a
+// dense contraction, so there is no tensor-core path).
+//
+// Per batch of rsteps (one rstep = corr_uselen interbinned fundamental
+// bins), three kernels run on one stream:
+//
+//  1. prep_kernel      one CTA per (rstep, subharmonic): gathers fftlen/2
+//                      spectral bins, block-median normalises them exactly as
+//                      the reference does, spreads them to interbins, takes
+//                      the forward FFT, and writes the rinds lookup table.
+//                      (reference: src/accel_utils.c:1107-1210, done there on
+//                      the host; src/accel_utils_cu.c:464-588)
+//  2. corr_kernel<N>   one CTA per response-kernel row (w, z) of every
+//                      subharmonic with fftlen N; the kernel row stays in
+//                      registers while the CTA walks all rsteps of the batch:
+//                      multiply by conj(kernel), inverse FFT in shared memory,
+//                      |.|^2 / fftlen^2 of the numrs good bins straight to the
+//                      ffdot volume.  (reference: src/accel_utils.c:1245-1285;
+//                      src/accel_kernels.cu:930-988 + cuFFT)
+//  3. harmsum_kernel   one thread per fundamental (w, z, r): the stage-0
+//                      threshold, then the subharmonic adds in the reference's
+//                      order with a threshold after each stage; hits go to a
+//                      compact list through warp-aggregated atomics.
+//                      (reference: src/accel_utils.c:1356-1377, 1507-1555;
+//                      src/accel_kernels.cu:781-862)
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "jerk_fft.cuh"
+#include "jerk_kernels.cuh"
+
+namespace jerk {
+
+// ---------------------------------------------------------------------------
+// Exact double-precision index arithmetic (no FMA contraction), as the
+// reference's host code computes it (src/accel_utils.c:54-97).
+
+__device__ __forceinline__ double calc_required_r_d(double hf, double rfull)
+{
+    return __dmul_rn(rint(__dmul_rn(__dmul_rn(2.0, rfull), hf)), 0.5);
+}
+
+__device__ __forceinline__ int index_from_r_d(double r, double lor)
+{
+    return __double2int_rz(__dadd_rn(__dmul_rn(__dsub_rn(r, lor), 2.0), 1e-14));
+}
+
+// ---------------------------------------------------------------------------
+// 1. Data preparation.
+
+constexpr double kLn2 = 0.69314718055994530942;  // log(2.0), correctly rounded
+
+template <int M>
+struct NextPow2 {
+    static constexpr int value = (M <= 1) ? 1 : 2 * NextPow2<(M + 1) / 2>::value;
+};
+template <>
+struct NextPow2<1> {
+    static constexpr int value = 1;
+};
+
+template <int N>
+__device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
+{
+    constexpr int M = N / 2;  // numdata = fftlen / ACCEL_NUMBETWEEN
+    constexpr int MP = NextPow2<M>::value;
+    constexpr int R0 = FftPlan<N>::R0;
+    const SubDev sd = P.subs[s];
+    const StepDev st = P.steps[(P.first_rstep + b) * P.nsubs + s];
+    float2 *buf = reinterpret_cast<float2 *>(smem);
+    float2 *tw = buf + N;
+    float2 *data = tw + N;
+    float *keys = reinterpret_cast<float *>(data + M);
+    const int tid = threadIdx.x, nt = blockDim.x;
+
+    for (int i = tid; i < N; i += nt)
+        tw[i] = P.twiddles[sd.twoff + i];
+
+    // get_fourier_amplitudes: M bins from lobin, zero outside the file
+    const long long lobin = st.rlo - sd.halfwidth;
+    for (int i = tid; i < M; i += nt) {
+        const long long bi = lobin - P.lobin + i;
+        float2 v = make_float2(0.f, 0.f);
+        if (bi >= 0 && bi < P.numbins)
+            v = P.spec[bi];
+        data[i] = v;
+        keys[i] = __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+    }
+    for (int i = M + tid; i < MP; i += nt)
+        keys[i] = INFINITY;
+    __syncthreads();
+
+    double norm;
+    if (P.nph > 0.0f) {
+        norm = __ddiv_rn(1.0, __dsqrt_rn((double)P.nph));
+    } else {
+        // median(): the order statistic of rank (M-1)/2 (src/median.c);
+        // bitonic sort of the powers, padded with +inf
+        for (int k = 2; k <= MP; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = tid; i < MP; i += nt) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const float a = keys[i], c = keys[ixj];
+                        const bool up = (i & k) == 0;
+                        if ((a > c) == up) {
+                            keys[i] = c;
+                            keys[ixj] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        const double med = (double)keys[(M - 1) / 2];
+        norm = __ddiv_rn(1.0, __dsqrt_rn(__ddiv_rn(med, kLn2)));
+    }
+    for (int i = tid; i < M; i += nt) {
+        float2 v = data[i];
+        v.x = __double2float_rn(__dmul_rn((double)v.x, norm));
+        v.y = __double2float_rn(__dmul_rn((double)v.y, norm));
+        data[i] = v;
+    }
+    __syncthreads();
+
+    // spread_no_pad (data at even interbins) + forward FFT (sign -1)
+    float2 *outp = P.prepped + sd.data_off + (long long)b * N;
+    auto in = [&](int r) -> float2 {
+        const int m = tid + r * (N / R0);
+        return (m & 1) ? make_float2(0.f, 0.f) : data[m >> 1];
+    };
+    auto out = [&](int m, float2 y) { outp[m] = y; };
+    fft_block<N, -1>(buf, tw, tid, in, out);
+
+    // rinds: fundamental r -> subharmonic r index (src/accel_utils.c:1114-1123)
+    if (sd.numharm > 1) {
+        uint16_t *rinds = P.rinds + ((long long)b * P.nsubs + s) * P.corr_uselen;
+        const double rlo = (double)st.rlo;
+        for (int ii = tid; ii < P.corr_uselen; ii += nt) {
+            const double rr = __dadd_rn(st.fullrlo, __dmul_rn((double)ii, 0.5));
+            const double subr = calc_required_r_d(sd.harm_fract, rr);
+            rinds[ii] = (uint16_t)index_from_r_d(subr, rlo);
+        }
+    }
+}
+
+__global__ void prep_kernel(const SearchDev P)
+{
+    extern __shared__ float smem[];
+    const int b = blockIdx.x, s = blockIdx.y;
+    switch (P.subs[s].fftlen) {
+#define JERK_PREP_CASE(NN)                   \
+    case NN:                                 \
+        prep_impl<NN>(P, b, s, smem);        \
+        break;
+        JERK_PREP_CASE(128)
+        JERK_PREP_CASE(192)
+        JERK_PREP_CASE(256)
+        JERK_PREP_CASE(384)
+        JERK_PREP_CASE(512)
+        JERK_PREP_CASE(768)
+        JERK_PREP_CASE(1024)
+        JERK_PREP_CASE(1280)
+        JERK_PREP_CASE(2048)
+        JERK_PREP_CASE(4096)
+        JERK_PREP_CASE(5120)
+        JERK_PREP_CASE(7680)
+#undef JERK_PREP_CASE
+    default:
+        break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Correlation: one CTA per kernel row, all rsteps of the batch.
+
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N>::T) corr_kernel(const SearchDev P, const RowGroup G)
+{
+    constexpr int R0 = FftPlan<N>::R0;
+    constexpr int T = FftPlan<N>::T;
+    extern __shared__ float2 sm2[];
+    float2 *buf = sm2;
+    float2 *tw = sm2 + N;
+    const int tid = threadIdx.x;
+    const int row = blockIdx.x;
+    int gi = 0;
+    while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
+        gi++;
+    const int s = G.sub[gi];
+    const int lrow = row - G.rowstart[gi];
+    const SubDev sd = P.subs[s];
+
+    for (int i = tid; i < N; i += T)
+        tw[i] = P.twiddles[sd.twoff + i];
+
+    // the kernel row, in the order this thread's first-stage butterfly reads it
+    float2 kreg[R0];
+    const float2 *K = P.bank + sd.kern_off + (long long)lrow * N;
+#pragma unroll
+    for (int r = 0; r < R0; r++)
+        kreg[r] = K[tid + r * (N / R0)];
+    __syncthreads();
+
+    const int offset = sd.halfwidth * 2;  // binoffset * ACCEL_NUMBETWEEN
+    const float norm = sd.pownorm;
+    for (int b = 0; b < P.nb; b++) {
+        const float2 *D = P.prepped + sd.data_off + (long long)b * N;
+        const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
+        float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
+                      (long long)lrow * sd.stride;
+        auto in = [&](int r) -> float2 { return cmulconj(D[tid + r * (N / R0)], kreg[r]); };
+        auto out = [&](int m, float2 y) {
+            const int kk = m - offset;
+            if (kk >= 0 && kk < numrs)
+                outp[kk] = __fmul_rn(__fadd_rn(__fmul_rn(y.x, y.x), __fmul_rn(y.y, y.y)), norm);
+        };
+        fft_block<N, +1>(buf, tw, tid, in, out);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Harmonic summing + threshold + compaction.
+
+constexpr int kHarmThreads = 256;
+
+__global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P)
+{
+    __shared__ uint16_t s_rind[kMaxSubs][kHarmThreads];
+    __shared__ long long s_base[kMaxSubs];
+    __shared__ int s_stride[kMaxSubs];
+    __shared__ int s_numrs[kMaxSubs];
+    const int b = blockIdx.z;
+    const int ii = blockIdx.y;
+    const int tid = threadIdx.x;
+    const int kk = blockIdx.x * kHarmThreads + tid;
+    const bool valid = kk < P.corr_uselen;
+    const int lane = tid & 31;
+    const long long rstep = P.first_rstep + b;
+
+    if (tid < P.nsubs) {
+        const SubDev sd = P.subs[tid];
+        const int wind = tid == 0 ? ii : P.wind[sd.wind_off + ii];
+        s_base[tid] = sd.plane_off + (long long)b * sd.plane_size +
+                      (long long)wind * sd.numz * sd.stride;
+        s_stride[tid] = sd.stride;
+        s_numrs[tid] = P.steps[rstep * P.nsubs + tid].numrs;
+    }
+    __syncthreads();
+    for (int s = 1; s < P.nsubs; s++) {
+        uint16_t ri = valid ? P.rinds[((long long)b * P.nsubs + s) * P.corr_uselen + kk] : 0;
+        if (ri >= s_numrs[s]) {
+            // cannot happen for tables built as the reference builds them;
+            // record it and read a cell that exists
+            atomicOr(P.status, 1u);
+            ri = 0;
+        }
+        s_rind[s][tid] = ri;
+    }
+    __syncthreads();
+
+    const float *planes = P.planes;
+    const long long base0 = s_base[0];
+    const int stride0 = s_stride[0];
+    for (int jj = 0; jj < P.numz0; jj++) {
+        float v = valid ? planes[base0 + (long long)jj * stride0 + kk] : 0.0f;
+        int s = 1;
+        for (int stage = 0; stage < P.nstages; stage++) {
+            if (stage > 0) {
+                const int nadd = 1 << (stage - 1);
+                for (int h = 0; h < nadd; h++, s++) {
+                    const SubDev &sd = P.subs[s];
+                    const int zind = P.zinds[sd.zinds_off + jj];
+                    if (valid)
+                        v = __fadd_rn(v, planes[s_base[s] + (long long)zind * s_stride[s] +
+                                                s_rind[s][tid]]);
+                }
+            }
+            const bool hit = valid && v > P.powcut[stage];
+            const unsigned mask = __ballot_sync(0xffffffffu, hit);
+            if (mask) {
+                const int leader = __ffs(mask) - 1;
+                unsigned int base = 0;
+                if (lane == leader)
+                    base = atomicAdd(P.hit_count, (unsigned int)__popc(mask));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (hit) {
+                    const unsigned long long idx = base + __popc(mask & ((1u << lane) - 1u));
+                    if ((long long)idx < P.max_hits) {
+                        const unsigned long long key =
+                            ((((unsigned long long)rstep * P.nstages + stage) * P.numw0 + ii) *
+                                 P.numz0 + jj) * P.corr_uselen + kk;
+                        P.hit_keys[idx] = key;
+                        P.hit_pows[idx] = v;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers (host side of this translation unit).
+
+size_t prep_smem_bytes(int maxfft)
+{
+    const int M = maxfft / 2;
+    int MP = 1;
+    while (MP < M)
+        MP <<= 1;
+    return sizeof(float2) * (size_t)(2 * maxfft + M) + sizeof(float) * (size_t)MP;
+}
+
+int prep_threads(int maxfft)
+{
+    // the widest FFT plan's thread count, at least a warp multiple of 128
+    int t = 128;
+    switch (maxfft) {
+    case 4096: t = FftPlan<4096>::T; break;
+    case 5120: t = FftPlan<5120>::T; break;
+    case 7680: t = FftPlan<7680>::T; break;
+    default: t = 256; break;
+    }
+    return t < 256 ? 256 : t;
+}
+
+cudaError_t launch_prep(const SearchDev &P, int maxfft, cudaStream_t st)
+{
+    const size_t smem = prep_smem_bytes(maxfft);
+    cudaError_t e = cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    prep_kernel<<<dim3(P.nb, P.nsubs), prep_threads(maxfft), smem, st>>>(P);
+    return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t launch_corr_n(const SearchDev &P, const RowGroup &G, int rows, cudaStream_t st)
+{
+    const size_t smem = sizeof(float2) * 2 * N;
+    cudaError_t e = cudaFuncSetAttribute(corr_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    corr_kernel<N><<<rows, FftPlan<N>::T, smem, st>>>(P, G);
+    return cudaGetLastError();
+}
+
+bool fftlen_supported(int n)
+{
+    switch (n) {
+    case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 1280:
+    case 2048: case 4096: case 5120: case 7680:
+        return true;
+    default:
+        return false;
+    }
+}
+
+cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int rows,
+                        cudaStream_t st)
+{
+    switch (fftlen) {
+    case 128: return launch_corr_n<128>(P, G, rows, st);
+    case 192: return launch_corr_n<192>(P, G, rows, st);
+    case 256: return launch_corr_n<256>(P, G, rows, st);
+    case 384: return launch_corr_n<384>(P, G, rows, st);
+    case 512: return launch_corr_n<512>(P, G, rows, st);
+    case 768: return launch_corr_n<768>(P, G, rows, st);
+    case 1024: return launch_corr_n<1024>(P, G, rows, st);
+    case 1280: return launch_corr_n<1280>(P, G, rows, st);
+    case 2048: return launch_corr_n<2048>(P, G, rows, st);
+    case 4096: return launch_corr_n<4096>(P, G, rows, st);
+    case 5120: return launch_corr_n<5120>(P, G, rows, st);
+    case 7680: return launch_corr_n<7680>(P, G, rows, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st)
+{
+    const dim3 grid((P.corr_uselen + kHarmThreads - 1) / kHarmThreads, P.numw0, P.nb);
+    harmsum_kernel<<<grid, kHarmThreads, 0, st>>>(P);
+    return cudaGetLastError();
+}
+
+}  // namespace jerk

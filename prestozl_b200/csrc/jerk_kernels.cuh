@@ -1,0 +1,81 @@
+// Device-side data structures shared by the jerk-search kernels and the host
+// plan (jerk_plan.cpp).  Plain structs, no torch types.
+#pragma once
+
+#include <cstdint>
+
+namespace jerk {
+
+constexpr int kMaxSubs = 32;      // numharm <= 32 -> 1 + 31 subharmonic planes
+constexpr int kMaxStages = 6;
+
+// One subharmonic (harmnum / numharm) as laid out on the device.
+struct SubDev {
+    int numharm, harmnum;
+    double harm_fract;        // harmnum / numharm, computed on the host
+    int numz, numw;           // kernel grid (numkern_zdim, numkern_wdim)
+    int fftlen;
+    int halfwidth;            // kern[0][0].kern_half_width (bins)
+    int stride;               // plane row stride in floats (>= max numrs, multiple of 4)
+    int zlo, wlo;             // lowest z / w of this subharmonic's volume
+    float pownorm;            // (float)(1.0 / (fftlen * fftlen))
+    int twoff;                // offset (float2) of this fftlen's twiddle table
+    long long kern_off;       // offset (float2) of kernel [0][0] in the bank
+    long long plane_off;      // offset (floats) of the b = 0 volume in the batch planes
+    long long plane_size;     // floats per volume (numw * numz * stride)
+    long long data_off;       // offset (float2) of the b = 0 prepared chunk
+    int zinds_off;            // offset of zinds (u16, fundamental numz entries)
+    int wind_off;             // offset of wind (int, fundamental numw entries)
+};
+
+// One (rstep, subharmonic): where its chunk starts and how many r it yields.
+struct StepDev {
+    long long rlo;            // floor(calc_required_r(hf, fullrlo))
+    double fullrlo;           // fundamental r of the rstep's first bin
+    int numrs;
+    int pad;
+};
+
+struct SearchDev {
+    // spectrum
+    const float2 *spec;
+    long long numbins;
+    long long lobin;          // obs lobin: bin 0 of spec
+    // geometry
+    int nsubs;
+    int nstages;
+    int corr_uselen;
+    int numz0, numw0;         // fundamental volume dims
+    int norm_type;
+    float nph;
+    float powcut[kMaxStages];
+    // tables
+    const SubDev *subs;
+    const StepDev *steps;     // [rstep][nsubs], whole spectrum
+    const float2 *bank;
+    const float2 *twiddles;
+    const uint16_t *zinds;
+    const int *wind;
+    // per-batch work
+    long long first_rstep;    // rstep index of b = 0
+    int nb;                   // rsteps in this batch
+    float2 *prepped;          // prepared chunks
+    float *planes;            // ffdot volumes
+    uint16_t *rinds;          // [b][s][corr_uselen]
+    // hits
+    unsigned long long *hit_keys;
+    float *hit_pows;
+    unsigned int *hit_count;
+    long long max_hits;
+    unsigned int *status;     // bit 0: a subharmonic r index fell outside its row
+};
+
+// The corr_kernel launch for one fftlen covers the rows (w, z) of every
+// subharmonic with that fftlen, numbered consecutively.
+struct RowGroup {
+    int n;                       // subharmonics in this fftlen group
+    int sub[kMaxSubs];
+    int rowstart[kMaxSubs + 1];  // prefix sums of numw * numz
+};
+
+}  // namespace jerk

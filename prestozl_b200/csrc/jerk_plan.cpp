@@ -1,0 +1,1072 @@
+// Host side of libjerk: search geometry, the device plan, the batch loop,
+// candidate assembly, and the C ABI of include/jerk.h.
+//
+// The plan owns every device buffer of one search configuration (kernel bank,
+// twiddles, lookup tables, per-batch volumes, hit buffer) so that a search
+// allocates nothing per rstep (the reference allocates and frees per call,
+// src/accel_utils_cu.c:451-455, 591-611).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "jerk.h"
+#include "jerk_kernels.cuh"
+
+namespace jerk {
+size_t prep_smem_bytes(int maxfft);
+cudaError_t launch_prep(const SearchDev &P, int maxfft, cudaStream_t st);
+cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int rows,
+                        cudaStream_t st);
+cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st);
+bool fftlen_supported(int n);
+}  // namespace jerk
+
+using namespace jerk;
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+static int cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(JERK_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define JERK_CUDA(call)                                  \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess)                           \
+            return cuda_fail(e_, #call);                 \
+    } while (0)
+
+extern "C" const char *jerk_last_error(void) { return g_err.c_str(); }
+extern "C" void jerk_free(void *p) { free(p); }
+
+// ---------------------------------------------------------------------------
+// Reference index arithmetic (src/accel_utils.c:36-97), host side.
+
+static constexpr double kDR = 0.5;
+static constexpr int kRDR = 2;
+static constexpr int kDZ = 2;
+static constexpr double kRDZ = 0.5;
+static constexpr int kDW = 20;
+static constexpr double kRDW = 0.05;
+static constexpr double kDblCorrect = 1e-14;
+static constexpr double kClosestR = 15.0;
+
+static inline int nearest_int(double x) { return (int)(x < 0 ? x - 0.5 : x + 0.5); }
+static inline double calc_required_r(double hf, double rfull) { return rint(kRDR * rfull * hf) * kDR; }
+static inline int calc_required_z(double hf, double zfull) { return nearest_int(kRDZ * zfull * hf) * kDZ; }
+static inline int calc_required_w(double hf, double wfull) { return nearest_int(kRDW * wfull * hf) * kDW; }
+static inline int index_from_z(double z, double loz) { return (int)((z - loz) * kRDZ + kDblCorrect); }
+static inline int index_from_w(double w, double low) { return (int)((w - low) * kRDW + kDblCorrect); }
+
+// src/responses.c:27-84 (LOWACC)
+static int z_resp_halfwidth(double z) { return (int)(0.5 * 1.1 * fabs(z)) + 16; }
+static int w_resp_halfwidth(double z, double w)
+{
+    if (fabs(w) < 1.0e-7)
+        return z_resp_halfwidth(z);
+    const double r0 = 0.5 * (w / 6.0 - z), r1 = 0.5 * (w / 6.0 + z);
+    double maxdev = fabs(r0) > fabs(r1) ? fabs(r0) : fabs(r1);
+    const double u_ext = 0.5 - z / w;
+    if (u_ext > 0.0 && u_ext < 1.0) {
+        const double z0 = z - w / 2.0;
+        const double r_ext = 0.5 * w * u_ext * u_ext + z0 * u_ext + r0;
+        maxdev = fabs(r_ext) > maxdev ? fabs(r_ext) : maxdev;
+    }
+    return (int)(1.1 * maxdev) + 16;
+}
+
+static long long next2_to_n(long long x)
+{
+    long long n = 1;
+    while (n < x)
+        n <<= 1;
+    return n;
+}
+
+// src/corr_prep.c:3-35
+static int next_good_fftlen(int N)
+{
+    static const int lens[17] = {128, 192, 256, 384, 512, 768, 1024, 1280, 2048,
+                                 4096, 5120, 7680, 10240, 12288, 15360, 16384, 25600};
+    int ii = 0;
+    if (N <= lens[0])
+        return lens[0];
+    if (N > lens[16])
+        return (int)next2_to_n(N);
+    while (N > lens[ii])
+        ii++;
+    return lens[ii];
+}
+
+static int fftlen_from_kernwidth(int kw)
+{
+    if (kw < 6) return 128;
+    if (kw < 52) return 256;
+    if (kw < 67) return 512;
+    if (kw < 378) return 1024;
+    if (kw < 664) return 2048;
+    if (kw < 1672) return 4096;
+    if (kw < 3015) return 10240;
+    if (kw < 3554) return 15360;
+    if (kw < 6000) return 25600;
+    return (int)next2_to_n(kw * 5);
+}
+
+// ---------------------------------------------------------------------------
+// Statistics: restatement of src/characteristics.c:400-705 for the integer
+// numsum the search uses.
+
+static double log_asymtotic_incomplete_gamma(double a, double z)
+{
+    double x = 1.0, newxpart = 1.0, term = 1.0;
+    int ii = 1;
+    while (fabs(newxpart) > 1e-15) {
+        term *= (a - ii);
+        newxpart = term / pow(z, ii);
+        x += newxpart;
+        ii += 1;
+    }
+    return (a - 1.0) * log(z) - z + log(x);
+}
+
+static double log_asymtotic_gamma(double z)
+{
+    double x = (z - 0.5) * log(z) - z + 0.91893853320467267;
+    const double y = 1.0 / (z * z);
+    x += (((-5.9523809523809529e-4 * y + 7.9365079365079365079365e-4) * y -
+           2.7777777777777777777778e-3) * y + 8.3333333333333333333333e-2) / z;
+    return x;
+}
+
+// Q(a, x) for integer a: exp(-x) sum_{n<a} x^n / n!
+static double q_gamma_int(int a, double x)
+{
+    if (x <= 0.0)
+        return 1.0;
+    double t = exp(-x), sum = t;
+    for (int n = 1; n < a; n++) {
+        t = t * x / n;
+        sum += t;
+    }
+    return sum;
+}
+
+static double chi2_logp(double chi2, double dof)
+{
+    if (chi2 <= 0.0)
+        return -INFINITY;
+    if (chi2 / dof > 15.0 || (dof > 150 && chi2 / dof > 6.0))
+        return log_asymtotic_incomplete_gamma(0.5 * dof, 0.5 * chi2) -
+               log_asymtotic_gamma(0.5 * dof);
+    return log(q_gamma_int((int)(0.5 * dof + 0.5), 0.5 * chi2));
+}
+
+// x with 1 - Phi(x) = q, full double precision
+static double upper_normal_quantile(double q)
+{
+    double lo = -40.0, hi = 40.0, x = 0.0;
+    for (int it = 0; it < 200; it++) {
+        x = 0.5 * (lo + hi);
+        if (0.5 * erfc(x / M_SQRT2) > q)
+            lo = x;
+        else
+            hi = x;
+        if (hi - lo < 1e-15 * (fabs(x) + 1.0))
+            break;
+    }
+    for (int it = 0; it < 3; it++) {
+        const double dens = exp(-0.5 * x * x) / sqrt(2.0 * M_PI);
+        if (dens <= 0.0)
+            break;
+        x += (0.5 * erfc(x / M_SQRT2) - q) / dens;
+    }
+    return x;
+}
+
+static double equivalent_gaussian_sigma(double logp)
+{
+    double x;
+    if (logp < -600.0) {
+        // A&S 26.2.23 on log p
+        const double t = sqrt(-2.0 * logp);
+        const double num = 2.515517 + t * (0.802853 + t * 0.010328);
+        const double den = 1.0 + t * (1.432788 + t * (0.189269 + t * 0.001308));
+        x = t - num / den;
+    } else {
+        const double q = exp(logp);
+        /* p = 1 - q < 0 has no normal quantile: the reference's cdfnor2 gives
+           NaN there, and -inf (clamped to 0) at q == 1 */
+        if (q > 1.0)
+            return NAN;
+        if (q == 1.0)
+            return 0.0;
+        x = upper_normal_quantile(q);
+    }
+    return x < 0.0 ? 0.0 : x;
+}
+
+extern "C" double jerk_candidate_sigma(double power, int numsum, double numtrials)
+{
+    if (power <= 0.0)
+        return 0.0;
+    double logp = chi2_logp(2.0 * power, 2.0 * numsum);
+    logp += log(numtrials);
+    return equivalent_gaussian_sigma(logp);
+}
+
+extern "C" double jerk_power_for_sigma(double sigma, int numsum, double numtrials)
+{
+    const double q = 0.5 * erfc(sigma / M_SQRT2) / numtrials;
+    const double logq = log(q);
+    double lo = 0.0, hi = 1.0;
+    while (log(q_gamma_int(numsum, hi)) > logq)
+        hi *= 2.0;
+    for (int it = 0; it < 200; it++) {
+        const double mid = 0.5 * (lo + hi);
+        if (log(q_gamma_int(numsum, mid)) > logq)
+            lo = mid;
+        else
+            hi = mid;
+        if (hi - lo <= 1e-15 * hi)
+            break;
+    }
+    return 0.5 * (lo + hi);
+}
+
+// ---------------------------------------------------------------------------
+// Geometry (the sizing part of create_accelobs, src/accel_utils.c:1795-2004)
+
+extern "C" int jerk_obs_from_params(long long numbins, long long N, double dt, int zmax, int wmax,
+                                    int wmax_given, int numharm, float sigma, double flo,
+                                    double fhi, jerk_obs *obs, int *fftlen_out,
+                                    int *maxkernlen_out)
+{
+    if (!obs || numbins < 2 || dt <= 0.0)
+        return fail(JERK_EINVAL, "jerk_obs_from_params: bad arguments");
+    if (numharm != 1 && numharm != 2 && numharm != 4 && numharm != 8 && numharm != 16 &&
+        numharm != 32)
+        return fail(JERK_EINVAL, "numharm must be a power of two <= 32");
+    memset(obs, 0, sizeof(*obs));
+    if (zmax % kDZ)
+        zmax = (zmax / kDZ + 1) * kDZ;
+    const double T = dt * (double)N;
+    obs->numbins = numbins;
+    obs->lobin = 0;
+    int stages = 0;
+    while ((1 << stages) < numharm)
+        stages++;
+    obs->numharmstages = stages + 1;
+    obs->numz = (zmax / kDZ) * 2 + 1;
+    double whi = 0.0;
+    int numw = 0;
+    if (wmax_given) {
+        if (wmax % kDW)
+            wmax = (wmax / kDW + 1) * kDW;
+        whi = wmax;
+        numw = (wmax / kDW) * 2 + 1;
+        if (wmax == 0)
+            numw = 0;
+    } else {
+        wmax = 0;
+    }
+    obs->numw = numw;
+    obs->zlo = -zmax;
+    obs->wlo = -whi;
+    obs->rlo = floor(flo * T);
+    if (obs->rlo < obs->lobin)
+        obs->rlo = obs->lobin;
+    if (obs->rlo > numbins - 1)
+        return fail(JERK_EINVAL, "flo is above the highest frequency");
+    obs->highestbin = numbins - 1;
+    obs->highestbin = (long long)ceil(fhi * T);
+    if (obs->highestbin > numbins - 1)
+        obs->highestbin = numbins - 1;
+    const double rhi = (double)obs->highestbin;
+    if (obs->highestbin < obs->rlo)
+        return fail(JERK_EINVAL, "fhi is below flo");
+    const double dz = kDZ, dw = wmax_given ? kDW : 0.0;
+    for (int ii = 0; ii < obs->numharmstages; ii++) {
+        const int h = 1 << ii;
+        if (obs->numz == 1 && obs->numw == 0)
+            obs->numindep[ii] = (long long)((rhi - obs->rlo) / h);
+        else if (obs->numz > 1 && obs->numw == 0)
+            obs->numindep[ii] = (long long)((rhi - obs->rlo) * (obs->numz + 1) * (dz / 6.95) / h);
+        else
+            obs->numindep[ii] = (long long)((rhi - obs->rlo) * (obs->numz + 1) * (dz / 6.95) *
+                                            (obs->numw + 1) * (dw / 44.2) / h);
+        obs->powcut[ii] = (float)jerk_power_for_sigma(sigma, h, (double)obs->numindep[ii]);
+    }
+    const int maxkernlen = 2 * 2 * w_resp_halfwidth(zmax, whi);
+    int fftlen = fftlen_from_kernwidth(maxkernlen);
+    if (fftlen < 2048)
+        fftlen = 2048;
+    int uselen = fftlen - maxkernlen;
+    if (uselen % kRDR)
+        uselen = uselen / kRDR * kRDR;
+    obs->corr_uselen = uselen;
+    if (fftlen_out)
+        *fftlen_out = fftlen;
+    if (maxkernlen_out)
+        *maxkernlen_out = maxkernlen;
+    return JERK_OK;
+}
+
+extern "C" int jerk_subharm_count(int numharmstages)
+{
+    return numharmstages < 1 ? 0 : (1 << (numharmstages - 1));
+}
+
+// Bank order (src/accel_utils.c:236-282): (1/1), (1/2), (1/4), (3/4), (1/8), ...
+static void index_to_harm(int index, int *numharm, int *harmnum)
+{
+    if (index == 0) {
+        *numharm = 1;
+        *harmnum = 1;
+        return;
+    }
+    int stage = 1;
+    while (index >= (1 << stage))
+        stage++;
+    // stage s holds subharmonics 2^(s-1) .. 2^s - 1, harm = 2*(index - 2^(s-1)) + 1
+    *numharm = 1 << stage;
+    *harmnum = 2 * (index - (1 << (stage - 1))) + 1;
+}
+
+extern "C" int jerk_subharm_sizes(const jerk_obs *obs, int fftlen, int index, jerk_subharm *out)
+{
+    if (!obs || !out || index < 0 || index >= jerk_subharm_count(obs->numharmstages))
+        return fail(JERK_EINVAL, "jerk_subharm_sizes: bad index");
+    int nh, hn;
+    index_to_harm(index, &nh, &hn);
+    const double hf = (double)hn / (double)nh;
+    const int zmax = (int)-obs->zlo, wmax = (int)-obs->wlo;
+    memset(out, 0, sizeof(*out));
+    out->numharm = nh;
+    out->harmnum = hn;
+    out->zmax = calc_required_z(hf, zmax);
+    out->wmax = calc_required_w(hf, wmax);
+    out->numz = (out->zmax / kDZ) * 2 + 1;
+    out->numw = (out->wmax / kDW) * 2 + 1;
+    if (nh == 1 && hn == 1) {
+        out->fftlen = fftlen;
+    } else {
+        const int bins_needed = (int)ceil(obs->corr_uselen * hf) + 2;
+        const int end_effects = 2 * 2 * w_resp_halfwidth(calc_required_z(hf, zmax),
+                                                         calc_required_w(hf, wmax));
+        out->fftlen = next_good_fftlen(bins_needed + end_effects);
+    }
+    out->halfwidth = w_resp_halfwidth((double)-out->zmax, (double)-out->wmax);
+    out->kernels = nullptr;
+    return JERK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Candidate list: insert_new_accelcand (src/accel_utils.c:382-480).
+//
+// The reference walks a linked list from its head to the first node with
+// r >= rr (or to the last node).  The list is not always sorted -- when the
+// walk ends at the last node and only the node before it is overwritten, a
+// larger r lands before a smaller one -- so the walk cannot be replaced by a
+// binary search.  CandList keeps the list in blocks with each block's max r:
+// "first node with r >= rr" skips whole blocks whose max is below rr, which
+// gives the walk's exact answer in O(sqrt n) instead of O(n).
+
+namespace {
+
+class CandList {
+  public:
+    struct Pos {
+        size_t b, o;
+    };
+
+    bool empty() const { return n_ == 0; }
+    size_t size() const { return n_; }
+
+    // the reference walk's stopping node
+    Pos walk(double rr) const
+    {
+        for (size_t b = 0; b < blocks_.size(); b++) {
+            if (blocks_[b].maxr >= rr) {
+                const auto &v = blocks_[b].v;
+                for (size_t o = 0; o < v.size(); o++)
+                    if (!(v[o].r < rr))
+                        return {b, o};
+            }
+        }
+        return last();
+    }
+    Pos last() const { return {blocks_.size() - 1, blocks_.back().v.size() - 1}; }
+    bool is_last(Pos p) const { return p.b == blocks_.size() - 1 && p.o == blocks_[p.b].v.size() - 1; }
+    bool has_prev(Pos p) const { return p.o > 0 || p.b > 0; }
+    Pos prev(Pos p) const { return p.o > 0 ? Pos{p.b, p.o - 1} : Pos{p.b - 1, blocks_[p.b - 1].v.size() - 1}; }
+    const jerk_cand &at(Pos p) const { return blocks_[p.b].v[p.o]; }
+
+    void push_back(const jerk_cand &c)
+    {
+        if (blocks_.empty() || blocks_.back().v.size() >= 2 * kBlock)
+            blocks_.push_back(Block{});
+        Block &B = blocks_.back();
+        B.v.push_back(c);
+        B.maxr = B.v.size() == 1 ? c.r : std::max(B.maxr, c.r);
+        n_++;
+    }
+    void replace(Pos p, const jerk_cand &c)
+    {
+        Block &B = blocks_[p.b];
+        B.v[p.o] = c;
+        remax(B);
+    }
+    void insert_before(Pos p, const jerk_cand &c)
+    {
+        Block &B = blocks_[p.b];
+        B.v.insert(B.v.begin() + p.o, c);
+        B.maxr = std::max(B.maxr, c.r);
+        n_++;
+        if (B.v.size() > 2 * kBlock)
+            split(p.b);
+    }
+    void erase(Pos p)
+    {
+        Block &B = blocks_[p.b];
+        B.v.erase(B.v.begin() + p.o);
+        n_--;
+        if (B.v.empty())
+            blocks_.erase(blocks_.begin() + p.b);
+        else
+            remax(B);
+    }
+    void export_to(std::vector<jerk_cand> &out) const
+    {
+        out.clear();
+        out.reserve(n_);
+        for (const auto &B : blocks_)
+            out.insert(out.end(), B.v.begin(), B.v.end());
+    }
+
+  private:
+    static constexpr size_t kBlock = 256;
+    struct Block {
+        std::vector<jerk_cand> v;
+        double maxr = -INFINITY;
+    };
+    static void remax(Block &B)
+    {
+        double m = -INFINITY;
+        for (const auto &c : B.v)
+            m = std::max(m, c.r);
+        B.maxr = m;
+    }
+    void split(size_t b)
+    {
+        Block nb;
+        Block &B = blocks_[b];
+        nb.v.assign(B.v.begin() + kBlock, B.v.end());
+        B.v.resize(kBlock);
+        remax(B);
+        remax(nb);
+        blocks_.insert(blocks_.begin() + b + 1, std::move(nb));
+    }
+    std::vector<Block> blocks_;
+    size_t n_ = 0;
+};
+
+bool insert_cand(CandList &L, const jerk_cand &v)
+{
+    if (L.empty()) {
+        L.push_back(v);
+        return true;
+    }
+    const CandList::Pos tmp = L.walk(v.r);
+    const bool have_prev = L.has_prev(tmp);
+    const double next_diff = fabs(v.r - L.at(tmp).r);
+    const double prev_diff = have_prev ? fabs(v.r - L.at(L.prev(tmp)).r) : kClosestR + 1.0;
+    bool added = false;
+    if (prev_diff < kClosestR) {
+        const CandList::Pos prev = L.prev(tmp);
+        if (L.at(prev).sigma < v.sigma) {
+            L.replace(prev, v);
+            added = true;
+        }
+        if (next_diff < kClosestR && L.at(tmp).sigma < v.sigma) {
+            if (added)
+                L.erase(tmp);
+            else {
+                L.replace(tmp, v);
+                added = true;
+            }
+        }
+    } else if (next_diff < kClosestR) {
+        if (L.at(tmp).sigma < v.sigma) {
+            L.replace(tmp, v);
+            added = true;
+        }
+    } else {
+        added = true;
+        if (L.is_last(tmp) && L.at(tmp).r < v.r - kClosestR)
+            L.push_back(v);
+        else
+            L.insert_before(tmp, v);
+    }
+    return added;
+}
+
+long long export_list(const CandList &CL, jerk_cand **out)
+{
+    std::vector<jerk_cand> L;
+    CL.export_to(L);
+    if (!out)
+        return (long long)L.size();
+    *out = (jerk_cand *)malloc(sizeof(jerk_cand) * (L.size() ? L.size() : 1));
+    if (!*out)
+        return -1;
+    if (!L.empty())
+        memcpy(*out, L.data(), sizeof(jerk_cand) * L.size());
+    return (long long)L.size();
+}
+
+}  // namespace
+
+extern "C" long long jerk_insert_hits(const jerk_cand *hits, long long nhits, jerk_cand **cands)
+{
+    CandList L;
+    for (long long i = 0; i < nhits; i++)
+        insert_cand(L, hits[i]);
+    return export_list(L, cands);
+}
+
+// ---------------------------------------------------------------------------
+// The plan
+
+struct jerk_plan {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    jerk_obs obs{};
+    int nsubs = 0, maxfft = 0, batch = 8;
+    int zlo0 = 0, wlo0 = 0;
+    long long nrsteps = 0;
+    std::vector<jerk_subharm> subs;
+    std::vector<SubDev> hsubs;
+    std::vector<StepDev> hsteps;  // [nrsteps][nsubs]
+    std::map<int, std::vector<int>> groups;  // fftlen -> subs
+    // device
+    float2 *d_bank = nullptr;
+    bool own_bank = false;
+    float2 *d_tw = nullptr;
+    SubDev *d_subs = nullptr;
+    StepDev *d_steps = nullptr;
+    uint16_t *d_zinds = nullptr;
+    int *d_wind = nullptr;
+    float2 *d_prepped = nullptr;
+    float *d_planes = nullptr;
+    uint16_t *d_rinds = nullptr;
+    float2 *d_spec = nullptr;
+    long long spec_cap = 0;
+    unsigned long long *d_hit_keys = nullptr;
+    float *d_hit_pows = nullptr;
+    unsigned int *d_hit_count = nullptr;
+    unsigned int *d_status = nullptr;
+    long long max_hits = 0;
+    long long plane_floats = 0, prepped_f2 = 0;
+};
+
+static void plan_free_device(jerk_plan *p)
+{
+    if (p->own_bank)
+        cudaFree(p->d_bank);
+    cudaFree(p->d_tw);
+    cudaFree(p->d_subs);
+    cudaFree(p->d_steps);
+    cudaFree(p->d_zinds);
+    cudaFree(p->d_wind);
+    cudaFree(p->d_prepped);
+    cudaFree(p->d_planes);
+    cudaFree(p->d_rinds);
+    cudaFree(p->d_spec);
+    cudaFree(p->d_hit_keys);
+    cudaFree(p->d_hit_pows);
+    cudaFree(p->d_hit_count);
+    cudaFree(p->d_status);
+}
+
+extern "C" void jerk_plan_destroy(jerk_plan *p)
+{
+    if (!p)
+        return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(p->device);
+    if (p->stream)
+        cudaStreamSynchronize(p->stream);
+    plan_free_device(p);
+    if (p->own_stream && p->stream)
+        cudaStreamDestroy(p->stream);
+    cudaSetDevice(cur);
+    delete p;
+}
+
+static int alloc_hits(jerk_plan *p, long long cap)
+{
+    cudaFree(p->d_hit_keys);
+    cudaFree(p->d_hit_pows);
+    p->d_hit_keys = nullptr;
+    p->d_hit_pows = nullptr;
+    JERK_CUDA(cudaMalloc(&p->d_hit_keys, sizeof(unsigned long long) * cap));
+    JERK_CUDA(cudaMalloc(&p->d_hit_pows, sizeof(float) * cap));
+    p->max_hits = cap;
+    return JERK_OK;
+}
+
+static long long count_rsteps(const jerk_obs &o)
+{
+    const int rstep = (int)(o.corr_uselen * kDR);
+    long long n = 0;
+    double startr = o.rlo;
+    while (startr + rstep < (double)o.highestbin) {
+        n++;
+        startr += rstep;
+    }
+    return n;
+}
+
+extern "C" long long jerk_num_rsteps(const jerk_plan *p) { return p ? p->nrsteps : 0; }
+
+extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk_subharm *subs,
+                                int nsubs, const jerk_config *cfg)
+{
+    if (!out || !obs || !subs)
+        return fail(JERK_EINVAL, "jerk_plan_create: null argument");
+    *out = nullptr;
+    if (obs->numharmstages < 1 || obs->numharmstages > kMaxStages ||
+        nsubs != jerk_subharm_count(obs->numharmstages))
+        return fail(JERK_EINVAL, "jerk_plan_create: nsubs does not match numharmstages");
+    if (obs->norm_type != 0 && !(obs->nph > 0.0f))
+        return fail(JERK_EUNSUPPORTED, "only block-median or photon normalisation is supported");
+    if (obs->corr_uselen <= 0 || obs->corr_uselen % 2 || obs->corr_uselen > 65535)
+        return fail(JERK_EINVAL, "bad corr_uselen");
+
+    jerk_plan *p = new jerk_plan();
+    cudaGetDevice(&p->device);
+    p->obs = *obs;
+    p->nsubs = nsubs;
+    p->subs.assign(subs, subs + nsubs);
+    p->batch = (cfg && cfg->batch_rsteps > 0) ? cfg->batch_rsteps : 8;
+    const long long want_hits = (cfg && cfg->max_hits > 0) ? cfg->max_hits : (1LL << 22);
+    if (cfg && cfg->stream) {
+        p->stream = (cudaStream_t)cfg->stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete p;
+            return cuda_fail(e, "cudaStreamCreate");
+        }
+        p->own_stream = true;
+    }
+    auto bail = [&](int code) {
+        jerk_plan_destroy(p);
+        return code;
+    };
+
+    const jerk_subharm &f = subs[0];
+    if (f.numharm != 1 || f.harmnum != 1 || f.numz != obs->numz)
+        return bail(fail(JERK_EINVAL, "subharmonic 0 must be the fundamental (1/1)"));
+    p->zlo0 = calc_required_z(1.0, obs->zlo);
+    p->wlo0 = calc_required_w(1.0, obs->wlo);
+    p->nrsteps = count_rsteps(*obs);
+
+    // steps: rlo / numrs of every (rstep, subharmonic)
+    p->hsteps.resize((size_t)p->nrsteps * nsubs);
+    std::vector<int> maxnumrs(nsubs, 0);
+    const int rstep = (int)(obs->corr_uselen * kDR);
+    for (long long k = 0; k < p->nrsteps; k++) {
+        const double startr = obs->rlo + (double)k * rstep;
+        const double lastr = startr + rstep - kDR;
+        for (int s = 0; s < nsubs; s++) {
+            const double hf = (double)subs[s].harmnum / (double)subs[s].numharm;
+            const double drlo = calc_required_r(hf, startr), drhi = calc_required_r(hf, lastr);
+            StepDev &st = p->hsteps[(size_t)k * nsubs + s];
+            st.rlo = (long long)floor(drlo);
+            st.fullrlo = startr;
+            int numrs = (int)((ceil(drhi) - floor(drlo)) * kRDR + kDblCorrect) + 1;
+            if (s == 0)
+                numrs = obs->corr_uselen;
+            else if (numrs % kRDR)
+                numrs = (numrs / kRDR + 1) * kRDR;
+            st.numrs = numrs;
+            st.pad = 0;
+            maxnumrs[s] = std::max(maxnumrs[s], numrs);
+        }
+    }
+
+    // subharmonic layout
+    p->hsubs.resize(nsubs);
+    long long kern_off = 0, plane_off = 0, data_off = 0;
+    int zinds_off = 0, wind_off = 0;
+    std::vector<uint16_t> zinds;
+    std::vector<int> wind;
+    std::map<int, int> twoff;
+    int twtotal = 0;
+    for (int s = 0; s < nsubs; s++) {
+        const jerk_subharm &sh = subs[s];
+        if (!fftlen_supported(sh.fftlen))
+            return bail(fail(JERK_EUNSUPPORTED, "unsupported fftlen " + std::to_string(sh.fftlen)));
+        if (maxnumrs[s] + 2 * sh.halfwidth > sh.fftlen)
+            return bail(fail(JERK_EINVAL, "fftlen too short for the good bins"));
+        SubDev &d = p->hsubs[s];
+        d.numharm = sh.numharm;
+        d.harmnum = sh.harmnum;
+        d.harm_fract = (double)sh.harmnum / (double)sh.numharm;
+        d.numz = sh.numz;
+        d.numw = sh.numw;
+        d.fftlen = sh.fftlen;
+        d.halfwidth = sh.halfwidth;
+        d.stride = (maxnumrs[s] + 3) & ~3;
+        d.zlo = calc_required_z(d.harm_fract, obs->zlo);
+        d.wlo = calc_required_w(d.harm_fract, obs->wlo);
+        d.pownorm = (float)(1.0 / (double)(sh.fftlen * sh.fftlen));
+        if (!twoff.count(sh.fftlen)) {
+            twoff[sh.fftlen] = twtotal;
+            twtotal += sh.fftlen;
+        }
+        d.twoff = twoff[sh.fftlen];
+        d.kern_off = kern_off;
+        kern_off += (long long)sh.numw * sh.numz * sh.fftlen;
+        d.plane_size = (long long)sh.numw * sh.numz * d.stride;
+        d.plane_off = plane_off;
+        plane_off += d.plane_size * p->batch;
+        d.data_off = data_off;
+        data_off += (long long)sh.fftlen * p->batch;
+        d.zinds_off = zinds_off;
+        d.wind_off = wind_off;
+        // zinds (src/accel_utils.c:1124-1130) and wind (src/accel_utils.c:1362-1364)
+        for (int ii = 0; ii < obs->numz; ii++) {
+            const double zz = obs->zlo + ii * kDZ;
+            const int subz = calc_required_z(d.harm_fract, zz);
+            const int zi = index_from_z(subz, d.zlo);
+            if (s > 0 && (zi < 0 || zi >= sh.numz))
+                return bail(fail(JERK_EINVAL, "zinds out of range"));
+            zinds.push_back((uint16_t)zi);
+        }
+        for (int ii = 0; ii < subs[0].numw; ii++) {
+            const int ww = p->wlo0 + ii * kDW;
+            const int subw = calc_required_w(d.harm_fract, ww);
+            const int wi = index_from_w(subw, d.wlo);
+            if (s > 0 && (wi < 0 || wi >= sh.numw))
+                return bail(fail(JERK_EINVAL, "wind out of range"));
+            wind.push_back(wi);
+        }
+        zinds_off += obs->numz;
+        wind_off += subs[0].numw;
+        p->maxfft = std::max(p->maxfft, sh.fftlen);
+        p->groups[sh.fftlen].push_back(s);
+    }
+    p->plane_floats = plane_off;
+    p->prepped_f2 = data_off;
+
+    // twiddles: exp(-2 pi i m / N), double on the host
+    std::vector<float2> tw(twtotal);
+    for (auto &kv : twoff) {
+        const int N = kv.first;
+        for (int m = 0; m < N; m++) {
+            const double a = -2.0 * M_PI * (double)m / (double)N;
+            tw[kv.second + m] = make_float2((float)cos(a), (float)sin(a));
+        }
+    }
+
+#define JERK_CUDA_B(call)                                \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess)                           \
+            return bail(cuda_fail(e_, #call));           \
+    } while (0)
+
+    // kernel bank
+    if (cfg && cfg->device_bank) {
+        p->d_bank = (float2 *)cfg->device_bank;
+        p->own_bank = false;
+    } else {
+        JERK_CUDA_B(cudaMalloc(&p->d_bank, sizeof(float2) * kern_off));
+        p->own_bank = true;
+        for (int s = 0; s < nsubs; s++) {
+            if (!subs[s].kernels)
+                return bail(fail(JERK_EINVAL, "subharmonic without kernels and no device bank"));
+            const size_t n = (size_t)subs[s].numw * subs[s].numz * subs[s].fftlen;
+            JERK_CUDA_B(cudaMemcpyAsync(p->d_bank + p->hsubs[s].kern_off, subs[s].kernels,
+                                        sizeof(float2) * n, cudaMemcpyHostToDevice, p->stream));
+        }
+    }
+    JERK_CUDA_B(cudaMalloc(&p->d_tw, sizeof(float2) * twtotal));
+    JERK_CUDA_B(cudaMemcpyAsync(p->d_tw, tw.data(), sizeof(float2) * twtotal,
+                                cudaMemcpyHostToDevice, p->stream));
+    JERK_CUDA_B(cudaMalloc(&p->d_subs, sizeof(SubDev) * nsubs));
+    JERK_CUDA_B(cudaMemcpyAsync(p->d_subs, p->hsubs.data(), sizeof(SubDev) * nsubs,
+                                cudaMemcpyHostToDevice, p->stream));
+    if (p->nrsteps > 0) {
+        JERK_CUDA_B(cudaMalloc(&p->d_steps, sizeof(StepDev) * p->hsteps.size()));
+        JERK_CUDA_B(cudaMemcpyAsync(p->d_steps, p->hsteps.data(),
+                                    sizeof(StepDev) * p->hsteps.size(), cudaMemcpyHostToDevice,
+                                    p->stream));
+    }
+    JERK_CUDA_B(cudaMalloc(&p->d_zinds, sizeof(uint16_t) * zinds.size()));
+    JERK_CUDA_B(cudaMemcpyAsync(p->d_zinds, zinds.data(), sizeof(uint16_t) * zinds.size(),
+                                cudaMemcpyHostToDevice, p->stream));
+    JERK_CUDA_B(cudaMalloc(&p->d_wind, sizeof(int) * wind.size()));
+    JERK_CUDA_B(cudaMemcpyAsync(p->d_wind, wind.data(), sizeof(int) * wind.size(),
+                                cudaMemcpyHostToDevice, p->stream));
+    JERK_CUDA_B(cudaMalloc(&p->d_prepped, sizeof(float2) * p->prepped_f2));
+    JERK_CUDA_B(cudaMalloc(&p->d_planes, sizeof(float) * p->plane_floats));
+    JERK_CUDA_B(cudaMalloc(&p->d_rinds, sizeof(uint16_t) * (size_t)p->batch * nsubs *
+                                            obs->corr_uselen));
+    JERK_CUDA_B(cudaMalloc(&p->d_hit_count, sizeof(unsigned int)));
+    JERK_CUDA_B(cudaMalloc(&p->d_status, sizeof(unsigned int)));
+    JERK_CUDA_B(cudaMemsetAsync(p->d_status, 0, sizeof(unsigned int), p->stream));
+    {
+        int rc = alloc_hits(p, want_hits);
+        if (rc != JERK_OK)
+            return bail(rc);
+    }
+    JERK_CUDA_B(cudaStreamSynchronize(p->stream));
+#undef JERK_CUDA_B
+    *out = p;
+    return JERK_OK;
+}
+
+static int stage_spectrum(jerk_plan *p, const void *spectrum, int on_device, const float2 **spec)
+{
+    if (on_device) {
+        *spec = (const float2 *)spectrum;
+        return JERK_OK;
+    }
+    if (p->spec_cap < p->obs.numbins) {
+        cudaFree(p->d_spec);
+        p->d_spec = nullptr;
+        JERK_CUDA(cudaMalloc(&p->d_spec, sizeof(float2) * p->obs.numbins));
+        p->spec_cap = p->obs.numbins;
+    }
+    JERK_CUDA(cudaMemcpyAsync(p->d_spec, spectrum, sizeof(float2) * p->obs.numbins,
+                              cudaMemcpyHostToDevice, p->stream));
+    *spec = p->d_spec;
+    return JERK_OK;
+}
+
+static SearchDev make_args(const jerk_plan *p, const float2 *spec)
+{
+    SearchDev a{};
+    a.spec = spec;
+    a.numbins = p->obs.numbins;
+    a.lobin = p->obs.lobin;
+    a.nsubs = p->nsubs;
+    a.nstages = p->obs.numharmstages;
+    a.corr_uselen = p->obs.corr_uselen;
+    a.numz0 = p->subs[0].numz;
+    a.numw0 = p->subs[0].numw;
+    a.norm_type = p->obs.norm_type;
+    a.nph = p->obs.nph;
+    for (int i = 0; i < kMaxStages; i++)
+        a.powcut[i] = i < p->obs.numharmstages ? p->obs.powcut[i] : INFINITY;
+    a.subs = p->d_subs;
+    a.steps = p->d_steps;
+    a.bank = p->d_bank;
+    a.twiddles = p->d_tw;
+    a.zinds = p->d_zinds;
+    a.wind = p->d_wind;
+    a.prepped = p->d_prepped;
+    a.planes = p->d_planes;
+    a.rinds = p->d_rinds;
+    a.hit_keys = p->d_hit_keys;
+    a.hit_pows = p->d_hit_pows;
+    a.hit_count = p->d_hit_count;
+    a.max_hits = p->max_hits;
+    a.status = p->d_status;
+    return a;
+}
+
+// prep + correlation for one batch (volumes only)
+static int run_volumes(jerk_plan *p, SearchDev &a)
+{
+    cudaError_t e = launch_prep(a, p->maxfft, p->stream);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "prep_kernel");
+    for (auto &kv : p->groups) {
+        RowGroup G{};
+        G.n = (int)kv.second.size();
+        int rows = 0;
+        for (int i = 0; i < G.n; i++) {
+            const int s = kv.second[i];
+            G.sub[i] = s;
+            G.rowstart[i] = rows;
+            rows += p->subs[s].numw * p->subs[s].numz;
+        }
+        G.rowstart[G.n] = rows;
+        e = launch_corr(a, kv.first, G, rows, p->stream);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "corr_kernel");
+    }
+    return JERK_OK;
+}
+
+static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, long long count,
+                           unsigned int *nhits_out)
+{
+    unsigned int status = 0;
+    SearchDev a = make_args(p, spec);
+    JERK_CUDA(cudaMemsetAsync(p->d_hit_count, 0, sizeof(unsigned int), p->stream));
+    for (long long k = first; k < first + count; k += p->batch) {
+        a.first_rstep = k;
+        a.nb = (int)std::min<long long>(p->batch, first + count - k);
+        int rc = run_volumes(p, a);
+        if (rc != JERK_OK)
+            return rc;
+        cudaError_t e = launch_harmsum(a, p->stream);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "harmsum_kernel");
+    }
+    JERK_CUDA(cudaMemcpyAsync(nhits_out, p->d_hit_count, sizeof(unsigned int),
+                              cudaMemcpyDeviceToHost, p->stream));
+    JERK_CUDA(cudaMemcpyAsync(&status, p->d_status, sizeof(unsigned int),
+                              cudaMemcpyDeviceToHost, p->stream));
+    JERK_CUDA(cudaStreamSynchronize(p->stream));
+    if (status)
+        return fail(JERK_EINVAL, "harmonic sum: a subharmonic r index left its row");
+    return JERK_OK;
+}
+
+extern "C" int jerk_search(jerk_plan *p, const void *spectrum, int spectrum_on_device,
+                           long long first_rstep, long long num_rsteps, jerk_cand **cands,
+                           long long *ncands, jerk_hits *hits)
+{
+    if (!p || !spectrum)
+        return fail(JERK_EINVAL, "jerk_search: null argument");
+    if (first_rstep < 0 || first_rstep > p->nrsteps)
+        return fail(JERK_EINVAL, "jerk_search: first_rstep out of range");
+    long long count = p->nrsteps - first_rstep;
+    if (num_rsteps > 0 && num_rsteps < count)
+        count = num_rsteps;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p->device)
+        JERK_CUDA(cudaSetDevice(p->device));
+    const float2 *spec = nullptr;
+    int rc = stage_spectrum(p, spectrum, spectrum_on_device, &spec);
+    if (rc != JERK_OK)
+        return rc;
+
+    unsigned int nh = 0;
+    for (int attempt = 0;; attempt++) {
+        rc = run_search_pass(p, spec, first_rstep, count, &nh);
+        if (rc != JERK_OK)
+            return rc;
+        if ((long long)nh <= p->max_hits)
+            break;
+        // overflow: the counter kept counting, so one retry with the exact
+        // size always suffices
+        if (attempt > 2)
+            return fail(JERK_OVERFLOW, "hit buffer overflow persisted");
+        rc = alloc_hits(p, (long long)nh + (nh >> 3) + 1024);
+        if (rc != JERK_OK)
+            return rc;
+    }
+
+    // hits back, in the reference's insertion order
+    std::vector<unsigned long long> keys(nh);
+    std::vector<float> pows(nh);
+    if (nh) {
+        JERK_CUDA(cudaMemcpyAsync(keys.data(), p->d_hit_keys, sizeof(unsigned long long) * nh,
+                                  cudaMemcpyDeviceToHost, p->stream));
+        JERK_CUDA(cudaMemcpyAsync(pows.data(), p->d_hit_pows, sizeof(float) * nh,
+                                  cudaMemcpyDeviceToHost, p->stream));
+        JERK_CUDA(cudaStreamSynchronize(p->stream));
+    }
+    std::vector<uint32_t> order(nh);
+    for (uint32_t i = 0; i < nh; i++)
+        order[i] = i;
+    std::sort(order.begin(), order.end(),
+              [&](uint32_t x, uint32_t y) { return keys[x] < keys[y]; });
+
+    const int S = p->obs.numharmstages;
+    const long long numrs0 = p->obs.corr_uselen, numz0 = p->subs[0].numz,
+                    numw0 = p->subs[0].numw;
+    CandList L;
+    for (uint32_t i = 0; i < nh; i++) {
+        unsigned long long key = keys[order[i]];
+        const int kk = (int)(key % numrs0);
+        key /= numrs0;
+        const int jj = (int)(key % numz0);
+        key /= numz0;
+        const int ii = (int)(key % numw0);
+        key /= numw0;
+        const int stage = (int)(key % S);
+        const long long rs = (long long)(key / S);
+        const int nhm = 1 << stage;
+        jerk_cand c;
+        c.power = pows[order[i]];
+        c.sigma = (float)jerk_candidate_sigma(c.power, nhm, (double)p->obs.numindep[stage]);
+        c.numharm = nhm;
+        c.r = ((double)p->hsteps[(size_t)rs * p->nsubs].rlo + kk * kDR) / (double)nhm;
+        c.z = (p->zlo0 + jj * (double)kDZ) / (double)nhm;
+        c.w = (p->wlo0 + ii * (double)kDW) / (double)nhm;
+        insert_cand(L, c);
+    }
+    if (hits) {
+        hits->count = nh;
+        hits->keys = (unsigned long long *)malloc(sizeof(unsigned long long) * (nh ? nh : 1));
+        hits->powers = (float *)malloc(sizeof(float) * (nh ? nh : 1));
+        for (uint32_t i = 0; i < nh; i++) {
+            hits->keys[i] = keys[order[i]];
+            hits->powers[i] = pows[order[i]];
+        }
+    }
+    const long long n = export_list(L, cands);
+    if (n < 0)
+        return fail(JERK_ENOMEM, "candidate list allocation");
+    if (ncands)
+        *ncands = n;
+    return JERK_OK;
+}
+
+extern "C" int jerk_debug_volume(jerk_plan *p, const void *spectrum, int spectrum_on_device,
+                                 long long rstep, int sub, float *out, int *numrs, long long *rlo)
+{
+    if (!p || !spectrum || !out || sub < 0 || sub >= p->nsubs || rstep < 0 ||
+        rstep >= p->nrsteps)
+        return fail(JERK_EINVAL, "jerk_debug_volume: bad argument");
+    const float2 *spec = nullptr;
+    int rc = stage_spectrum(p, spectrum, spectrum_on_device, &spec);
+    if (rc != JERK_OK)
+        return rc;
+    SearchDev a = make_args(p, spec);
+    a.first_rstep = rstep;
+    a.nb = 1;
+    rc = run_volumes(p, a);
+    if (rc != JERK_OK)
+        return rc;
+    const SubDev &d = p->hsubs[sub];
+    const StepDev &st = p->hsteps[(size_t)rstep * p->nsubs + sub];
+    JERK_CUDA(cudaMemcpy2DAsync(out, sizeof(float) * st.numrs, p->d_planes + d.plane_off,
+                                sizeof(float) * d.stride, sizeof(float) * st.numrs,
+                                (size_t)d.numw * d.numz, cudaMemcpyDeviceToHost, p->stream));
+    JERK_CUDA(cudaStreamSynchronize(p->stream));
+    if (numrs)
+        *numrs = st.numrs;
+    if (rlo)
+        *rlo = st.rlo;
+    return JERK_OK;
+}

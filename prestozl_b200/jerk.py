@@ -1,0 +1,272 @@
+"""Python mirror of libjerk's C ABI (``include/jerk.h``), through ctypes.
+
+This is the host-side interface the tests and the benchmark use; C callers
+link ``prestozl_b200/lib/libjerk.so`` directly.  There is no fallback: if the
+CUDA library is missing, every entry point raises.
+
+Names follow the reference (``accelobs`` -> ``Obs``, ``subharminfo`` ->
+``Subharm``, ``accelcand`` -> ``Cand``; ``include/accel.h`` in PrestoZL).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libjerk.so")
+
+JERK_OK = 0
+JERK_OVERFLOW = 1
+JERK_TIMEOUT = 2
+JERK_EINVAL = -1
+JERK_ECUDA = -2
+JERK_ENOMEM = -3
+JERK_EUNSUPPORTED = -4
+
+MAX_STAGES = 6
+
+
+class JerkError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libjerk error {code}: {msg}")
+        self.code = code
+
+
+class Obs(C.Structure):
+    """jerk_obs: the search geometry (accelobs fields the loop reads)."""
+    _fields_ = [
+        ("numbins", C.c_longlong), ("lobin", C.c_longlong), ("highestbin", C.c_longlong),
+        ("rlo", C.c_double), ("zlo", C.c_double), ("wlo", C.c_double),
+        ("corr_uselen", C.c_int), ("numz", C.c_int), ("numw", C.c_int),
+        ("numharmstages", C.c_int), ("norm_type", C.c_int), ("nph", C.c_float),
+        ("powcut", C.c_float * MAX_STAGES), ("numindep", C.c_longlong * MAX_STAGES),
+    ]
+
+
+class Subharm(C.Structure):
+    _fields_ = [("numharm", C.c_int), ("harmnum", C.c_int), ("zmax", C.c_int),
+                ("wmax", C.c_int), ("numz", C.c_int), ("numw", C.c_int),
+                ("fftlen", C.c_int), ("halfwidth", C.c_int), ("kernels", C.c_void_p)]
+
+
+class Cand(C.Structure):
+    _fields_ = [("power", C.c_float), ("sigma", C.c_float), ("numharm", C.c_int),
+                ("r", C.c_double), ("z", C.c_double), ("w", C.c_double)]
+
+
+class Config(C.Structure):
+    _fields_ = [("batch_rsteps", C.c_int), ("max_hits", C.c_longlong),
+                ("stream", C.c_void_p), ("device_bank", C.c_void_p)]
+
+
+class Hits(C.Structure):
+    _fields_ = [("count", C.c_longlong), ("keys", C.POINTER(C.c_ulonglong)),
+                ("powers", C.POINTER(C.c_float))]
+
+
+CAND_DTYPE = np.dtype([("power", np.float32), ("sigma", np.float32), ("numharm", np.int32),
+                       ("r", np.float64), ("z", np.float64), ("w", np.float64)], align=True)
+assert CAND_DTYPE.itemsize == C.sizeof(Cand)
+
+_lib = None
+
+EXPORTS = [
+    "jerk_obs_from_params", "jerk_subharm_count", "jerk_subharm_sizes", "jerk_plan_create",
+    "jerk_plan_destroy", "jerk_search", "jerk_num_rsteps", "jerk_debug_volume",
+    "jerk_candidate_sigma", "jerk_power_for_sigma", "jerk_insert_hits", "jerk_free",
+    "jerk_last_error",
+]
+
+
+def lib() -> C.CDLL:
+    """Load libjerk.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise JerkError(JERK_ECUDA, f"{LIB_PATH} is missing; run prestozl_b200.build.build()")
+    L = C.CDLL(LIB_PATH)
+    L.jerk_last_error.restype = C.c_char_p
+    L.jerk_obs_from_params.argtypes = [C.c_longlong, C.c_longlong, C.c_double, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, C.c_float, C.c_double, C.c_double,
+                                       C.POINTER(Obs), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.jerk_subharm_count.argtypes = [C.c_int]
+    L.jerk_subharm_sizes.argtypes = [C.POINTER(Obs), C.c_int, C.c_int, C.POINTER(Subharm)]
+    L.jerk_plan_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Obs), C.POINTER(Subharm),
+                                   C.c_int, C.POINTER(Config)]
+    L.jerk_plan_destroy.argtypes = [C.c_void_p]
+    L.jerk_plan_destroy.restype = None
+    L.jerk_search.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_longlong,
+                              C.POINTER(C.POINTER(Cand)), C.POINTER(C.c_longlong),
+                              C.POINTER(Hits)]
+    L.jerk_num_rsteps.argtypes = [C.c_void_p]
+    L.jerk_num_rsteps.restype = C.c_longlong
+    L.jerk_debug_volume.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int,
+                                    C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+    L.jerk_candidate_sigma.restype = C.c_double
+    L.jerk_candidate_sigma.argtypes = [C.c_double, C.c_int, C.c_double]
+    L.jerk_power_for_sigma.restype = C.c_double
+    L.jerk_power_for_sigma.argtypes = [C.c_double, C.c_int, C.c_double]
+    L.jerk_insert_hits.restype = C.c_longlong
+    L.jerk_insert_hits.argtypes = [C.POINTER(Cand), C.c_longlong, C.POINTER(C.POINTER(Cand))]
+    L.jerk_free.argtypes = [C.c_void_p]
+    L.jerk_free.restype = None
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != JERK_OK:
+        raise JerkError(rc, lib().jerk_last_error().decode())
+
+
+def obs_from_params(numbins: int, N: int, dt: float, zmax: int, wmax: int, numharm: int,
+                    sigma: float, flo: float = 1.0, fhi: float = 10000.0,
+                    wmax_given: bool = True) -> Tuple[Obs, int, int]:
+    """create_accelobs sizing with accelsearch's defaults (-flo 1 -fhi 10000)."""
+    o = Obs()
+    fftlen, mk = C.c_int(0), C.c_int(0)
+    _check(lib().jerk_obs_from_params(numbins, N, dt, zmax, wmax, int(wmax_given), numharm,
+                                      sigma, flo, fhi, C.byref(o), C.byref(fftlen), C.byref(mk)))
+    return o, fftlen.value, mk.value
+
+
+def subharm_sizes(obs: Obs, fftlen: int) -> List[dict]:
+    out = []
+    for i in range(lib().jerk_subharm_count(obs.numharmstages)):
+        s = Subharm()
+        _check(lib().jerk_subharm_sizes(C.byref(obs), fftlen, i, C.byref(s)))
+        out.append({k: getattr(s, k) for k, _ in Subharm._fields_ if k != "kernels"})
+    return out
+
+
+def candidate_sigma(power: float, numsum: int, numtrials: float) -> float:
+    return lib().jerk_candidate_sigma(power, numsum, numtrials)
+
+
+def power_for_sigma(sigma: float, numsum: int, numtrials: float) -> float:
+    return lib().jerk_power_for_sigma(sigma, numsum, numtrials)
+
+
+def insert_hits(hits: np.ndarray) -> np.ndarray:
+    hits = np.ascontiguousarray(hits, dtype=CAND_DTYPE)
+    out = C.POINTER(Cand)()
+    n = lib().jerk_insert_hits(hits.ctypes.data_as(C.POINTER(Cand)), len(hits), C.byref(out))
+    arr = np.ctypeslib.as_array(C.cast(out, C.POINTER(C.c_byte)), shape=(n * CAND_DTYPE.itemsize,))
+    res = np.frombuffer(arr.tobytes(), dtype=CAND_DTYPE).copy()
+    lib().jerk_free(out)
+    return res
+
+
+def _spectrum_arg(spectrum):
+    """(pointer, on_device, keepalive) for a numpy array or a CUDA tensor."""
+    if isinstance(spectrum, np.ndarray):
+        a = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        return C.c_void_p(a.ctypes.data), 0, a
+    # a torch tensor on the GPU (complex64 or float32 pairs)
+    if getattr(spectrum, "is_cuda", False):
+        return C.c_void_p(spectrum.data_ptr()), 1, spectrum
+    a = np.ascontiguousarray(np.asarray(spectrum), dtype=np.complex64)
+    return C.c_void_p(a.ctypes.data), 0, a
+
+
+class JerkPlan:
+    """A search plan on the current CUDA device (jerk_plan_create)."""
+
+    def __init__(self, obs: Obs, subs: Sequence[dict], batch: int = 8, max_hits: int = 0,
+                 stream: int = 0, device_bank: int = 0):
+        self.obs = obs
+        self._kerns = []
+        arr = (Subharm * len(subs))()
+        for i, s in enumerate(subs):
+            k = s.get("kern")
+            kp = None
+            if k is not None:
+                k = np.ascontiguousarray(k, dtype=np.complex64)
+                self._kerns.append(k)
+                kp = k.ctypes.data
+            arr[i] = Subharm(s["numharm"], s["harmnum"], s.get("zmax", 0), s.get("wmax", 0),
+                             s["numz"], s["numw"], s["fftlen"], s["halfwidth"], kp)
+        self.subs = arr
+        cfg = Config(batch, max_hits, stream or None, device_bank or None)
+        self._p = C.c_void_p()
+        _check(lib().jerk_plan_create(C.byref(self._p), C.byref(obs), arr, len(subs),
+                                      C.byref(cfg)))
+        self._kerns = []  # the bank is on the device now
+
+    @property
+    def num_rsteps(self) -> int:
+        return lib().jerk_num_rsteps(self._p)
+
+    def close(self) -> None:
+        if self._p:
+            lib().jerk_plan_destroy(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def search(self, spectrum, first_rstep: int = 0, num_rsteps: int = 0,
+               want_hits: bool = False):
+        """Candidates (CAND_DTYPE, list order) and optionally raw hits
+        (keys u64, powers f32) in the reference's insertion order."""
+        ptr, dev, keep = _spectrum_arg(spectrum)
+        out = C.POINTER(Cand)()
+        n = C.c_longlong(0)
+        hits = Hits()
+        _check(lib().jerk_search(self._p, ptr, dev, first_rstep, num_rsteps, C.byref(out),
+                                 C.byref(n), C.byref(hits) if want_hits else None))
+        nb = n.value * CAND_DTYPE.itemsize
+        cands = np.frombuffer(C.string_at(out, nb), dtype=CAND_DTYPE).copy() if nb else \
+            np.zeros(0, dtype=CAND_DTYPE)
+        lib().jerk_free(out)
+        if not want_hits:
+            return cands
+        k = np.ctypeslib.as_array(hits.keys, shape=(max(hits.count, 1),))[: hits.count].copy()
+        p = np.ctypeslib.as_array(hits.powers, shape=(max(hits.count, 1),))[: hits.count].copy()
+        lib().jerk_free(C.cast(hits.keys, C.c_void_p))
+        lib().jerk_free(C.cast(hits.powers, C.c_void_p))
+        return cands, k, p
+
+    def volume(self, spectrum, rstep: int, sub: int):
+        """ffdot volume [numw][numz][numrs] of one (rstep, subharmonic)."""
+        ptr, dev, keep = _spectrum_arg(spectrum)
+        s = self.subs[sub]
+        fftlen = s.fftlen
+        out = np.zeros(s.numw * s.numz * fftlen, dtype=np.float32)
+        numrs, rlo = C.c_int(0), C.c_longlong(0)
+        _check(lib().jerk_debug_volume(self._p, ptr, dev, rstep, sub, out.ctypes.data,
+                                       C.byref(numrs), C.byref(rlo)))
+        n = s.numw * s.numz * numrs.value
+        return out[:n].reshape(s.numw, s.numz, numrs.value), rlo.value
+
+    def decode(self, keys: np.ndarray):
+        """(rstep, stage, w index, z index, r index) of encoded hit keys."""
+        k = keys.astype(np.uint64)
+        numrs, numz, numw = self.obs.corr_uselen, self.subs[0].numz, self.subs[0].numw
+        S = self.obs.numharmstages
+        kk = k % numrs; k //= numrs
+        jj = k % numz; k //= numz
+        ii = k % numw; k //= numw
+        st = k % S; rs = k // S
+        return rs, st, ii, jj, kk
+
+
+def obs_from_refobs(ro) -> Obs:
+    """jerk_obs from the reference's accelobs summary (oracle bindings)."""
+    o = Obs()
+    o.numbins, o.lobin, o.highestbin = ro.numbins, ro.lobin, ro.highestbin
+    o.rlo, o.zlo, o.wlo = ro.rlo, ro.zlo, ro.wlo
+    o.corr_uselen, o.numz, o.numw = ro.corr_uselen, ro.numz, ro.numw
+    o.numharmstages, o.norm_type, o.nph = ro.numharmstages, ro.norm_type, ro.nph
+    for i in range(MAX_STAGES):
+        o.powcut[i] = ro.powcut[i]
+        o.numindep[i] = ro.numindep[i]
+    return o

@@ -1,0 +1,139 @@
+"""CUDA path vs the oracle and the reference's golden results, through the
+C ABI (libjerk.so).  Small spectrum: 2^20 samples with one binary pulsar,
+-zmax 20 -wmax 60 -numharm 8 -sigma 2.0 (546 rsteps).
+
+Tolerances (FP32 CUDA correlation against the oracle's FP64 one):
+  * ffdot powers: |gpu - oracle| <= 1e-5 * max(oracle, 1)  (normalised power)
+  * summed powers of hits and candidates: 1e-5 relative; sigma 1e-5 relative
+  * integer/index work (rlo, rinds, hit keys): exact, except hits whose power
+    lies within 1e-4 relative of their stage's cutoff
+"""
+
+import numpy as np
+import pytest
+
+from prestozl_b200 import build, jerk
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+POW_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def small(tmp_path_factory):
+    build.build()
+    H.ensure_oracle()
+    if not H.have_ref():
+        pytest.skip("the reference build (oracle/_ref) provides the kernel bank")
+    return H.small_problem(str(tmp_path_factory.mktemp("gpu_small")))
+
+
+@pytest.fixture(scope="module")
+def plan(small):
+    p = jerk.JerkPlan(jerk.obs_from_refobs(small.obs), small.subs, batch=8)
+    yield p
+    p.close()
+
+
+def test_plan_geometry(small, plan):
+    assert plan.num_rsteps == H.golden("small_cands.json")["nrsteps"]
+
+
+@pytest.mark.parametrize("which", ["first", "pulsar", "late", "last"])
+def test_volumes_match_oracle(small, plan, which):
+    k = {"first": 0, "pulsar": small.rstep_of(8281.0), "late": 540,
+         "last": plan.num_rsteps - 1}[which]
+    startr = small.startr(k)
+    lastr = startr + small.rstep - 0.5
+    worst = 0.0
+    for i in range(len(small.subs)):
+        got, rlo = plan.volume(small.spec, k, i)
+        h, want, _, _ = small.oracle.fderivs(i, startr, lastr)
+        assert rlo == h["rlo"]
+        assert got.shape == want.shape
+        err = np.abs(got.astype(np.float64) - want) / np.maximum(want, 1.0)
+        worst = max(worst, float(err.max()))
+        assert err.max() <= POW_TOL, (which, i, err.max())
+    print(f"max FP32 power error vs FP64 oracle ({which}): {worst:.3e}")
+
+
+def _oracle_hits(small, first, count):
+    _, _, keys, pows = small.oracle.search_hits(first, count)
+    return keys, pows
+
+
+def _compare_hits(small, gk, gp, ok, op):
+    powcut = np.array(list(small.obs.powcut))
+    S = small.obs.numharmstages
+    per = small.obs.corr_uselen * small.subs[0]["numz"] * small.subs[0]["numw"]
+    stage_of = lambda k: ((k // per) % S).astype(int)
+    gd = dict(zip(gk.tolist(), gp.tolist()))
+    od = dict(zip(ok.tolist(), op.tolist()))
+    near = lambda k, p: abs(p - powcut[stage_of(np.uint64(k))]) <= 1e-4 * powcut[stage_of(np.uint64(k))]
+    missing = [k for k in od if k not in gd and not near(k, od[k])]
+    extra = [k for k in gd if k not in od and not near(k, gd[k])]
+    assert not missing and not extra, (len(missing), len(extra))
+    common = [k for k in od if k in gd]
+    rel = max((abs(gd[k] - od[k]) / od[k] for k in common), default=0.0)
+    assert rel <= POW_TOL, rel
+    # insertion order (sorted keys) equals the oracle's order
+    assert np.all(np.diff(gk.astype(np.uint64)) > 0)
+    return len(common), rel
+
+
+def test_hits_match_oracle(small, plan):
+    first, count = 0, 48
+    cands, gk, gp = plan.search(small.spec, first, count, want_hits=True)
+    ok, op = _oracle_hits(small, first, count)
+    n, rel = _compare_hits(small, gk, gp, ok, op)
+    assert n > 1000
+    print(f"{n} hits, max summed-power rel error {rel:.3e}")
+
+
+def test_hits_around_pulsar_match_oracle(small, plan):
+    first = max(0, small.rstep_of(8281.0) - 4)
+    cands, gk, gp = plan.search(small.spec, first, 9, want_hits=True)
+    ok, op = _oracle_hits(small, first, 9)
+    _compare_hits(small, gk, gp, ok, op)
+
+
+def test_full_search_matches_reference_golden(small, plan):
+    g = H.golden("small_cands.json")
+    want = np.array([tuple(c) for c in g["cands"]], dtype=jerk.CAND_DTYPE)
+    got = plan.search(small.spec)
+    probs = H.compare_cands(got, want, g["obs"]["powcut"])
+    assert not probs, probs[:10]
+
+
+def test_batch_size_does_not_change_results(small):
+    obs = jerk.obs_from_refobs(small.obs)
+    res = []
+    for b in (1, 5, 8, 16):
+        p = jerk.JerkPlan(obs, small.subs, batch=b)
+        c, k, pw = p.search(small.spec, 100, 23, want_hits=True)
+        res.append((c, k, pw))
+        p.close()
+    for c, k, pw in res[1:]:
+        assert np.array_equal(k, res[0][1]) and np.array_equal(pw, res[0][2])
+        assert np.array_equal(c, res[0][0])
+
+
+def test_device_resident_spectrum(small, plan):
+    torch = pytest.importorskip("torch")
+    d = torch.from_numpy(small.spec.view(np.float32).copy()).cuda()
+    c1 = plan.search(small.spec, 200, 16)
+    c2 = plan.search(d, 200, 16)
+    torch.cuda.synchronize()
+    assert np.array_equal(c1, c2)
+
+
+def test_hit_buffer_overflow_is_recovered(small):
+    p = jerk.JerkPlan(jerk.obs_from_refobs(small.obs), small.subs, batch=8, max_hits=64)
+    c, k, pw = p.search(small.spec, 0, 30, want_hits=True)
+    p.close()
+    q = jerk.JerkPlan(jerk.obs_from_refobs(small.obs), small.subs, batch=8)
+    c2, k2, pw2 = q.search(small.spec, 0, 30, want_hits=True)
+    q.close()
+    assert len(k) > 64
+    assert np.array_equal(k, k2) and np.array_equal(c, c2)

@@ -1,0 +1,157 @@
+"""The oracle pinned against the reference itself (CPU only).
+
+The reference's CPU accelsearch is compiled from its sources into
+oracle/_ref (oracle/Makefile).  Where it is present these tests compare the
+oracle's restatement with it directly; the golden fixtures (made by
+tests/golden/make_golden.py from the same build) pin it everywhere.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import bindings as ob
+from prestozl_b200 import synth
+from tests import helpers as H
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _build():
+    H.ensure_oracle()
+
+
+def test_sizing_matches_reference_golden():
+    L = ob.orclib()
+    for e in H.golden("sizing.json"):
+        o = e["obs"]
+        zmax = int(-o["zlo"])
+        wmax = int(-o["wlo"])
+        out = (ob.C.c_int * 3)()
+        L.orc_obs_sizes(zmax, wmax, out)
+        assert (out[0], out[1], out[2]) == (o["maxkernlen"], o["fftlen"], o["corr_uselen"]), e
+        for i, sub in enumerate(e.get("subs", [])):
+            so = (ob.C.c_int * 6)()
+            L.orc_sub_sizes(sub["numharm"], sub["harmnum"], zmax, wmax, o["corr_uselen"],
+                            o["fftlen"], so)
+            got = dict(zip(["zmax", "wmax", "numz", "numw", "fftlen", "halfwidth"], list(so)))
+            for k, v in got.items():
+                assert v == sub[k], (e["zmax"], e["wmax"], e["numharm"], i, k, v, sub[k])
+
+
+def test_sigma_matches_reference_golden():
+    g = H.golden("sigma.json")
+    for power, numsum, numindep, want in g["candidate_sigma"]:
+        got = ob.orc_candidate_sigma(power, numsum, numindep)
+        if np.isnan(want):
+            assert np.isnan(got), (power, numsum, numindep)
+            continue
+        assert got == pytest.approx(want, rel=1e-9, abs=1e-9), (power, numsum, numindep)
+    for sig, numsum, numindep, want in g["power_for_sigma"]:
+        got = ob.orc_power_for_sigma(sig, numsum, numindep)
+        # the reference inverts the chi^2 CDF to a 1e-8 search tolerance
+        assert got == pytest.approx(want, rel=2e-7), (sig, numsum, numindep)
+
+
+def test_median_rank_matches_reference():
+    if not H.have_ref():
+        pytest.skip("reference build not present")
+    rng = np.random.default_rng(3)
+    for n in (1, 2, 3, 96, 192, 640, 1024, 1025):
+        a = (rng.standard_normal(n) ** 2).astype(np.float32)
+        scratch = a.copy()  # the reference reorders its input in place
+        want = ob.reflib().ref_median(scratch.ctypes.data, n)
+        assert np.sort(a)[(n - 1) // 2] == want
+
+
+@pytest.fixture(scope="module")
+def small(tmp_path_factory):
+    if not H.have_ref():
+        pytest.skip("reference build not present")
+    return H.small_problem(str(tmp_path_factory.mktemp("small")))
+
+
+def test_small_spectrum_is_the_golden_one(small):
+    g = H.golden("small_cands.json")
+    assert H.golden("small_cands.json")["spectrum_sha256"] == \
+        __import__("hashlib").sha256(small.spec.tobytes()).hexdigest()
+    assert small.obs.corr_uselen == g["obs"]["corr_uselen"]
+
+
+def test_oracle_volumes_match_reference(small):
+    # the pulsar's rstep, the first rstep and one near the top of the spectrum
+    for k in (small.rstep_of(8281.0), 0, 540):
+        startr = small.startr(k)
+        lastr = startr + small.rstep - 0.5
+        for i, (st, h) in enumerate(small.ref.subharmonics()):
+            hr, pr, ri, zi = small.ref.fderivs(1 << st, h, startr, lastr)
+            ho, po, ri2, zi2 = small.oracle.fderivs(i, startr, lastr)
+            assert hr == ho
+            if st > 0:
+                assert np.array_equal(ri, ri2) and np.array_equal(zi, zi2)
+            # the reference correlates in float FFTW, the oracle in double
+            err = np.abs(pr - po)
+            assert np.all(err <= 2e-6 * np.maximum(po, 1.0)), (k, st, h, err.max())
+
+
+def test_oracle_candidates_match_reference_prefix(small):
+    cr, _ = small.ref.search(max_steps=80)
+    co, _, _ = small.oracle.search(0, 80)
+    assert not H.compare_cands(co, cr, list(small.obs.powcut))
+
+
+def test_oracle_full_search_matches_golden(small):
+    g = H.golden("small_cands.json")
+    want = np.array([tuple(c) for c in g["cands"]], dtype=ob.CAND_DTYPE)
+    co, steps, _ = small.oracle.search()
+    assert steps == g["nrsteps"]
+    assert not H.compare_cands(co, want, g["obs"]["powcut"])
+
+
+def test_oracle_insert_replays_search(small):
+    # replaying the recorded hits through the insertion gives the same list
+    co, _, keys, pows = small.oracle.search_hits(0, 40)
+    assert len(keys) > 0
+    o = small.obs
+    nz, nw = small.subs[0]["numz"], small.subs[0]["numw"]
+    k = keys.astype(np.uint64)
+    kk = k % o.corr_uselen; k //= o.corr_uselen
+    jj = k % nz; k //= nz
+    ii = k % nw; k //= nw
+    st = k % o.numharmstages; rs = k // o.numharmstages
+    nh = (1 << st.astype(np.int64))
+    rlo = np.floor(np.rint(2 * (o.rlo + rs * small.rstep)) * 0.5)
+    hits = np.zeros(len(keys), dtype=ob.CAND_DTYPE)
+    hits["power"] = pows
+    hits["numharm"] = nh
+    hits["r"] = (rlo + kk * 0.5) / nh
+    hits["z"] = (o.zlo + jj * 2.0) / nh
+    hits["w"] = (o.wlo + ii * 20.0) / nh
+    again = ob.insert_hits(hits, list(o.numindep))
+    assert len(again) == len(co)
+    assert np.array_equal(again["r"], co["r"]) and np.array_equal(again["power"], co["power"])
+
+
+def test_insertion_walk_matches_reference_on_crafted_sequences(small):
+    """Random hit orders, including the ones that leave the reference's list
+    unsorted, give the same final list in the oracle as in the reference."""
+    rng = np.random.default_rng(5)
+    o = small.obs
+    unsorted = 0
+    for trial in range(15):
+        n = int(rng.integers(1, 2500))
+        nh = (1 << rng.integers(0, o.numharmstages, n)).astype(np.int32)
+        st = np.log2(nh).astype(int)
+        pc = np.array(list(o.powcut))[st]
+        pows = (pc + rng.uniform(0.01, 40.0, n)).astype(np.float32)
+        rlo = rng.integers(0, 4000, n).astype(np.int64)
+        want = small.ref.insert_sequence(pows, rlo, nh)
+        hits = np.zeros(n, dtype=ob.CAND_DTYPE)
+        hits["power"], hits["numharm"] = pows, nh
+        hits["r"] = rlo / nh.astype(np.float64)
+        hits["z"], hits["w"] = 0.0, 0.0
+        got = ob.insert_hits(hits, list(o.numindep))
+        assert len(got) == len(want)
+        assert np.array_equal(got["r"], want["r"])
+        assert np.array_equal(got["power"], want["power"])
+        assert np.array_equal(got["sigma"], want["sigma"])
+        unsorted += int(np.any(np.diff(want["r"]) < 0))
+    assert unsorted > 0
