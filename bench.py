@@ -1,0 +1,373 @@
+"""Benchmark: jerk-search throughput (spectra/hour) on one B200 per rank.
+
+Workload (the paper-scale configuration): 2^25-sample spectra (2^24 complex
+bins, dt = 54.6 us, T ~ 1832 s) of seeded Gaussian noise plus four injected
+pulsars, searched with -zmax 200 -wmax 300 -numharm 16 -sigma 3.0
+(23,366 rsteps of 718 bins per spectrum).  Data are synthetic (no dataset is
+available offline); the reference's published runs used real GBT data.
+
+A step is one full search of one spectrum.  value: spectra/hour over K timed
+steps with the spectra already resident in HBM.  e2e: the same through the
+public C ABI with the spectrum in pinned host memory (host-to-device copy and
+the hit/candidate read-back inside the timed region).  Each spectrum (128 MiB)
+and the per-batch ffdot volumes (~1.3 GB) exceed the 126 MB L2, so no flush is
+needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank searches its own spectra (weak scaling, no data-path
+collective); the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "spectra/hr (2^25 bins, z200 w300 h16) batched+served vs plain on B200; p50/p99"
+UNIT = "spectra/hour"
+N_SAMPLES = 1 << 25
+DT = 54.6e-6
+ZMAX, WMAX, NUMHARM, SIGMA = 200, 300, 16, 3.0
+WORKLOAD = "jerk search, 2^25-sample spectra, -zmax 200 -wmax 300 -numharm 16 -sigma 3.0"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def paper_setup():
+    from prestozl_b200 import jerk
+
+    obs, fftlen, _ = jerk.obs_from_params(N_SAMPLES // 2, N_SAMPLES, DT, ZMAX, WMAX, NUMHARM,
+                                          SIGMA)
+    subs = jerk.subharm_sizes(obs, fftlen)
+    return obs, fftlen, subs
+
+
+def make_spectrum(seed: int, device):
+    from prestozl_b200 import synth
+
+    rng = np.random.default_rng(seed)
+    pulsars = synth.random_pulsars(rng, 4)
+    ts = synth.timeseries_torch(N_SAMPLES, DT, pulsars, seed, device=device)
+    return synth.presto_fft_torch(ts)
+
+
+# --------------------------------------------------------------------------
+# CPU reference: the reference's own accelsearch (compiled from its sources
+# into oracle/_ref), on a bounded sample of rsteps of one spectrum.
+
+def reference_sample(spec_np, threads: int, target_s: float = 15.0, max_steps: int = 0):
+    """(seconds per rstep, rsteps timed, threads) of the reference CPU search."""
+    from oracle import bindings as ob
+    from prestozl_b200 import synth
+
+    with tempfile.TemporaryDirectory() as tmp:
+        root = os.path.join(tmp, "paper")
+        synth.write_fft(root, spec_np, N_SAMPLES, DT)
+        ob.set_threads(threads)
+        ref = ob.RefSearch(root + ".fft", ["-zmax", str(ZMAX), "-wmax", str(WMAX), "-numharm",
+                                           str(NUMHARM), "-sigma", str(SIGMA)])
+        ref.make_bank()
+        # calibrate on one rstep, then time a sample of about target_s seconds
+        t0 = time.perf_counter()
+        ref.search(max_steps=1)
+        t1 = time.perf_counter() - t0
+        n = max(1, min(int(target_s / max(t1, 1e-3)), 400))
+        if max_steps:
+            n = min(n, max_steps)
+        t0 = time.perf_counter()
+        ref.search(max_steps=n)
+        dt = time.perf_counter() - t0
+        ref.close()
+    return dt / n, n, threads
+
+
+def run_reference(args):
+    """--impl reference: the reference CPU search on this host's cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import bindings as ob
+
+    if not ob.have_reference():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference sources absent)"}))
+        return
+    import torch
+
+    obs, fftlen, subs = paper_setup()
+    from prestozl_b200 import jerk
+    plan_rsteps = _count_rsteps(obs)
+    spec = make_spectrum(7, "cpu").numpy()
+    threads = os.cpu_count() or 1
+    per, times = [], []
+    for i in range(args.warmup + args.steps):
+        sec, n, _ = reference_sample(spec, threads, target_s=args.ref_seconds)
+        if i >= args.warmup:
+            times.append(sec * plan_rsteps)
+            per.append(n)
+    t = statistics.mean(times)
+    value = 3600.0 / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rsteps_per_spectrum": plan_rsteps,
+                   "sample": f"first {per[0]} rsteps of one spectrum per step, scaled by "
+                             f"{plan_rsteps} rsteps"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{per[0]} rsteps x {args.steps} steps, OpenMP over "
+                                   f"{threads} threads, FFT = project FFTW stand-in"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def _count_rsteps(obs) -> int:
+    rstep = obs.corr_uselen // 2
+    n, startr = 0, obs.rlo
+    while startr + rstep < obs.highestbin:
+        n += 1
+        startr += rstep
+    return n
+
+
+# --------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=16, help="rsteps per batch")
+    ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0)
+    args = ap.parse_args()
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from prestozl_b200 import build, jerk
+    build.build()
+
+    obs, fftlen, subs = paper_setup()
+    bank = jerk.DeviceBank(subs)
+    plan = jerk.JerkPlan(obs, subs, batch=args.batch, device_bank=bank.ptr.value)
+    nrsteps = plan.num_rsteps
+
+    # two resident spectra per rank, alternated (each is larger than L2)
+    specs = [make_spectrum(1000 * rank + i, "cuda") for i in range(2)]
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        plan.search(specs[i % 2])
+    torch.cuda.synchronize()
+
+    plan.reset_stats()
+    plan.set_profiling(True)
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    step_ms = []
+    ncands = []
+    t_all0 = time.perf_counter()
+    for i in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = plan.search(specs[i % 2])
+        e1.record()
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        ncands.append(len(c))
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - t_all0
+    clocks = sampler.stop()
+    plan.set_profiling(False)
+    kstats = plan.kernel_stats()
+
+    total_ms = float(sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1000.0) * 3600.0
+
+    # e2e: pinned host spectrum through the C ABI, copy-in and read-back timed
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 2))
+    host = [s.cpu().pin_memory() for s in specs]
+    hnp = [h.numpy() for h in host]
+    plan.reset_stats()
+    barrier()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for i in range(e2e_steps):
+        t0 = time.perf_counter()
+        plan.search(hnp[i % 2])
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+    h2d, d2h = plan.transfer_stats()
+    e2e_total = float(sum(e2e_ms))
+    if dist is not None:
+        t = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * e2e_steps / (e2e_total / 1000.0) * 3600.0
+
+    # roofline of the dominant kernel class
+    dom = max(kstats.items(), key=lambda kv: kv[1]["ms"])
+    dname, d = dom
+    launches = max(d["launches"], 1)
+    per_launch_s = d["ms"] / 1000.0 / launches
+    achieved = d["bytes"] / launches / per_launch_s / 1e9
+    peak, peak_kind = peaks()
+    launches_total = sum(v["launches"] for v in kstats.values())
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "numbins": N_SAMPLES // 2,
+                       "rsteps_per_spectrum": nrsteps, "batch_rsteps": args.batch,
+                       "form": "plain (one spectrum per search call)",
+                       "l2": "inputs larger than L2 (128 MiB spectrum, ~GB volumes per batch)",
+                       "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                           "p99": float(np.percentile(step_ms, 99))},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d // e2e_steps,
+                    "d2h_bytes_per_step": d2h // e2e_steps},
+            "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "traffic": None,
+                         "fp32_tflops": d["flops"] / launches / per_launch_s / 1e12},
+            "kernels": {k: {"launches": v["launches"], "ms": v["ms"],
+                            "share": v["ms"] / max(sum(x["ms"] for x in kstats.values()), 1e-9),
+                            "gbs": v["bytes"] / max(v["ms"], 1e-9) / 1e6,
+                            "tflops": v["flops"] / max(v["ms"], 1e-9) / 1e9}
+                        for k, v in kstats.items()},
+            "gpu_launches": launches_total,
+            "clocks": clocks,
+            "wall_s": wall,
+            "candidates_per_spectrum": ncands,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                from oracle import bindings as ob
+                if ob.have_reference():
+                    spec_np = specs[0].cpu().numpy()
+                    threads = os.cpu_count() or 1
+                    sec, n, th = reference_sample(spec_np, threads, target_s=args.ref_seconds)
+                    cpu_val = 3600.0 / (sec * nrsteps)
+                    line["cpu_baseline"] = {
+                        "value": cpu_val, "unit": UNIT, "cores": th, "kind": "reference",
+                        "sample": f"first {n} rsteps of one spectrum ({sec * n:.1f} s), scaled "
+                                  f"by {nrsteps} rsteps; OpenMP, FFT = project FFTW stand-in"}
+            except Exception as exc:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)}
+        print(json.dumps(line))
+
+    plan.close()
+    bank.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

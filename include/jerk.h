@@ -135,6 +135,36 @@ long long jerk_num_rsteps(const jerk_plan *plan);
 int jerk_debug_volume(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
                       long long rstep, int sub, float *out, int *numrs, long long *rlo);
 
+/* Instrumentation.  Every launch is counted with its algorithmic bytes and
+ * flops; with profiling on, each launch is also bracketed by CUDA events on
+ * the plan's stream and its device time accumulated per kernel class
+ * ("prep", "corr_<fftlen>", "harmsum"). */
+typedef struct jerk_kernel_stat {
+    char name[32];
+    long long launches;
+    double ms;                /* summed device time (profiling on) */
+    double bytes;             /* summed algorithmic bytes */
+    double flops;             /* summed algorithmic flops */
+} jerk_kernel_stat;
+
+int jerk_plan_set_profiling(jerk_plan *plan, int on);
+void jerk_plan_reset_stats(jerk_plan *plan);
+/* Number of kernel classes; fills up to max entries of out. */
+int jerk_plan_kernel_stats(const jerk_plan *plan, int max, jerk_kernel_stat *out);
+/* Bytes copied host->device (spectra) and device->host (hit lists). */
+void jerk_plan_transfer_stats(const jerk_plan *plan, long long *h2d, long long *d2h);
+
+/* Kernel bank on the device: [sub][w][z][fftlen] complex64 for the given
+ * subharmonics (in jerk_subharm_sizes order), the layout jerk_plan_create
+ * takes as jerk_config.device_bank.  device_bank must hold
+ * jerk_bank_elements() complex64 values; stream may be NULL. */
+long long jerk_bank_elements(const jerk_subharm *subs, int nsubs);
+/* cudaMalloc / cudaFree for callers without their own device allocator. */
+int jerk_device_alloc(long long bytes, void **out);
+void jerk_device_free(void *p);
+int jerk_copy_to_host(void *dst, const void *device_src, long long bytes);
+int jerk_bank_generate(const jerk_subharm *subs, int nsubs, void *device_bank, void *stream);
+
 /* Statistics (host, double precision). */
 double jerk_candidate_sigma(double power, int numsum, double numtrials);
 double jerk_power_for_sigma(double sigma, int numsum, double numtrials);

@@ -1,0 +1,291 @@
+// Kernel-bank generation on the GPU.
+//
+// The reference builds, for every subharmonic and every (w, z) of its grid,
+// the Fourier response of a signal with f-dot z and f-dot-dot w, places it
+// wrapped around an fftlen array and takes its forward FFT -- on the host,
+// in double precision plus float FFTW (src/accel_utils.c:151-168
+// init_kernel, src/responses.c:158-418 gen_r/z/w_response,
+// src/corr_prep.c:92-114 place_complex_kernel).  Here every kernel is one
+// CTA, in two passes:
+//
+//   bank_response_kernel   the numkern response values in double, rounded to
+//                          float and placed into the bank row (zeros between):
+//     w != 0  the reference's method: a float cosine series of num_pts
+//             samples, zero-padded to twice its length, whose real FFT is
+//             sampled at numkern bins; here those bins are evaluated as a
+//             direct DFT in double (phasor recurrence, re-seeded every 64
+//             samples), which is the same sum without the FFT's rounding;
+//     w == 0, z != 0  the closed form with Fresnel integrals;
+//     w == 0, z == 0  the interbinning sinc.
+//   bank_fft_kernel<N>     in-place forward FFT (sign -1) of each row with the
+//                          shared-memory Stockham FFT of jerk_fft.cuh.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "jerk.h"
+#include "jerk_fft.cuh"
+#include "jerk_kernels.cuh"
+
+namespace jerk {
+
+
+// Fresnel integrals C(x) = int_0^x cos(pi t^2/2) dt, S(x) = int_0^x sin(pi t^2/2) dt.
+// |x| < 1.5: the power series of int_0^x exp(i pi t^2/2) dt,
+//   sum_k (i pi/2)^k x^(2k+1) / (k! (2k+1));
+// otherwise C + iS = (1+i)/2 * erf(sqrt(pi)/2 (1-i) x), with erfc from its
+// even continued fraction (denominators 1 - i pi x^2 + 4k, numerators
+// -(2k-1)(2k)), evaluated by the modified Lentz method.
+__device__ void fresnel(double x, double *S, double *C)
+{
+    const double ax = fabs(x);
+    double c = 0.0, s = 0.0;
+    if (ax < 1.5) {
+        const double p = 0.5 * M_PI * ax * ax;
+        double ft = ax;
+        for (int k = 0; k < 60; k++) {
+            const double term = ft / (2 * k + 1);
+            switch (k & 3) {
+            case 0: c += term; break;
+            case 1: s += term; break;
+            case 2: c -= term; break;
+            default: s -= term; break;
+            }
+            ft *= p / (k + 1);
+            if (ft < 1e-18 * (fabs(c) + fabs(s)))
+                break;
+        }
+    } else {
+        const double pix2 = M_PI * ax * ax;
+        double br = 1.0, bi = -pix2;
+        double ccr = 1e300, cci = 0.0;
+        // d = h = 1 / b
+        double den = br * br + bi * bi;
+        double dr = br / den, di = -bi / den;
+        double hr = dr, hi = di;
+        int n = -1;
+        for (int k = 2; k < 300; k++) {
+            n += 2;
+            const double a = -(double)n * (n + 1);
+            br += 4.0;
+            // d = 1 / (a d + b)
+            double tr = a * dr + br, ti = a * di + bi;
+            den = tr * tr + ti * ti;
+            dr = tr / den;
+            di = -ti / den;
+            // cc = b + a / cc
+            den = ccr * ccr + cci * cci;
+            const double qr = a * ccr / den, qi = -a * cci / den;
+            ccr = br + qr;
+            cci = bi + qi;
+            // del = cc d ; h = h del
+            const double er = ccr * dr - cci * di, ei = ccr * di + cci * dr;
+            const double nhr = hr * er - hi * ei, nhi = hr * ei + hi * er;
+            hr = nhr;
+            hi = nhi;
+            if (fabs(er - 1.0) + fabs(ei) < 1e-16)
+                break;
+        }
+        // h = (ax - i ax) h
+        const double h2r = ax * hr + ax * hi, h2i = ax * hi - ax * hr;
+        double sn, cs;
+        sincos(0.5 * pix2, &sn, &cs);
+        // (cos + i sin) h
+        const double mr = cs * h2r - sn * h2i, mi = cs * h2i + sn * h2r;
+        // (0.5 + 0.5 i)(1 - m)
+        const double ur = 1.0 - mr, ui = -mi;
+        c = 0.5 * ur - 0.5 * ui;
+        s = 0.5 * ur + 0.5 * ui;
+    }
+    if (x < 0.0) {
+        c = -c;
+        s = -s;
+    }
+    *C = c;
+    *S = s;
+}
+
+constexpr int kBankThreads = 256;
+
+// value numbers ii of the raw response (src/responses.c), then placement:
+// raw index ii < numkern/2 goes to fftlen - numkern/2 + ii, the rest to
+// ii - numkern/2 (src/corr_prep.c:92-114)
+__device__ __forceinline__ long long placed(int ii, int numkern, int fftlen)
+{
+    const int half = numkern / 2;
+    return ii < half ? (long long)(fftlen - half + ii) : (long long)(ii - half);
+}
+
+__global__ void __launch_bounds__(kBankThreads)
+    bank_response_kernel(const BankRow *rows, float2 *bank)
+{
+    extern __shared__ float xs[];
+    const BankRow R = rows[blockIdx.x];
+    const int tid = threadIdx.x;
+    float2 *row = bank + R.off;
+    const int numkern = R.numkern;
+    const int numbetween = 2;
+
+    // zero the parts of the row the response does not cover
+    for (int m = numkern / 2 + tid; m < R.fftlen - numkern / 2; m += kBankThreads)
+        row[m] = make_float2(0.f, 0.f);
+
+    const double z = R.z, w = R.w;
+    if (fabs(w) >= 1e-4) {
+        // gen_w_response (src/responses.c:333-418), roffset = 0
+        const int npts = R.num_pts;
+        const double dt = 1.0 / (double)npts;
+        const double amp = 2.0 * dt;
+        const int fbar = npts / 4;
+        const double f = __dadd_rn(__dsub_rn((double)fbar, 0.5 * z), w / 12.0);
+        const double fd = (z - 0.5 * w) / 2.0;
+        const double fdd = w / 6.0;
+        for (int n = tid; n < npts; n += kBankThreads) {
+            const double t = __dmul_rn((double)n, dt);
+            // TWOPI * (t * (t * (t * fdd + fd) + f)), no contraction
+            const double in1 = __dadd_rn(__dmul_rn(t, fdd), fd);
+            const double in2 = __dadd_rn(__dmul_rn(t, in1), f);
+            const double ph = __dmul_rn(6.2831853071795864769252867665590057683943387987502,
+                                        __dmul_rn(t, in2));
+            xs[n] = (float)__dmul_rn(amp, cos(ph));
+        }
+        __syncthreads();
+        // complex bins k0 + k of the length-2*npts real DFT
+        const int L = npts * numbetween;
+        const int k0 = fbar * numbetween - numkern / 2;
+        for (int k = tid; k < numkern; k += kBankThreads) {
+            const long long kc = k0 + k;
+            double accr = 0.0, acci = 0.0;
+            double wr, wi;  // exp(-2 pi i kc / L)
+            sincospi(-2.0 * (double)kc / (double)L, &wi, &wr);
+            for (int n0 = 0; n0 < npts; n0 += 64) {
+                double pr, pi;  // exp(-2 pi i kc n0 / L), exact reduction of kc*n0 mod L
+                const long long m = (kc * (long long)n0) % L;
+                sincospi(-2.0 * (double)m / (double)L, &pi, &pr);
+                const int nend = min(npts, n0 + 64);
+                for (int n = n0; n < nend; n++) {
+                    const double x = (double)xs[n];
+                    accr = fma(x, pr, accr);
+                    acci = fma(x, pi, acci);
+                    const double tr = pr * wr - pi * wi;
+                    pi = pr * wi + pi * wr;
+                    pr = tr;
+                }
+            }
+            row[placed(k, numkern, R.fftlen)] = make_float2((float)accr, (float)acci);
+        }
+    } else if (fabs(z) >= 1e-4) {
+        // gen_z_response (src/responses.c:228-313), roffset = 0
+        const double absz = fabs(z);
+        const double startr0 = -0.5 * z;
+        const int signz = z < 0.0 ? -1 : 1;
+        const double zd = signz * 1.4142135623730950488016887242096980785696718753769 / sqrt(absz);
+        const double cons = zd / 2.0;
+        const double pibyz = M_PI / z;
+        const double startr = startr0 + numkern / (double)(2 * numbetween);
+        const double delta = -1.0 / numbetween;
+        for (int ii = tid; ii < numkern; ii += kBankThreads) {
+            const double r = startr + ii * delta;
+            const double yy = __dmul_rn(r, zd);
+            const double zz = __dadd_rn(yy, __dmul_rn(z, zd));
+            const double xx = __dmul_rn(__dmul_rn(pibyz, r), r);
+            double sn, cs, fsy, fcy, fsz, fcz;
+            sincos(xx, &sn, &cs);
+            fresnel(yy, &fsy, &fcy);
+            fresnel(zz, &fsz, &fcz);
+            const double tmprl = signz * (fcz - fcy);
+            const double tmpim = fsy - fsz;
+            const float re = (float)__dmul_rn(__dsub_rn(__dmul_rn(tmprl, cs), __dmul_rn(tmpim, sn)), cons);
+            const float im = (float)-__dmul_rn(__dadd_rn(__dmul_rn(tmprl, sn), __dmul_rn(tmpim, cs)), cons);
+            row[placed(ii, numkern, R.fftlen)] = make_float2(re, im);
+        }
+    } else {
+        // gen_r_response (src/responses.c:158-226), roffset = 0:
+        // value ii = exp(i r) sin(r) / r at r = pi (numkern/4 - ii/2)
+        for (int ii = tid; ii < numkern; ii += kBankThreads) {
+            const double q = numkern / (double)(2 * numbetween) - 0.5 * ii;  // r / pi
+            float re = 1.0f, im = 0.0f;
+            if (q != 0.0) {
+                double sn, cs;
+                sincospi(q, &sn, &cs);
+                const double sinc = sn / (M_PI * q);
+                re = (float)(cs * sinc);
+                im = (float)(sn * sinc);
+            }
+            row[placed(ii, numkern, R.fftlen)] = make_float2(re, im);
+        }
+    }
+}
+
+struct BankGroup {
+    int first, count;  // rows [first, first + count) of one fftlen
+};
+
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N>::T)
+    bank_fft_kernel(const BankRow *rows, int first, const float2 *twiddles, int twoff,
+                    float2 *bank)
+{
+    constexpr int R0 = FftPlan<N>::R0;
+    constexpr int T = FftPlan<N>::T;
+    extern __shared__ float2 smb[];
+    float2 *buf = smb, *tw = smb + N;
+    const int tid = threadIdx.x;
+    const BankRow R = rows[first + blockIdx.x];
+    float2 *row = bank + R.off;
+    for (int i = tid; i < N; i += T)
+        tw[i] = twiddles[twoff + i];
+    __syncthreads();
+    auto in = [&](int r) -> float2 { return row[tid + r * (N / R0)]; };
+    auto out = [&](int m, float2 y) { row[m] = y; };
+    fft_block<N, -1>(buf, tw, tid, in, out);
+}
+
+template <int N>
+static cudaError_t launch_bank_fft(const BankRow *rows, int first, int count, const float2 *tw,
+                                   int twoff, float2 *bank, cudaStream_t st)
+{
+    const size_t smem = sizeof(float2) * 2 * N;
+    cudaError_t e = cudaFuncSetAttribute(bank_fft_kernel<N>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    bank_fft_kernel<N><<<count, FftPlan<N>::T, smem, st>>>(rows, first, tw, twoff, bank);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bank_fft_any(int N, const BankRow *rows, int first, int count, const float2 *tw,
+                                int twoff, float2 *bank, cudaStream_t st)
+{
+    switch (N) {
+    case 128: return launch_bank_fft<128>(rows, first, count, tw, twoff, bank, st);
+    case 192: return launch_bank_fft<192>(rows, first, count, tw, twoff, bank, st);
+    case 256: return launch_bank_fft<256>(rows, first, count, tw, twoff, bank, st);
+    case 384: return launch_bank_fft<384>(rows, first, count, tw, twoff, bank, st);
+    case 512: return launch_bank_fft<512>(rows, first, count, tw, twoff, bank, st);
+    case 768: return launch_bank_fft<768>(rows, first, count, tw, twoff, bank, st);
+    case 1024: return launch_bank_fft<1024>(rows, first, count, tw, twoff, bank, st);
+    case 1280: return launch_bank_fft<1280>(rows, first, count, tw, twoff, bank, st);
+    case 2048: return launch_bank_fft<2048>(rows, first, count, tw, twoff, bank, st);
+    case 4096: return launch_bank_fft<4096>(rows, first, count, tw, twoff, bank, st);
+    case 5120: return launch_bank_fft<5120>(rows, first, count, tw, twoff, bank, st);
+    case 7680: return launch_bank_fft<7680>(rows, first, count, tw, twoff, bank, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_bank_response(const BankRow *rows, int nrows, int max_pts, float2 *bank,
+                                 cudaStream_t st)
+{
+    const size_t smem = sizeof(float) * (size_t)(max_pts > 0 ? max_pts : 1);
+    cudaError_t e = cudaFuncSetAttribute(bank_response_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    bank_response_kernel<<<nrows, kBankThreads, smem, st>>>(rows, bank);
+    return cudaGetLastError();
+}
+
+}  // namespace jerk

@@ -70,6 +70,15 @@ struct SearchDev {
     unsigned int *status;     // bit 0: a subharmonic r index fell outside its row
 };
 
+// One response kernel of the bank (jerk_bank.cu).
+struct BankRow {
+    long long off;     // float2 offset of the row in the bank
+    int z, w;          // this kernel's f-dot and f-dot-dot
+    int fftlen;
+    int numkern;       // 2 * numbetween * w_resp_halfwidth(z, w)
+    int num_pts;       // w != 0: length of the cosine series
+};
+
 // The corr_kernel launch for one fftlen covers the rows (w, z) of every
 // subharmonic with that fftlen, numbered consecutively.
 struct RowGroup {

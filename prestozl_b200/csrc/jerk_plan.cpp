@@ -27,6 +27,10 @@ cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int r
                         cudaStream_t st);
 cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st);
 bool fftlen_supported(int n);
+cudaError_t launch_bank_response(const BankRow *rows, int nrows, int max_pts, float2 *bank,
+                                 cudaStream_t st);
+cudaError_t launch_bank_fft_any(int N, const BankRow *rows, int first, int count, const float2 *tw,
+                                int twoff, float2 *bank, cudaStream_t st);
 }  // namespace jerk
 
 using namespace jerk;
@@ -398,7 +402,6 @@ class CandList {
     };
 
     bool empty() const { return n_ == 0; }
-    size_t size() const { return n_; }
 
     // the reference walk's stopping node
     Pos walk(double rr) const
@@ -553,7 +556,131 @@ extern "C" long long jerk_insert_hits(const jerk_cand *hits, long long nhits, je
 }
 
 // ---------------------------------------------------------------------------
+// twiddle tables exp(-2 pi i m / N), computed in double
+
+static void append_twiddles(int N, std::vector<float2> &tw)
+{
+    for (int m = 0; m < N; m++) {
+        const double a = -2.0 * M_PI * (double)m / (double)N;
+        tw.push_back(make_float2((float)cos(a), (float)sin(a)));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel bank (create_subharminfos / init_kernel, src/accel_utils.c:151-282)
+
+extern "C" long long jerk_bank_elements(const jerk_subharm *subs, int nsubs)
+{
+    long long n = 0;
+    for (int s = 0; s < nsubs; s++)
+        n += (long long)subs[s].numw * subs[s].numz * subs[s].fftlen;
+    return n;
+}
+
+extern "C" int jerk_device_alloc(long long bytes, void **out)
+{
+    if (!out || bytes <= 0)
+        return fail(JERK_EINVAL, "jerk_device_alloc: bad argument");
+    JERK_CUDA(cudaMalloc(out, (size_t)bytes));
+    return JERK_OK;
+}
+
+extern "C" void jerk_device_free(void *p) { cudaFree(p); }
+
+extern "C" int jerk_copy_to_host(void *dst, const void *src, long long bytes)
+{
+    JERK_CUDA(cudaMemcpy(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost));
+    return JERK_OK;
+}
+
+extern "C" int jerk_bank_generate(const jerk_subharm *subs, int nsubs, void *device_bank,
+                                  void *stream)
+{
+    if (!subs || nsubs <= 0 || !device_bank)
+        return fail(JERK_EINVAL, "jerk_bank_generate: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    // rows grouped by fftlen so each FFT launch covers a contiguous range
+    std::map<int, std::vector<BankRow>> byN;
+    long long off = 0;
+    int max_pts = 1;
+    for (int s = 0; s < nsubs; s++) {
+        const jerk_subharm &sh = subs[s];
+        if (!fftlen_supported(sh.fftlen))
+            return fail(JERK_EUNSUPPORTED, "unsupported fftlen " + std::to_string(sh.fftlen));
+        for (int ii = 0; ii < sh.numw; ii++)
+            for (int jj = 0; jj < sh.numz; jj++) {
+                BankRow r{};
+                r.z = -sh.zmax + jj * kDZ;
+                r.w = -sh.wmax + ii * kDW;
+                r.fftlen = sh.fftlen;
+                const int hw = w_resp_halfwidth((double)r.z, (double)r.w);
+                r.numkern = 2 * 2 * hw;
+                r.num_pts = 0;
+                if (fabs((double)r.w) >= 1e-4) {
+                    r.num_pts = (int)next2_to_n(6 * hw + 200 + r.numkern / 2);
+                    max_pts = std::max(max_pts, r.num_pts);
+                }
+                if (r.numkern > sh.fftlen)
+                    return fail(JERK_EINVAL, "response wider than its fftlen");
+                r.off = off + ((long long)ii * sh.numz + jj) * sh.fftlen;
+                byN[sh.fftlen].push_back(r);
+            }
+        off += (long long)sh.numw * sh.numz * sh.fftlen;
+    }
+    if ((size_t)max_pts * sizeof(float) > 200 * 1024)
+        return fail(JERK_EUNSUPPORTED, "response series too long for shared memory");
+    std::vector<BankRow> rows;
+    std::vector<std::pair<int, std::pair<int, int>>> groups;  // N, (first, count)
+    std::vector<float2> tw;
+    std::map<int, int> twoff;
+    for (auto &kv : byN) {
+        groups.push_back({kv.first, {(int)rows.size(), (int)kv.second.size()}});
+        rows.insert(rows.end(), kv.second.begin(), kv.second.end());
+        twoff[kv.first] = (int)tw.size();
+        append_twiddles(kv.first, tw);
+    }
+    BankRow *d_rows = nullptr;
+    float2 *d_tw = nullptr;
+    int rc = JERK_OK;
+    cudaError_t e = cudaMalloc(&d_rows, sizeof(BankRow) * rows.size());
+    if (e == cudaSuccess)
+        e = cudaMalloc(&d_tw, sizeof(float2) * tw.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_rows, rows.data(), sizeof(BankRow) * rows.size(),
+                            cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice,
+                            st);
+    if (e == cudaSuccess)
+        e = launch_bank_response(d_rows, (int)rows.size(), max_pts, (float2 *)device_bank, st);
+    for (size_t g = 0; g < groups.size() && e == cudaSuccess; g++)
+        e = launch_bank_fft_any(groups[g].first, d_rows, groups[g].second.first,
+                                groups[g].second.second, d_tw, twoff[groups[g].first],
+                                (float2 *)device_bank, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        rc = cuda_fail(e, "jerk_bank_generate");
+    cudaFree(d_rows);
+    cudaFree(d_tw);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
 // The plan
+
+// per kernel class: launches, device time (CUDA events on the plan's stream,
+// only while profiling is on), and algorithmic bytes / flops of the launches
+struct KernelClass {
+    std::string name;
+    long long launches = 0;
+    double ms = 0.0, bytes = 0.0, flops = 0.0;
+};
+
+struct PendingTiming {
+    int cls;
+    cudaEvent_t start, stop;
+};
 
 struct jerk_plan {
     int device = 0;
@@ -586,7 +713,118 @@ struct jerk_plan {
     unsigned int *d_status = nullptr;
     long long max_hits = 0;
     long long plane_floats = 0, prepped_f2 = 0;
+    // instrumentation
+    bool profiling = false;
+    std::vector<KernelClass> classes;
+    std::map<std::string, int> class_index;
+    std::vector<PendingTiming> pending;
+    std::vector<cudaEvent_t> event_pool;
+    long long h2d_bytes = 0, d2h_bytes = 0;
 };
+
+static int kclass(jerk_plan *p, const std::string &name)
+{
+    auto it = p->class_index.find(name);
+    if (it != p->class_index.end())
+        return it->second;
+    KernelClass k;
+    k.name = name;
+    p->classes.push_back(k);
+    p->class_index[name] = (int)p->classes.size() - 1;
+    return (int)p->classes.size() - 1;
+}
+
+static cudaEvent_t take_event(jerk_plan *p)
+{
+    if (!p->event_pool.empty()) {
+        cudaEvent_t e = p->event_pool.back();
+        p->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Bracket one launch: returns a token to pass to launch_end.
+static int launch_begin(jerk_plan *p, int cls, double bytes, double flops)
+{
+    KernelClass &k = p->classes[cls];
+    k.launches++;
+    k.bytes += bytes;
+    k.flops += flops;
+    if (!p->profiling)
+        return -1;
+    PendingTiming t{cls, take_event(p), take_event(p)};
+    cudaEventRecord(t.start, p->stream);
+    p->pending.push_back(t);
+    return (int)p->pending.size() - 1;
+}
+
+static void launch_end(jerk_plan *p, int token)
+{
+    if (token >= 0)
+        cudaEventRecord(p->pending[token].stop, p->stream);
+}
+
+// after a stream synchronisation: fold the recorded intervals into the classes
+static void collect_timings(jerk_plan *p)
+{
+    for (auto &t : p->pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t.start, t.stop) == cudaSuccess)
+            p->classes[t.cls].ms += ms;
+        p->event_pool.push_back(t.start);
+        p->event_pool.push_back(t.stop);
+    }
+    p->pending.clear();
+}
+
+extern "C" int jerk_plan_set_profiling(jerk_plan *p, int on)
+{
+    if (!p)
+        return fail(JERK_EINVAL, "null plan");
+    p->profiling = on != 0;
+    return JERK_OK;
+}
+
+extern "C" void jerk_plan_reset_stats(jerk_plan *p)
+{
+    if (!p)
+        return;
+    for (auto &k : p->classes) {
+        k.launches = 0;
+        k.ms = k.bytes = k.flops = 0.0;
+    }
+    p->h2d_bytes = p->d2h_bytes = 0;
+}
+
+extern "C" int jerk_plan_kernel_stats(const jerk_plan *p, int max, jerk_kernel_stat *out)
+{
+    if (!p)
+        return 0;
+    int n = 0;
+    for (const auto &k : p->classes) {
+        if (n < max && out) {
+            memset(&out[n], 0, sizeof(out[n]));
+            strncpy(out[n].name, k.name.c_str(), sizeof(out[n].name) - 1);
+            out[n].launches = k.launches;
+            out[n].ms = k.ms;
+            out[n].bytes = k.bytes;
+            out[n].flops = k.flops;
+        }
+        n++;
+    }
+    return n;
+}
+
+extern "C" void jerk_plan_transfer_stats(const jerk_plan *p, long long *h2d, long long *d2h)
+{
+    if (h2d)
+        *h2d = p ? p->h2d_bytes : 0;
+    if (d2h)
+        *d2h = p ? p->d2h_bytes : 0;
+}
 
 static void plan_free_device(jerk_plan *p)
 {
@@ -617,6 +855,12 @@ extern "C" void jerk_plan_destroy(jerk_plan *p)
     if (p->stream)
         cudaStreamSynchronize(p->stream);
     plan_free_device(p);
+    for (auto &t : p->pending) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    for (auto e : p->event_pool)
+        cudaEventDestroy(e);
     if (p->own_stream && p->stream)
         cudaStreamDestroy(p->stream);
     cudaSetDevice(cur);
@@ -782,13 +1026,14 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     p->prepped_f2 = data_off;
 
     // twiddles: exp(-2 pi i m / N), double on the host
-    std::vector<float2> tw(twtotal);
-    for (auto &kv : twoff) {
-        const int N = kv.first;
-        for (int m = 0; m < N; m++) {
-            const double a = -2.0 * M_PI * (double)m / (double)N;
-            tw[kv.second + m] = make_float2((float)cos(a), (float)sin(a));
-        }
+    std::vector<float2> tw;
+    {
+        std::vector<std::pair<int, int>> byoff;
+        for (auto &kv : twoff)
+            byoff.push_back({kv.second, kv.first});
+        std::sort(byoff.begin(), byoff.end());
+        for (auto &o : byoff)
+            append_twiddles(o.second, tw);
     }
 
 #define JERK_CUDA_B(call)                                \
@@ -863,6 +1108,7 @@ static int stage_spectrum(jerk_plan *p, const void *spectrum, int on_device, con
     }
     JERK_CUDA(cudaMemcpyAsync(p->d_spec, spectrum, sizeof(float2) * p->obs.numbins,
                               cudaMemcpyHostToDevice, p->stream));
+    p->h2d_bytes += (long long)sizeof(float2) * p->obs.numbins;
     *spec = p->d_spec;
     return JERK_OK;
 }
@@ -900,11 +1146,27 @@ static SearchDev make_args(const jerk_plan *p, const float2 *spec)
 }
 
 // prep + correlation for one batch (volumes only)
+static inline double fft_flops(int n)
+{
+    return 5.0 * n * log2((double)n);
+}
+
 static int run_volumes(jerk_plan *p, SearchDev &a)
 {
-    cudaError_t e = launch_prep(a, p->maxfft, p->stream);
-    if (e != cudaSuccess)
-        return cuda_fail(e, "prep_kernel");
+    {
+        double bytes = 0, flops = 0;
+        for (int s = 0; s < p->nsubs; s++) {
+            const int N = p->subs[s].fftlen;
+            bytes += (double)a.nb * (N / 2 * 8.0 + N * 8.0);
+            flops += (double)a.nb * fft_flops(N);
+        }
+        const int tok = launch_begin(p, kclass(p, "prep"), bytes, flops);
+        cudaError_t e = launch_prep(a, p->maxfft, p->stream);
+        launch_end(p, tok);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "prep_kernel");
+    }
+    cudaError_t e = cudaSuccess;
     for (auto &kv : p->groups) {
         RowGroup G{};
         G.n = (int)kv.second.size();
@@ -916,7 +1178,22 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
             rows += p->subs[s].numw * p->subs[s].numz;
         }
         G.rowstart[G.n] = rows;
-        e = launch_corr(a, kv.first, G, rows, p->stream);
+        // algorithmic traffic: each kernel row read once per batch, each
+        // prepared chunk read once, every good power written once
+        const int N = kv.first;
+        double bytes = 0, flops = 0;
+        for (int i = 0; i < G.n; i++) {
+            const int s = G.sub[i];
+            const double nrow = (double)p->subs[s].numw * p->subs[s].numz;
+            double numrs = 0;
+            for (int b = 0; b < a.nb; b++)
+                numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
+            bytes += nrow * N * 8.0 + a.nb * N * 8.0 + nrow * numrs * 4.0;
+            flops += nrow * a.nb * (fft_flops(N) + 6.0 * N) + nrow * numrs * 3.0;
+        }
+        const int tok = launch_begin(p, kclass(p, "corr_" + std::to_string(N)), bytes, flops);
+        e = launch_corr(a, N, G, rows, p->stream);
+        launch_end(p, tok);
         if (e != cudaSuccess)
             return cuda_fail(e, "corr_kernel");
     }
@@ -935,7 +1212,19 @@ static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, lo
         int rc = run_volumes(p, a);
         if (rc != JERK_OK)
             return rc;
+        // algorithmic traffic: every volume of the batch read once
+        double bytes = 0, flops = 0;
+        const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
+        for (int s = 0; s < p->nsubs; s++) {
+            double numrs = 0;
+            for (int b = 0; b < a.nb; b++)
+                numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
+            bytes += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
+        }
+        flops = npts * p->nsubs;
+        const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops);
         cudaError_t e = launch_harmsum(a, p->stream);
+        launch_end(p, tok);
         if (e != cudaSuccess)
             return cuda_fail(e, "harmsum_kernel");
     }
@@ -944,6 +1233,8 @@ static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, lo
     JERK_CUDA(cudaMemcpyAsync(&status, p->d_status, sizeof(unsigned int),
                               cudaMemcpyDeviceToHost, p->stream));
     JERK_CUDA(cudaStreamSynchronize(p->stream));
+    collect_timings(p);
+    p->d2h_bytes += 2 * sizeof(unsigned int);
     if (status)
         return fail(JERK_EINVAL, "harmonic sum: a subharmonic r index left its row");
     return JERK_OK;
@@ -994,6 +1285,7 @@ extern "C" int jerk_search(jerk_plan *p, const void *spectrum, int spectrum_on_d
         JERK_CUDA(cudaMemcpyAsync(pows.data(), p->d_hit_pows, sizeof(float) * nh,
                                   cudaMemcpyDeviceToHost, p->stream));
         JERK_CUDA(cudaStreamSynchronize(p->stream));
+        p->d2h_bytes += (long long)nh * (sizeof(unsigned long long) + sizeof(float));
     }
     std::vector<uint32_t> order(nh);
     for (uint32_t i = 0; i < nh; i++)
@@ -1058,6 +1350,8 @@ extern "C" int jerk_debug_volume(jerk_plan *p, const void *spectrum, int spectru
     rc = run_volumes(p, a);
     if (rc != JERK_OK)
         return rc;
+    JERK_CUDA(cudaStreamSynchronize(p->stream));
+    collect_timings(p);
     const SubDev &d = p->hsubs[sub];
     const StepDev &st = p->hsteps[(size_t)rstep * p->nsubs + sub];
     JERK_CUDA(cudaMemcpy2DAsync(out, sizeof(float) * st.numrs, p->d_planes + d.plane_off,

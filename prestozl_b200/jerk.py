@@ -63,6 +63,11 @@ class Config(C.Structure):
                 ("stream", C.c_void_p), ("device_bank", C.c_void_p)]
 
 
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_longlong), ("ms", C.c_double),
+                ("bytes", C.c_double), ("flops", C.c_double)]
+
+
 class Hits(C.Structure):
     _fields_ = [("count", C.c_longlong), ("keys", C.POINTER(C.c_ulonglong)),
                 ("powers", C.POINTER(C.c_float))]
@@ -78,7 +83,9 @@ EXPORTS = [
     "jerk_obs_from_params", "jerk_subharm_count", "jerk_subharm_sizes", "jerk_plan_create",
     "jerk_plan_destroy", "jerk_search", "jerk_num_rsteps", "jerk_debug_volume",
     "jerk_candidate_sigma", "jerk_power_for_sigma", "jerk_insert_hits", "jerk_free",
-    "jerk_last_error",
+    "jerk_last_error", "jerk_bank_elements", "jerk_bank_generate", "jerk_device_alloc",
+    "jerk_device_free", "jerk_copy_to_host", "jerk_plan_set_profiling", "jerk_plan_reset_stats",
+    "jerk_plan_kernel_stats", "jerk_plan_transfer_stats",
 ]
 
 
@@ -115,6 +122,20 @@ def lib() -> C.CDLL:
     L.jerk_insert_hits.argtypes = [C.POINTER(Cand), C.c_longlong, C.POINTER(C.POINTER(Cand))]
     L.jerk_free.argtypes = [C.c_void_p]
     L.jerk_free.restype = None
+    L.jerk_bank_elements.restype = C.c_longlong
+    L.jerk_bank_elements.argtypes = [C.POINTER(Subharm), C.c_int]
+    L.jerk_bank_generate.argtypes = [C.POINTER(Subharm), C.c_int, C.c_void_p, C.c_void_p]
+    L.jerk_device_alloc.argtypes = [C.c_longlong, C.POINTER(C.c_void_p)]
+    L.jerk_device_free.argtypes = [C.c_void_p]
+    L.jerk_device_free.restype = None
+    L.jerk_copy_to_host.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
+    L.jerk_plan_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    L.jerk_plan_reset_stats.argtypes = [C.c_void_p]
+    L.jerk_plan_reset_stats.restype = None
+    L.jerk_plan_kernel_stats.argtypes = [C.c_void_p, C.c_int, C.POINTER(KernelStat)]
+    L.jerk_plan_transfer_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong),
+                                           C.POINTER(C.c_longlong)]
+    L.jerk_plan_transfer_stats.restype = None
     _lib = L
     return L
 
@@ -160,6 +181,50 @@ def insert_hits(hits: np.ndarray) -> np.ndarray:
     res = np.frombuffer(arr.tobytes(), dtype=CAND_DTYPE).copy()
     lib().jerk_free(out)
     return res
+
+
+def _subharm_array(subs: Sequence[dict]):
+    arr = (Subharm * len(subs))()
+    for i, s in enumerate(subs):
+        arr[i] = Subharm(s["numharm"], s["harmnum"], s.get("zmax", 0), s.get("wmax", 0),
+                         s["numz"], s["numw"], s["fftlen"], s["halfwidth"], None)
+    return arr
+
+
+class DeviceBank:
+    """A kernel bank generated on the device (jerk_bank_generate); pass it to
+    JerkPlan(device_bank=bank.ptr) to share it between plans."""
+
+    def __init__(self, subs: Sequence[dict], stream: int = 0):
+        arr = _subharm_array(subs)
+        self.elements = lib().jerk_bank_elements(arr, len(subs))
+        self.ptr = C.c_void_p()
+        _check(lib().jerk_device_alloc(self.elements * 8, C.byref(self.ptr)))
+        rc = lib().jerk_bank_generate(arr, len(subs), self.ptr, stream or None)
+        if rc != JERK_OK:
+            self.close()
+            _check(rc)
+
+    def close(self) -> None:
+        if self.ptr:
+            lib().jerk_device_free(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def rows(self, subs: Sequence[dict], sub: int, rows: Sequence[int]) -> np.ndarray:
+        """Copy kernel rows (flattened w * numz + z) of one subharmonic to the host."""
+        off = sum(s["numw"] * s["numz"] * s["fftlen"] for s in subs[:sub])
+        n = subs[sub]["fftlen"]
+        out = np.zeros((len(rows), n), dtype=np.complex64)
+        for i, r in enumerate(rows):
+            _check(lib().jerk_copy_to_host(out[i].ctypes.data, self.ptr.value + 8 * (off + r * n),
+                                           8 * n))
+        return out
 
 
 def _spectrum_arg(spectrum):
@@ -234,6 +299,24 @@ class JerkPlan:
         lib().jerk_free(C.cast(hits.keys, C.c_void_p))
         lib().jerk_free(C.cast(hits.powers, C.c_void_p))
         return cands, k, p
+
+    def set_profiling(self, on: bool) -> None:
+        _check(lib().jerk_plan_set_profiling(self._p, int(on)))
+
+    def reset_stats(self) -> None:
+        lib().jerk_plan_reset_stats(self._p)
+
+    def kernel_stats(self) -> dict:
+        n = lib().jerk_plan_kernel_stats(self._p, 0, None)
+        arr = (KernelStat * max(n, 1))()
+        lib().jerk_plan_kernel_stats(self._p, n, arr)
+        return {a.name.decode(): {"launches": a.launches, "ms": a.ms, "bytes": a.bytes,
+                                  "flops": a.flops} for a in arr[:n]}
+
+    def transfer_stats(self) -> Tuple[int, int]:
+        h, d = C.c_longlong(0), C.c_longlong(0)
+        lib().jerk_plan_transfer_stats(self._p, C.byref(h), C.byref(d))
+        return h.value, d.value
 
     def volume(self, spectrum, rstep: int, sub: int):
         """ffdot volume [numw][numz][numrs] of one (rstep, subharmonic)."""

@@ -134,3 +134,41 @@ def paper_pulsars(seed: int = 2025) -> List[Pulsar]:
     """Four pulsars: f~U(5,500) Hz, 1-8 harmonics, z~U(-180,180),
     w~U(-280,280), SNR~U(6,20)."""
     return random_pulsars(np.random.default_rng(seed), 4)
+
+
+# --------------------------------------------------------------------------
+# The same construction with torch on any device (the benchmark builds its
+# 2^25-sample spectra on the GPU; numpy would take tens of seconds each).
+
+def timeseries_torch(N: int, dt: float, pulsars: Sequence[Pulsar], seed: int, device="cuda"):
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    x = torch.randn(N, generator=g, device=device, dtype=torch.float64)
+    T = N * dt
+    u = torch.arange(N, device=device, dtype=torch.float64) / N
+    for p in pulsars:
+        r = p.f * T
+        r0 = r - 0.5 * p.z + p.w / 12.0
+        z0 = p.z - 0.5 * p.w
+        k = np.arange(1, p.nharm + 1, dtype=np.float64)
+        amps = 1.0 / k
+        amps = amps * (p.snr / np.sqrt(np.sum(amps ** 2) * N / 4.0))
+        phi = u * (r0 + u * (0.5 * z0 + u * (p.w / 6.0)))
+        for kk, a in zip(k, amps):
+            cyc = kk * phi
+            cyc = cyc - torch.floor(cyc)
+            x += float(a) * torch.cos(2.0 * np.pi * cyc + p.phase)
+    return x.float()
+
+
+def presto_fft_torch(ts):
+    """PRESTO-packed real FFT of a torch series: complex64 tensor of N/2 bins."""
+    import torch
+
+    N = ts.shape[0]
+    X = torch.fft.rfft(ts.double())
+    out = X[: N // 2].to(torch.complex64).clone()
+    out[0] = torch.complex(X[0].real, X[N // 2].real).to(torch.complex64)
+    return out
