@@ -35,7 +35,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     deps.append(os.path.abspath(__file__))
     if not force and not _stale(target, deps):
         return target
-    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+    cmd = [NVCC, "-O3", "-std=c++17", "--expt-relaxed-constexpr", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
            "-I" + os.path.join(ROOT, "include"), "-o", target]
     for f in SOURCES:
         p = os.path.join(CSRC, f)

@@ -230,12 +230,13 @@ __global__ void __launch_bounds__(FftPlan<N>::T)
 {
     constexpr int R0 = FftPlan<N>::R0;
     constexpr int T = FftPlan<N>::T;
+    constexpr int TWN = FftPlan<N>::twsize();
     extern __shared__ float2 smb[];
-    float2 *buf = smb, *tw = smb + N;
+    float2 *buf = smb, *tw = smb + fft_buf_len<N>();
     const int tid = threadIdx.x;
     const BankRow R = rows[first + blockIdx.x];
     float2 *row = bank + R.off;
-    for (int i = tid; i < N; i += T)
+    for (int i = tid; i < TWN; i += T)
         tw[i] = twiddles[twoff + i];
     __syncthreads();
     auto in = [&](int r) -> float2 { return row[tid + r * (N / R0)]; };
@@ -247,7 +248,7 @@ template <int N>
 static cudaError_t launch_bank_fft(const BankRow *rows, int first, int count, const float2 *tw,
                                    int twoff, float2 *bank, cudaStream_t st)
 {
-    const size_t smem = sizeof(float2) * 2 * N;
+    const size_t smem = sizeof(float2) * (fft_buf_len<N>() + FftPlan<N>::twsize());
     cudaError_t e = cudaFuncSetAttribute(bank_fft_kernel<N>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)

@@ -123,6 +123,12 @@ template <int SIGN> struct Dft<5, SIGN> {
 };
 
 // Radix plans: the first radix fixes the thread count T = N / R0.
+//
+// Twiddles live in per-stage tables: stage s >= 1 (Ns = product of the
+// earlier radices, radix R) has Ns * R entries W_{Ns R}^(r k) at [r * Ns + k],
+// so the lanes of a warp (consecutive k = j % Ns) read consecutive entries.
+// Shared buffers are padded by one float2 every 8 (pad() below), which makes
+// the strided writes of the early stages conflict-free.
 template <int N> struct FftPlan;
 #define JERK_FFT_PLAN(NN, ...)                                                  \
     template <> struct FftPlan<NN> {                                            \
@@ -130,6 +136,17 @@ template <int N> struct FftPlan;
         static constexpr int nstages = sizeof(radices) / sizeof(int);           \
         static constexpr int R0 = radices[0];                                   \
         static constexpr int T = NN / R0;                                       \
+        /* offset of stage s's table; twsize() is the total */                  \
+        static constexpr int twoff(int stage)               \
+        {                                                                       \
+            int off = 0, ns = radices[0];                                       \
+            for (int t = 1; t < stage; t++) {                                   \
+                off += ns * radices[t];                                         \
+                ns *= radices[t];                                               \
+            }                                                                   \
+            return off;                                                         \
+        }                                                                       \
+        static constexpr int twsize() { return twoff(nstages); } \
     };
 JERK_FFT_PLAN(128, 4, 8, 4)
 JERK_FFT_PLAN(192, 4, 4, 4, 3)
@@ -152,6 +169,11 @@ __device__ __forceinline__ float2 twiddle(const float2 *tw, int m)
     return SIGN > 0 ? make_float2(w.x, -w.y) : w;
 }
 
+// padded shared-buffer index and size
+__host__ __device__ __forceinline__ constexpr int pad(int i) { return i + (i >> 3); }
+template <int N>
+__host__ __device__ constexpr int fft_buf_len() { return N + N / 8; }
+
 // One middle stage, in place in buf.  Every thread of the block must call it
 // (it holds two barriers); only threads with act == true (tid < T) work.
 template <int N, int SIGN, int T, int Ns, int R>
@@ -167,7 +189,7 @@ __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw,
             if (NB % T == 0 || j < NB) {
 #pragma unroll
                 for (int r = 0; r < R; r++)
-                    v[p][r] = buf[j + r * NB];
+                    v[p][r] = buf[pad(j + r * NB)];
             }
         }
     }
@@ -181,13 +203,13 @@ __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw,
                 if (Ns > 1) {
 #pragma unroll
                     for (int r = 1; r < R; r++)
-                        v[p][r] = cmul(v[p][r], twiddle<SIGN>(tw, r * k * (N / (Ns * R))));
+                        v[p][r] = cmul(v[p][r], twiddle<SIGN>(tw, r * Ns + k));
                 }
                 Dft<R, SIGN>::run(v[p]);
                 const int idxD = (j / Ns) * Ns * R + k;
 #pragma unroll
                 for (int r = 0; r < R; r++)
-                    buf[idxD + r * Ns] = v[p][r];
+                    buf[pad(idxD + r * Ns)] = v[p][r];
             }
         }
     }
@@ -212,10 +234,10 @@ __device__ __forceinline__ void fft_stage_last(const float2 *buf, const float2 *
             float2 v[R];
 #pragma unroll
             for (int r = 0; r < R; r++)
-                v[r] = buf[j + r * NB];
+                v[r] = buf[pad(j + r * NB)];
 #pragma unroll
             for (int r = 1; r < R; r++)
-                v[r] = cmul(v[r], twiddle<SIGN>(tw, r * j * (N / (Ns * R))));
+                v[r] = cmul(v[r], twiddle<SIGN>(tw, r * Ns + j));
             Dft<R, SIGN>::run(v);
 #pragma unroll
             for (int r = 0; r < R; r++)
@@ -235,7 +257,8 @@ struct FftTail<N, SIGN, T, I, Ns, true> {
                                                Out &out)
     {
         constexpr int R = FftPlan<N>::radices[I];
-        fft_stage_last<N, SIGN, T, Ns, R>(buf, tw, tid, act, out);
+        constexpr int OFF = FftPlan<N>::twoff(I);
+        fft_stage_last<N, SIGN, T, Ns, R>(buf, tw + OFF, tid, act, out);
     }
 };
 
@@ -246,7 +269,8 @@ struct FftTail<N, SIGN, T, I, Ns, false> {
                                                Out &out)
     {
         constexpr int R = FftPlan<N>::radices[I];
-        fft_stage_inplace<N, SIGN, T, Ns, R>(buf, tw, tid, act);
+        constexpr int OFF = FftPlan<N>::twoff(I);
+        fft_stage_inplace<N, SIGN, T, Ns, R>(buf, tw + OFF, tid, act);
         FftTail<N, SIGN, T, I + 1, Ns * R>::run(buf, tw, tid, act, out);
     }
 };
@@ -257,7 +281,8 @@ struct FftTail<N, SIGN, T, I, Ns, false> {
 // must call it (barriers); threads with tid >= T do no work.  buf[N] is
 // shared memory.  When it returns, outputs have been handed to out(m, y) by
 // the threads that computed them; the caller must __syncthreads() before
-// buf is written again.
+// buf is written again.  buf holds fft_buf_len<N>() float2; tw holds the
+// per-stage tables of FftPlan<N> (fft_stage_twiddles on the host).
 template <int N, int SIGN, class In, class Out>
 __device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid, In &in,
                                           Out &out)
@@ -274,10 +299,30 @@ __device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid
         Dft<R0, SIGN>::run(v);
 #pragma unroll
         for (int r = 0; r < R0; r++)
-            buf[tid * R0 + r] = v[r];
+            buf[pad(tid * R0 + r)] = v[r];
     }
     __syncthreads();
     FftTail<N, SIGN, T, 1, R0>::run(buf, tw, tid, act, out);
+}
+
+// Host: the per-stage twiddle tables of FftPlan<N>, forward sign, computed
+// in double and rounded to float.
+template <int N>
+inline void fft_stage_twiddles(float2 *out)
+{
+    using P = FftPlan<N>;
+    int ns = P::radices[0];
+    for (int s = 1; s < P::nstages; s++) {
+        const int R = P::radices[s];
+        float2 *t = out + P::twoff(s);
+        for (int r = 0; r < R; r++)
+            for (int k = 0; k < ns; k++) {
+                const double a = -2.0 * 3.14159265358979323846264338327950288 * (double)(r * k) /
+                                 (double)(ns * R);
+                t[r * ns + k] = make_float2((float)cos(a), (float)sin(a));
+            }
+        ns *= R;
+    }
 }
 
 }  // namespace jerk

@@ -69,13 +69,14 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
     constexpr int R0 = FftPlan<N>::R0;
     const SubDev sd = P.subs[s];
     const StepDev st = P.steps[(P.first_rstep + b) * P.nsubs + s];
+    constexpr int TWN = FftPlan<N>::twsize();
     float2 *buf = reinterpret_cast<float2 *>(smem);
-    float2 *tw = buf + N;
-    float2 *data = tw + N;
+    float2 *tw = buf + fft_buf_len<N>();
+    float2 *data = tw + TWN;
     float *keys = reinterpret_cast<float *>(data + M);
     const int tid = threadIdx.x, nt = blockDim.x;
 
-    for (int i = tid; i < N; i += nt)
+    for (int i = tid; i < TWN; i += nt)
         tw[i] = P.twiddles[sd.twoff + i];
 
     // get_fourier_amplitudes: M bins from lobin, zero outside the file
@@ -181,9 +182,10 @@ __global__ void __launch_bounds__(FftPlan<N>::T) corr_kernel(const SearchDev P, 
 {
     constexpr int R0 = FftPlan<N>::R0;
     constexpr int T = FftPlan<N>::T;
+    constexpr int TWN = FftPlan<N>::twsize();
     extern __shared__ float2 sm2[];
     float2 *buf = sm2;
-    float2 *tw = sm2 + N;
+    float2 *tw = sm2 + fft_buf_len<N>();
     const int tid = threadIdx.x;
     const int row = blockIdx.x;
     int gi = 0;
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(FftPlan<N>::T) corr_kernel(const SearchDev P, 
     const int lrow = row - G.rowstart[gi];
     const SubDev sd = P.subs[s];
 
-    for (int i = tid; i < N; i += T)
+    for (int i = tid; i < TWN; i += T)
         tw[i] = P.twiddles[sd.twoff + i];
 
     // the kernel row, in the order this thread's first-stage butterfly reads it
@@ -305,13 +307,47 @@ __global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P
 // ---------------------------------------------------------------------------
 // Launchers (host side of this translation unit).
 
+template <int N>
+static size_t prep_bytes_n()
+{
+    constexpr int M = N / 2;
+    return sizeof(float2) * (size_t)(fft_buf_len<N>() + FftPlan<N>::twsize() + M) +
+           sizeof(float) * (size_t)NextPow2<M>::value;
+}
+
 size_t prep_smem_bytes(int maxfft)
 {
-    const int M = maxfft / 2;
-    int MP = 1;
-    while (MP < M)
-        MP <<= 1;
-    return sizeof(float2) * (size_t)(2 * maxfft + M) + sizeof(float) * (size_t)MP;
+    size_t b = 0;
+#define JERK_PB(NN)                                  \
+    if (NN <= maxfft && prep_bytes_n<NN>() > b)      \
+        b = prep_bytes_n<NN>();
+    JERK_PB(128) JERK_PB(192) JERK_PB(256) JERK_PB(384) JERK_PB(512) JERK_PB(768)
+    JERK_PB(1024) JERK_PB(1280) JERK_PB(2048) JERK_PB(4096) JERK_PB(5120) JERK_PB(7680)
+#undef JERK_PB
+    return b;
+}
+
+// twiddle tables of every supported fftlen's plan (host)
+int fft_twiddle_size(int N)
+{
+    switch (N) {
+#define JERK_TS(NN) case NN: return FftPlan<NN>::twsize();
+    JERK_TS(128) JERK_TS(192) JERK_TS(256) JERK_TS(384) JERK_TS(512) JERK_TS(768)
+    JERK_TS(1024) JERK_TS(1280) JERK_TS(2048) JERK_TS(4096) JERK_TS(5120) JERK_TS(7680)
+#undef JERK_TS
+    default: return -1;
+    }
+}
+
+void fft_twiddle_table(int N, float2 *out)
+{
+    switch (N) {
+#define JERK_TT(NN) case NN: fft_stage_twiddles<NN>(out); break;
+    JERK_TT(128) JERK_TT(192) JERK_TT(256) JERK_TT(384) JERK_TT(512) JERK_TT(768)
+    JERK_TT(1024) JERK_TT(1280) JERK_TT(2048) JERK_TT(4096) JERK_TT(5120) JERK_TT(7680)
+#undef JERK_TT
+    default: break;
+    }
 }
 
 int prep_threads(int maxfft)
@@ -341,7 +377,7 @@ cudaError_t launch_prep(const SearchDev &P, int maxfft, cudaStream_t st)
 template <int N>
 static cudaError_t launch_corr_n(const SearchDev &P, const RowGroup &G, int rows, cudaStream_t st)
 {
-    const size_t smem = sizeof(float2) * 2 * N;
+    const size_t smem = sizeof(float2) * (fft_buf_len<N>() + FftPlan<N>::twsize());
     cudaError_t e = cudaFuncSetAttribute(corr_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess)

@@ -27,6 +27,8 @@ cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int r
                         cudaStream_t st);
 cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st);
 bool fftlen_supported(int n);
+int fft_twiddle_size(int N);
+void fft_twiddle_table(int N, float2 *out);
 cudaError_t launch_bank_response(const BankRow *rows, int nrows, int max_pts, float2 *bank,
                                  cudaStream_t st);
 cudaError_t launch_bank_fft_any(int N, const BankRow *rows, int first, int count, const float2 *tw,
@@ -556,14 +558,13 @@ extern "C" long long jerk_insert_hits(const jerk_cand *hits, long long nhits, je
 }
 
 // ---------------------------------------------------------------------------
-// twiddle tables exp(-2 pi i m / N), computed in double
+// the per-stage twiddle tables of fftlen N's FFT plan (jerk_fft.cuh)
 
 static void append_twiddles(int N, std::vector<float2> &tw)
 {
-    for (int m = 0; m < N; m++) {
-        const double a = -2.0 * M_PI * (double)m / (double)N;
-        tw.push_back(make_float2((float)cos(a), (float)sin(a)));
-    }
+    const size_t at = tw.size();
+    tw.resize(at + fft_twiddle_size(N));
+    fft_twiddle_table(N, tw.data() + at);
 }
 
 // ---------------------------------------------------------------------------
@@ -988,7 +989,7 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
         d.pownorm = (float)(1.0 / (double)(sh.fftlen * sh.fftlen));
         if (!twoff.count(sh.fftlen)) {
             twoff[sh.fftlen] = twtotal;
-            twtotal += sh.fftlen;
+            twtotal += fft_twiddle_size(sh.fftlen);
         }
         d.twoff = twoff[sh.fftlen];
         d.kern_off = kern_off;

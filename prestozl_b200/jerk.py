@@ -222,7 +222,7 @@ class DeviceBank:
         n = subs[sub]["fftlen"]
         out = np.zeros((len(rows), n), dtype=np.complex64)
         for i, r in enumerate(rows):
-            _check(lib().jerk_copy_to_host(out[i].ctypes.data, self.ptr.value + 8 * (off + r * n),
+            _check(lib().jerk_copy_to_host(out[i].ctypes.data, self.ptr.value + 8 * (off + int(r) * n),
                                            8 * n))
         return out
 
