@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 REF_LIB = os.path.join(REF_DIR, "libprestoref.so")
 REF_CLI = os.path.join(REF_DIR, "accelsearch")
+DROPIN_CLI = os.path.join(REF_DIR, "accelsearch_b200")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REFERENCE_SOURCES = "/root/reference"
 
@@ -32,7 +33,7 @@ def build(reference: Optional[bool] = None) -> None:
     reference sources are present)."""
     if reference is None:
         reference = os.path.isdir(os.path.join(REFERENCE_SOURCES, "src"))
-    targets = ["oracle"] + (["ref"] if reference else [])
+    targets = ["oracle"] + (["ref", "dropin"] if reference else [])
     subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
 
 

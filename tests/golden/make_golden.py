@@ -12,6 +12,8 @@ drives them on seeded synthetic inputs and stores small results:
                          the reference for the benchmark's search parameters.
 * ``sigma.json``         candidate_sigma / power_for_sigma on a grid.
 * ``kernels_small.npz``  a few response-kernel FFTs of the small search's bank.
+* ``small_ACCEL.txt``    the reference CLI's ACCEL output for the small search
+                         (after its sort / harmonic removal / optimisation).
 
 Run from the repository root after ``make -C oracle``:
 
@@ -90,6 +92,19 @@ def small_cands(tmp: str) -> dict:
     return out
 
 
+def accel_small(tmp: str) -> None:
+    import shutil
+    import subprocess
+
+    spec, N, dt = synth.small_spectrum()
+    root = os.path.join(tmp, "small")
+    synth.write_fft(root, spec, N, dt)
+    env = dict(os.environ, PRESTO=tmp, OMP_NUM_THREADS="1")
+    subprocess.run([ob.REF_CLI, *SMALL_ARGS, "small.fft"], cwd=tmp, env=env, check=True,
+                   stdout=subprocess.DEVNULL)
+    shutil.copy(os.path.join(tmp, "small_ACCEL_20_JERK_60"), os.path.join(HERE, "small_ACCEL.txt"))
+
+
 def sizing(tmp: str) -> list:
     # geometry does not depend on the data: a short white-noise file will do
     N, dt = 1 << 18, 54.6e-6
@@ -132,6 +147,8 @@ def main() -> None:
             json.dump(small_cands(tmp), f, indent=1)
         with open(os.path.join(HERE, "sizing.json"), "w") as f:
             json.dump(sizing(tmp), f, indent=1)
+    with tempfile.TemporaryDirectory() as tmp:
+        accel_small(tmp)
     with open(os.path.join(HERE, "sigma.json"), "w") as f:
         json.dump(sigma_grid(), f, indent=1)
 
