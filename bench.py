@@ -217,6 +217,9 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0)
+    ap.add_argument("--rsteps", type=int, default=0,
+                    help="search only the first R rsteps of each spectrum (profiling runs; "
+                         "the line is then marked partial)")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -252,8 +255,10 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    nsearch = args.rsteps if args.rsteps > 0 else 0
+
     for i in range(args.warmup):
-        plan.search(specs[i % 2])
+        plan.search(specs[i % 2], 0, nsearch)
     torch.cuda.synchronize()
 
     plan.reset_stats()
@@ -268,7 +273,7 @@ def main():
     for i in range(args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        c = plan.search(specs[i % 2])
+        c = plan.search(specs[i % 2], 0, nsearch)
         e1.record()
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
@@ -297,7 +302,7 @@ def main():
     e2e_ms = []
     for i in range(e2e_steps):
         t0 = time.perf_counter()
-        plan.search(hnp[i % 2])
+        plan.search(hnp[i % 2], 0, nsearch)
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - t0) * 1000.0)
     h2d, d2h = plan.transfer_stats()
@@ -323,7 +328,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "numbins": N_SAMPLES // 2,
+            "config": {"workload": WORKLOAD if not nsearch else
+                       f"{WORKLOAD} (PARTIAL: first {nsearch} rsteps per spectrum)",
+                       "numbins": N_SAMPLES // 2,
                        "rsteps_per_spectrum": nrsteps, "batch_rsteps": args.batch,
                        "form": "plain (one spectrum per search call)",
                        "l2": "inputs larger than L2 (128 MiB spectrum, ~GB volumes per batch)",
@@ -347,7 +354,7 @@ def main():
             "wall_s": wall,
             "candidates_per_spectrum": ncands,
         }
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and not nsearch:
             try:
                 from oracle import bindings as ob
                 if ob.have_reference():

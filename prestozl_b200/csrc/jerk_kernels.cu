@@ -228,13 +228,45 @@ __global__ void __launch_bounds__(FftPlan<N>::T) corr_kernel(const SearchDev P, 
 // 3. Harmonic summing + threshold + compaction.
 
 constexpr int kHarmThreads = 256;
+constexpr int kHarmZ = 4;  // fundamental z rows in flight per thread
+
+// Warp-aggregated append of one hit per lane with hit == true.
+__device__ __forceinline__ void record_hits(const SearchDev &P, bool hit, int lane,
+                                            unsigned long long key, float v)
+{
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (!mask)
+        return;
+    const int leader = __ffs(mask) - 1;
+    unsigned int base = 0;
+    if (lane == leader)
+        base = atomicAdd(P.hit_count, (unsigned int)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (hit) {
+        const unsigned long long idx = base + __popc(mask & ((1u << lane) - 1u));
+        if ((long long)idx < P.max_hits) {
+            P.hit_keys[idx] = key;
+            P.hit_pows[idx] = v;
+        }
+    }
+}
+
+// Shared memory (dynamic): zrow[s][jj] = zinds_s[jj] * stride_s (the row
+// offset inside subharmonic s's volume for fundamental z row jj), then
+// rind[s][tid] (the subharmonic r index of this thread's fundamental r).
+size_t harmsum_smem_bytes(int nsubs, int numz0)
+{
+    return sizeof(int) * (size_t)nsubs * numz0 + sizeof(uint16_t) * (size_t)nsubs * kHarmThreads;
+}
 
 __global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P)
 {
-    __shared__ uint16_t s_rind[kMaxSubs][kHarmThreads];
+    extern __shared__ int hsm[];
     __shared__ long long s_base[kMaxSubs];
-    __shared__ int s_stride[kMaxSubs];
     __shared__ int s_numrs[kMaxSubs];
+    const int nsubs = P.nsubs, numz0 = P.numz0;
+    int *s_zrow = hsm;
+    uint16_t *s_rind = reinterpret_cast<uint16_t *>(hsm + nsubs * numz0);
     const int b = blockIdx.z;
     const int ii = blockIdx.y;
     const int tid = threadIdx.x;
@@ -243,61 +275,65 @@ __global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P
     const int lane = tid & 31;
     const long long rstep = P.first_rstep + b;
 
-    if (tid < P.nsubs) {
+    if (tid < nsubs) {
         const SubDev sd = P.subs[tid];
         const int wind = tid == 0 ? ii : P.wind[sd.wind_off + ii];
         s_base[tid] = sd.plane_off + (long long)b * sd.plane_size +
                       (long long)wind * sd.numz * sd.stride;
-        s_stride[tid] = sd.stride;
-        s_numrs[tid] = P.steps[rstep * P.nsubs + tid].numrs;
+        s_numrs[tid] = P.steps[rstep * nsubs + tid].numrs;
+    }
+    for (int i = tid; i < nsubs * numz0; i += kHarmThreads) {
+        const int s = i / numz0, jj = i - s * numz0;
+        const SubDev &sd = P.subs[s];
+        const int zi = s == 0 ? jj : P.zinds[sd.zinds_off + jj];
+        s_zrow[i] = zi * sd.stride;
     }
     __syncthreads();
-    for (int s = 1; s < P.nsubs; s++) {
-        uint16_t ri = valid ? P.rinds[((long long)b * P.nsubs + s) * P.corr_uselen + kk] : 0;
+    for (int s = 1; s < nsubs; s++) {
+        uint16_t ri = valid ? P.rinds[((long long)b * nsubs + s) * P.corr_uselen + kk] : 0;
         if (ri >= s_numrs[s]) {
             // cannot happen for tables built as the reference builds them;
             // record it and read a cell that exists
             atomicOr(P.status, 1u);
             ri = 0;
         }
-        s_rind[s][tid] = ri;
+        s_rind[s * kHarmThreads + tid] = ri;
     }
     __syncthreads();
 
-    const float *planes = P.planes;
-    const long long base0 = s_base[0];
-    const int stride0 = s_stride[0];
-    for (int jj = 0; jj < P.numz0; jj++) {
-        float v = valid ? planes[base0 + (long long)jj * stride0 + kk] : 0.0f;
+    const float *fund = P.planes + s_base[0] + (valid ? kk : 0);
+    const unsigned long long keybase =
+        (unsigned long long)rstep * P.nstages;  // * numw0 ... folded below
+    for (int jj0 = 0; jj0 < numz0; jj0 += kHarmZ) {
+        float v[kHarmZ];
+#pragma unroll
+        for (int u = 0; u < kHarmZ; u++) {
+            const int jj = jj0 + u;
+            v[u] = (valid && jj < numz0) ? fund[s_zrow[jj]] : 0.0f;
+        }
         int s = 1;
         for (int stage = 0; stage < P.nstages; stage++) {
             if (stage > 0) {
                 const int nadd = 1 << (stage - 1);
                 for (int h = 0; h < nadd; h++, s++) {
-                    const SubDev &sd = P.subs[s];
-                    const int zind = P.zinds[sd.zinds_off + jj];
-                    if (valid)
-                        v = __fadd_rn(v, planes[s_base[s] + (long long)zind * s_stride[s] +
-                                                s_rind[s][tid]]);
+                    const float *bp = P.planes + s_base[s] + s_rind[s * kHarmThreads + tid];
+                    const int *zr = s_zrow + s * numz0;
+#pragma unroll
+                    for (int u = 0; u < kHarmZ; u++) {
+                        const int jj = jj0 + u;
+                        if (jj < numz0)
+                            v[u] = __fadd_rn(v[u], bp[zr[jj]]);
+                    }
                 }
             }
-            const bool hit = valid && v > P.powcut[stage];
-            const unsigned mask = __ballot_sync(0xffffffffu, hit);
-            if (mask) {
-                const int leader = __ffs(mask) - 1;
-                unsigned int base = 0;
-                if (lane == leader)
-                    base = atomicAdd(P.hit_count, (unsigned int)__popc(mask));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (hit) {
-                    const unsigned long long idx = base + __popc(mask & ((1u << lane) - 1u));
-                    if ((long long)idx < P.max_hits) {
-                        const unsigned long long key =
-                            ((((unsigned long long)rstep * P.nstages + stage) * P.numw0 + ii) *
-                                 P.numz0 + jj) * P.corr_uselen + kk;
-                        P.hit_keys[idx] = key;
-                        P.hit_pows[idx] = v;
-                    }
+            const float cut = P.powcut[stage];
+#pragma unroll
+            for (int u = 0; u < kHarmZ; u++) {
+                const int jj = jj0 + u;
+                if (jj < numz0) {
+                    const unsigned long long key =
+                        (((keybase + stage) * P.numw0 + ii) * numz0 + jj) * P.corr_uselen + kk;
+                    record_hits(P, valid && v[u] > cut, lane, key, v[u]);
                 }
             }
         }
@@ -419,8 +455,13 @@ cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int r
 
 cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st)
 {
+    const size_t smem = harmsum_smem_bytes(P.nsubs, P.numz0);
+    cudaError_t e = cudaFuncSetAttribute(harmsum_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
     const dim3 grid((P.corr_uselen + kHarmThreads - 1) / kHarmThreads, P.numw0, P.nb);
-    harmsum_kernel<<<grid, kHarmThreads, 0, st>>>(P);
+    harmsum_kernel<<<grid, kHarmThreads, smem, st>>>(P);
     return cudaGetLastError();
 }
 
