@@ -251,22 +251,31 @@ __device__ __forceinline__ void record_hits(const SearchDev &P, bool hit, int la
     }
 }
 
-// Shared memory (dynamic): zrow[s][jj] = zinds_s[jj] * stride_s (the row
-// offset inside subharmonic s's volume for fundamental z row jj), then
-// rind[s][tid] (the subharmonic r index of this thread's fundamental r).
+// Shared memory (dynamic): zrow[s][jj] = zinds_s[jj] * stride_s, the row
+// offset inside subharmonic s's volume for fundamental z row jj; rows are
+// padded to a multiple of 4 entries so four rows load as one int4.
+__host__ __device__ __forceinline__ int zrow_pitch(int numz0) { return (numz0 + 3) & ~3; }
+
 size_t harmsum_smem_bytes(int nsubs, int numz0)
 {
-    return sizeof(int) * (size_t)nsubs * numz0 + sizeof(uint16_t) * (size_t)nsubs * kHarmThreads;
+    return sizeof(int) * (size_t)nsubs * zrow_pitch(numz0);
 }
 
+// Thread = one fundamental r (kk) of one w row (ii) of one rstep (b); it
+// walks all z rows four at a time.  Per point the float adds run in the
+// reference's order: stage 1 adds 1/2, stage 2 adds 1/4 then 3/4, ...
+// (src/accel_utils.c:1356-1377 applied stage by stage); after each stage the
+// value is compared with that stage's cutoff.  Offsets are 32-bit (the
+// batch's volumes hold fewer than 2^32 floats; checked on the host).
+template <int S>
 __global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P)
 {
+    constexpr int NS = 1 << (S - 1);
     extern __shared__ int hsm[];
-    __shared__ long long s_base[kMaxSubs];
-    __shared__ int s_numrs[kMaxSubs];
-    const int nsubs = P.nsubs, numz0 = P.numz0;
-    int *s_zrow = hsm;
-    uint16_t *s_rind = reinterpret_cast<uint16_t *>(hsm + nsubs * numz0);
+    __shared__ unsigned int s_base[NS];
+    __shared__ int s_numrs[NS];
+    const int numz0 = P.numz0;
+    const int pitch = zrow_pitch(numz0);
     const int b = blockIdx.z;
     const int ii = blockIdx.y;
     const int tid = threadIdx.x;
@@ -275,65 +284,74 @@ __global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P
     const int lane = tid & 31;
     const long long rstep = P.first_rstep + b;
 
-    if (tid < nsubs) {
+    if (tid < NS) {
         const SubDev sd = P.subs[tid];
         const int wind = tid == 0 ? ii : P.wind[sd.wind_off + ii];
-        s_base[tid] = sd.plane_off + (long long)b * sd.plane_size +
-                      (long long)wind * sd.numz * sd.stride;
-        s_numrs[tid] = P.steps[rstep * nsubs + tid].numrs;
+        s_base[tid] = (unsigned int)(sd.plane_off + (long long)b * sd.plane_size +
+                                     (long long)wind * sd.numz * sd.stride);
+        s_numrs[tid] = P.steps[rstep * NS + tid].numrs;
     }
-    for (int i = tid; i < nsubs * numz0; i += kHarmThreads) {
-        const int s = i / numz0, jj = i - s * numz0;
+    for (int i = tid; i < NS * pitch; i += kHarmThreads) {
+        const int s = i / pitch, jj = i - s * pitch;
         const SubDev &sd = P.subs[s];
-        const int zi = s == 0 ? jj : P.zinds[sd.zinds_off + jj];
-        s_zrow[i] = zi * sd.stride;
+        int zi = 0;
+        if (jj < numz0)
+            zi = s == 0 ? jj : P.zinds[sd.zinds_off + jj];
+        hsm[i] = zi * sd.stride;
     }
     __syncthreads();
-    for (int s = 1; s < nsubs; s++) {
-        uint16_t ri = valid ? P.rinds[((long long)b * nsubs + s) * P.corr_uselen + kk] : 0;
-        if (ri >= s_numrs[s]) {
+
+    // per-thread offsets: volume row base + this thread's r index
+    unsigned int off[NS];
+    off[0] = s_base[0] + (valid ? kk : 0);
+#pragma unroll
+    for (int s = 1; s < NS; s++) {
+        unsigned int ri = valid ? P.rinds[((long long)b * NS + s) * P.corr_uselen + kk] : 0u;
+        if (ri >= (unsigned int)s_numrs[s]) {
             // cannot happen for tables built as the reference builds them;
             // record it and read a cell that exists
             atomicOr(P.status, 1u);
             ri = 0;
         }
-        s_rind[s * kHarmThreads + tid] = ri;
+        off[s] = s_base[s] + ri;
     }
-    __syncthreads();
-
-    const float *fund = P.planes + s_base[0] + (valid ? kk : 0);
-    const unsigned long long keybase =
-        (unsigned long long)rstep * P.nstages;  // * numw0 ... folded below
-    for (int jj0 = 0; jj0 < numz0; jj0 += kHarmZ) {
-        float v[kHarmZ];
+    float cut[S];
 #pragma unroll
-        for (int u = 0; u < kHarmZ; u++) {
-            const int jj = jj0 + u;
-            v[u] = (valid && jj < numz0) ? fund[s_zrow[jj]] : 0.0f;
+    for (int st = 0; st < S; st++)
+        cut[st] = P.powcut[st];
+
+    const float *planes = P.planes;
+    for (int jj0 = 0; jj0 < numz0; jj0 += kHarmZ) {
+        const bool full = jj0 + kHarmZ <= numz0;
+        float v[kHarmZ];
+        {
+            const int4 z = *reinterpret_cast<const int4 *>(hsm + jj0);
+            v[0] = planes[off[0] + z.x];
+            v[1] = planes[off[0] + z.y];
+            v[2] = planes[off[0] + z.z];
+            v[3] = planes[off[0] + z.w];
         }
         int s = 1;
-        for (int stage = 0; stage < P.nstages; stage++) {
-            if (stage > 0) {
-                const int nadd = 1 << (stage - 1);
-                for (int h = 0; h < nadd; h++, s++) {
-                    const float *bp = P.planes + s_base[s] + s_rind[s * kHarmThreads + tid];
-                    const int *zr = s_zrow + s * numz0;
 #pragma unroll
-                    for (int u = 0; u < kHarmZ; u++) {
-                        const int jj = jj0 + u;
-                        if (jj < numz0)
-                            v[u] = __fadd_rn(v[u], bp[zr[jj]]);
-                    }
+        for (int stage = 0; stage < S; stage++) {
+            if (stage > 0) {
+#pragma unroll
+                for (int h = 0; h < (1 << (stage - 1)); h++, s++) {
+                    const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
+                    v[0] = __fadd_rn(v[0], planes[off[s] + z.x]);
+                    v[1] = __fadd_rn(v[1], planes[off[s] + z.y]);
+                    v[2] = __fadd_rn(v[2], planes[off[s] + z.z]);
+                    v[3] = __fadd_rn(v[3], planes[off[s] + z.w]);
                 }
             }
-            const float cut = P.powcut[stage];
 #pragma unroll
             for (int u = 0; u < kHarmZ; u++) {
-                const int jj = jj0 + u;
-                if (jj < numz0) {
+                const bool hit = valid && (full || jj0 + u < numz0) && v[u] > cut[stage];
+                if (__any_sync(0xffffffffu, hit)) {
                     const unsigned long long key =
-                        (((keybase + stage) * P.numw0 + ii) * numz0 + jj) * P.corr_uselen + kk;
-                    record_hits(P, valid && v[u] > cut, lane, key, v[u]);
+                        ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) * numz0 +
+                         (jj0 + u)) * P.corr_uselen + kk;
+                    record_hits(P, hit, lane, key, v[u]);
                 }
             }
         }
@@ -453,16 +471,30 @@ cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int r
     }
 }
 
-cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st)
+template <int S>
+static cudaError_t launch_harmsum_s(const SearchDev &P, cudaStream_t st)
 {
     const size_t smem = harmsum_smem_bytes(P.nsubs, P.numz0);
-    cudaError_t e = cudaFuncSetAttribute(harmsum_kernel,
+    cudaError_t e = cudaFuncSetAttribute(harmsum_kernel<S>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
     const dim3 grid((P.corr_uselen + kHarmThreads - 1) / kHarmThreads, P.numw0, P.nb);
-    harmsum_kernel<<<grid, kHarmThreads, smem, st>>>(P);
+    harmsum_kernel<S><<<grid, kHarmThreads, smem, st>>>(P);
     return cudaGetLastError();
+}
+
+cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st)
+{
+    switch (P.nstages) {
+    case 1: return launch_harmsum_s<1>(P, st);
+    case 2: return launch_harmsum_s<2>(P, st);
+    case 3: return launch_harmsum_s<3>(P, st);
+    case 4: return launch_harmsum_s<4>(P, st);
+    case 5: return launch_harmsum_s<5>(P, st);
+    case 6: return launch_harmsum_s<6>(P, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace jerk

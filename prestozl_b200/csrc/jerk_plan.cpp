@@ -1025,6 +1025,8 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     }
     p->plane_floats = plane_off;
     p->prepped_f2 = data_off;
+    if (plane_off >= (1LL << 32))
+        return bail(fail(JERK_EINVAL, "ffdot volumes of one batch exceed 2^32 floats: lower batch_rsteps"));
 
     // twiddles: exp(-2 pi i m / N), double on the host
     std::vector<float2> tw;
