@@ -87,6 +87,46 @@ template <int SIGN> struct Dft<8, SIGN> {
     }
 };
 
+// 16 = 4 x 4: DFT4 over n1 for each n2, twiddle W16^(n2 k1), DFT4 over n2.
+template <int SIGN> struct Dft<16, SIGN> {
+    __device__ __forceinline__ static float2 w16(float2 a, int m)
+    {
+        const float c1 = 0.92387953251128675613f;  // cos(pi/8)
+        const float s1 = 0.38268343236508977173f;  // sin(pi/8)
+        const float h = 0.70710678118654752440f;
+        switch (m) {
+        case 0: return a;
+        case 1: return cmul(a, make_float2(c1, SIGN * s1));
+        case 2: return make_float2(h * (a.x - SIGN * a.y), h * (a.y + SIGN * a.x));
+        case 3: return cmul(a, make_float2(s1, SIGN * c1));
+        case 4: return mul_si<SIGN>(a);
+        case 6: return make_float2(h * (-a.x - SIGN * a.y), h * (-a.y + SIGN * a.x));
+        case 9: return cmul(a, make_float2(-c1, -SIGN * s1));
+        default: return a;  // unreachable for n2, k1 in [0, 4)
+        }
+    }
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        float2 a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; n2++) {
+            float2 t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
+            Dft<4, SIGN>::run(t);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; k1++)
+                a[n2][k1] = w16(t[k1], n2 * k1);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 4; k1++) {
+            float2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            Dft<4, SIGN>::run(t);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; k2++)
+                v[k1 + 4 * k2] = t[k2];
+        }
+    }
+};
+
 template <int SIGN> struct Dft<3, SIGN> {
     __device__ __forceinline__ static void run(float2 *v)
     {
@@ -127,8 +167,6 @@ template <int SIGN> struct Dft<5, SIGN> {
 // Twiddles live in per-stage tables: stage s >= 1 (Ns = product of the
 // earlier radices, radix R) has Ns * R entries W_{Ns R}^(r k) at [r * Ns + k],
 // so the lanes of a warp (consecutive k = j % Ns) read consecutive entries.
-// Shared buffers are padded by one float2 every 8 (pad() below), which makes
-// the strided writes of the early stages conflict-free.
 template <int N> struct FftPlan;
 #define JERK_FFT_PLAN(NN, ...)                                                  \
     template <> struct FftPlan<NN> {                                            \
@@ -149,17 +187,17 @@ template <int N> struct FftPlan;
         static constexpr int twsize() { return twoff(nstages); } \
     };
 JERK_FFT_PLAN(128, 4, 8, 4)
-JERK_FFT_PLAN(192, 4, 4, 4, 3)
+JERK_FFT_PLAN(192, 4, 16, 3)
 JERK_FFT_PLAN(256, 8, 8, 4)
-JERK_FFT_PLAN(384, 8, 4, 4, 3)
-JERK_FFT_PLAN(512, 8, 8, 8)
-JERK_FFT_PLAN(768, 8, 8, 4, 3)
-JERK_FFT_PLAN(1024, 8, 8, 4, 4)
-JERK_FFT_PLAN(1280, 8, 8, 4, 5)
-JERK_FFT_PLAN(2048, 8, 8, 8, 4)
-JERK_FFT_PLAN(4096, 8, 8, 8, 8)
-JERK_FFT_PLAN(5120, 8, 8, 8, 2, 5)
-JERK_FFT_PLAN(7680, 8, 8, 8, 3, 5)
+JERK_FFT_PLAN(384, 8, 16, 3)
+JERK_FFT_PLAN(512, 8, 16, 4)
+JERK_FFT_PLAN(768, 16, 16, 3)
+JERK_FFT_PLAN(1024, 16, 16, 4)
+JERK_FFT_PLAN(1280, 16, 16, 5)
+JERK_FFT_PLAN(2048, 16, 16, 8)
+JERK_FFT_PLAN(4096, 16, 16, 16)
+JERK_FFT_PLAN(5120, 16, 16, 4, 5)
+JERK_FFT_PLAN(7680, 16, 16, 2, 3, 5)
 #undef JERK_FFT_PLAN
 
 template <int SIGN>
@@ -169,10 +207,13 @@ __device__ __forceinline__ float2 twiddle(const float2 *tw, int m)
     return SIGN > 0 ? make_float2(w.x, -w.y) : w;
 }
 
-// padded shared-buffer index and size
-__host__ __device__ __forceinline__ constexpr int pad(int i) { return i + (i >> 3); }
+// Shared-buffer index: the low 4 bits of the element index (one 16-element,
+// 128-byte row of banks) are XORed with the next 4 bits.  Contiguous runs of
+// 16 stay a permutation of one bank row, and the stride-R writes of the first
+// stage spread over all banks, so every stage's accesses are conflict-free.
+__host__ __device__ __forceinline__ constexpr int pad(int i) { return i ^ ((i >> 4) & 15); }
 template <int N>
-__host__ __device__ constexpr int fft_buf_len() { return N + N / 8; }
+__host__ __device__ constexpr int fft_buf_len() { return N; }
 
 // One middle stage, in place in buf.  Every thread of the block must call it
 // (it holds two barriers); only threads with act == true (tid < T) work.

@@ -177,8 +177,17 @@ __global__ void prep_kernel(const SearchDev P)
 // ---------------------------------------------------------------------------
 // 2. Correlation: one CTA per kernel row, all rsteps of the batch.
 
+// Occupancy target for corr_kernel: enough CTAs per SM that 128-thread CTAs
+// give 16 resident warps (registers are capped to fit).
 template <int N>
-__global__ void __launch_bounds__(FftPlan<N>::T) corr_kernel(const SearchDev P, const RowGroup G)
+struct CorrOcc {
+    static constexpr int T = FftPlan<N>::T;
+    static constexpr int value = T >= 512 ? 1 : (T >= 256 ? 2 : (T >= 128 ? 4 : 8));
+};
+
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
+    corr_kernel(const SearchDev P, const RowGroup G)
 {
     constexpr int R0 = FftPlan<N>::R0;
     constexpr int T = FftPlan<N>::T;
@@ -406,15 +415,15 @@ void fft_twiddle_table(int N, float2 *out)
 
 int prep_threads(int maxfft)
 {
-    // the widest FFT plan's thread count, at least a warp multiple of 128
-    int t = 128;
-    switch (maxfft) {
-    case 4096: t = FftPlan<4096>::T; break;
-    case 5120: t = FftPlan<5120>::T; break;
-    case 7680: t = FftPlan<7680>::T; break;
-    default: t = 256; break;
-    }
-    return t < 256 ? 256 : t;
+    // at least the widest FFT plan's thread count, and at least 256
+    int t = 256;
+#define JERK_PT(NN)                                  \
+    if (NN <= maxfft && FftPlan<NN>::T > t)          \
+        t = FftPlan<NN>::T;
+    JERK_PT(128) JERK_PT(192) JERK_PT(256) JERK_PT(384) JERK_PT(512) JERK_PT(768)
+    JERK_PT(1024) JERK_PT(1280) JERK_PT(2048) JERK_PT(4096) JERK_PT(5120) JERK_PT(7680)
+#undef JERK_PT
+    return (t + 31) / 32 * 32;
 }
 
 cudaError_t launch_prep(const SearchDev &P, int maxfft, cudaStream_t st)
