@@ -165,6 +165,25 @@ void jerk_device_free(void *p);
 int jerk_copy_to_host(void *dst, const void *device_src, long long bytes);
 int jerk_bank_generate(const jerk_subharm *subs, int nsubs, void *device_bank, void *stream);
 
+/* One subharmonic's ffdot volume for one rstep without allocating anything.
+ * No counterpart in the reference: it exists for callers that cannot
+ * allocate device memory when they search (memory handed out up front by a
+ * pool they do not own, real-time loops that forbid allocation after
+ * start-up).  All working memory is a fixed 192 KiB device array inside the
+ * library (fftlen <= 7680, corr_uselen <= 16384; larger sizes are rejected
+ * with JERK_EINVAL).  spectrum (numbins complex64, bin 0 = lobin), kernels
+ * (this subharmonic's [numw][numz][fftlen] rows) and volume
+ * ([numw][numz][numrs] floats, numrs <= corr_uselen + 8 is enough) are
+ * device pointers owned by the caller; fullrlo is the rstep's first
+ * fundamental r.  Asynchronous on stream (NULL = default stream).  The first
+ * call on each device looks the array up (cudaGetSymbolAddress): make it
+ * before any stream capture.  Calls share the array, so calls that overlap
+ * on the GPU race; serialise them. */
+int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
+                       const jerk_subharm *sub, const void *kernels, double fullrlo,
+                       int corr_uselen, float nph, float *volume, int *numrs, long long *rlo,
+                       void *stream);
+
 /* Statistics (host, double precision). */
 double jerk_candidate_sigma(double power, int numsum, double numtrials);
 double jerk_power_for_sigma(double sigma, int numsum, double numtrials);

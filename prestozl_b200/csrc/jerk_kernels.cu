@@ -507,3 +507,178 @@ cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st)
 }
 
 }  // namespace jerk
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot allocate device memory at the moment they need a search
+// step: a process whose device memory is handed out up front by a pool it
+// does not own, a real-time pipeline that forbids allocation after start-up,
+// or code running where cudaMalloc would stall or fail.  For them
+// jerk_volume_static computes one subharmonic's ffdot volume for one rstep
+// (the prep and correlation kernels above) with all of its working memory --
+// the subharmonic and rstep descriptors, the FFT twiddles, the prepared
+// spectrum chunk and the rinds table -- in one fixed device array,
+// g_static_scratch, compiled into this library.  The caller passes only its
+// inputs (spectrum, kernel rows) and its output (the volume).
+//
+// The array is JERK_STATIC_SCRATCH_BYTES (192 KiB) on every GPU that loads
+// the library, held until the process exits; it bounds fftlen to 7680 and
+// corr_uselen to 16384.  Every call shares it and it keeps the last call's
+// contents (each call rewrites all of it that it reads, so nothing needs
+// clearing); calls that overlap on the GPU -- two streams, or two host
+// threads -- race on it and must be serialised by the caller.  Host code
+// cannot use the array's name as a device address, so the first call on each
+// device looks the address up with cudaGetSymbolAddress (with that device
+// current); make that first call before any stream capture.
+
+#define JERK_STATIC_SCRATCH_BYTES (192 * 1024)
+static __device__ __align__(256) unsigned char g_static_scratch[JERK_STATIC_SCRATCH_BYTES];
+
+#include <cstdio>
+#include <mutex>
+
+#include "jerk.h"
+
+namespace jerk {
+namespace {
+
+constexpr int kStaticMaxFft = 7680;
+constexpr int kStaticMaxUselen = 16384;
+// scratch layout (byte offsets)
+constexpr size_t kOffSub = 0;
+constexpr size_t kOffStep = 256;
+constexpr size_t kOffTw = 512;
+constexpr size_t kOffData = kOffTw + 81920;                    // twiddles <= 10240 float2
+constexpr size_t kOffRinds = kOffData + 8 * (size_t)kStaticMaxFft;
+static_assert(kOffRinds + 2 * (size_t)kStaticMaxUselen <= JERK_STATIC_SCRATCH_BYTES,
+              "static scratch layout");
+
+std::mutex g_static_mu;
+unsigned char *g_static_addr[64];
+float2 g_static_tw[81920 / sizeof(float2)];  // host staging of one twiddle table
+
+int static_fail(const char *msg)
+{
+    fprintf(stderr, "jerk_volume_static: %s\n", msg);
+    return JERK_EINVAL;
+}
+
+}  // namespace
+}  // namespace jerk
+
+extern "C" int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
+                                  const jerk_subharm *sub, const void *kernels, double fullrlo,
+                                  int corr_uselen, float nph, float *volume, int *numrs_out,
+                                  long long *rlo_out, void *stream)
+{
+    using namespace jerk;
+    if (!spectrum || !sub || !kernels || !volume || numbins < 1)
+        return static_fail("null argument");
+    const int N = sub->fftlen;
+    const int tws = fft_twiddle_size(N);
+    if (N > kStaticMaxFft || tws < 0 || (size_t)tws * sizeof(float2) > kOffData - kOffTw)
+        return static_fail("fftlen beyond the static scratch (at most 7680, and supported)");
+    if (corr_uselen <= 0 || corr_uselen % 2 || corr_uselen > kStaticMaxUselen)
+        return static_fail("corr_uselen beyond the static scratch (even, at most 16384)");
+    if (sub->numharm < 1 || sub->harmnum < 1 || sub->numz < 1 || sub->numw < 1)
+        return static_fail("bad subharmonic");
+
+    // rstep geometry, as jerk_plan_create computes it (src/accel_utils.c:1107-1141)
+    const double hf = (double)sub->harmnum / (double)sub->numharm;
+    const int rstep = corr_uselen / 2;
+    const double lastr = fullrlo + rstep - 0.5;
+    const double drlo = rint(2.0 * fullrlo * hf) * 0.5, drhi = rint(2.0 * lastr * hf) * 0.5;
+    int numrs = (int)((ceil(drhi) - floor(drlo)) * 2 + 1e-14) + 1;
+    if (sub->numharm == 1 && sub->harmnum == 1)
+        numrs = corr_uselen;
+    else if (numrs % 2)
+        numrs = (numrs / 2 + 1) * 2;
+    if (numrs + 2 * sub->halfwidth > N)
+        return static_fail("fftlen too short for the good bins");
+
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return JERK_ECUDA;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void *addr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
+        if (e != cudaSuccess || !addr) {
+            fprintf(stderr, "jerk_volume_static: cudaGetSymbolAddress: %s\n",
+                    cudaGetErrorString(e));
+            return JERK_ECUDA;
+        }
+        g_static_addr[dev] = (unsigned char *)addr;
+    }
+    unsigned char *base = g_static_addr[dev];
+
+    SubDev sd{};
+    sd.numharm = sub->numharm;
+    sd.harmnum = sub->harmnum;
+    sd.harm_fract = hf;
+    sd.numz = sub->numz;
+    sd.numw = sub->numw;
+    sd.fftlen = N;
+    sd.halfwidth = sub->halfwidth;
+    sd.stride = numrs;
+    sd.pownorm = (float)(1.0 / (double)(N * N));
+    sd.twoff = 0;
+    sd.kern_off = 0;
+    sd.plane_off = 0;
+    sd.plane_size = (long long)sub->numw * sub->numz * numrs;
+    sd.data_off = 0;
+    StepDev sp{};
+    sp.rlo = (long long)floor(drlo);
+    sp.fullrlo = fullrlo;
+    sp.numrs = numrs;
+    fft_twiddle_table(N, g_static_tw);
+
+    cudaError_t e = cudaMemcpyAsync(base + kOffSub, &sd, sizeof(sd), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + kOffStep, &sp, sizeof(sp), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + kOffTw, g_static_tw, sizeof(float2) * tws,
+                            cudaMemcpyHostToDevice, st);
+
+    SearchDev P{};
+    P.spec = (const float2 *)spectrum;
+    P.numbins = numbins;
+    P.lobin = lobin;
+    P.nsubs = 1;
+    P.nstages = 1;
+    P.corr_uselen = corr_uselen;
+    P.numz0 = sub->numz;
+    P.numw0 = sub->numw;
+    P.norm_type = 0;
+    P.nph = nph;
+    P.subs = (const SubDev *)(base + kOffSub);
+    P.steps = (const StepDev *)(base + kOffStep);
+    P.bank = (const float2 *)kernels;
+    P.twiddles = (const float2 *)(base + kOffTw);
+    P.prepped = (float2 *)(base + kOffData);
+    P.planes = volume;
+    P.rinds = (uint16_t *)(base + kOffRinds);
+    P.first_rstep = 0;
+    P.nb = 1;
+    if (e == cudaSuccess)
+        e = launch_prep(P, N, st);
+    if (e == cudaSuccess) {
+        RowGroup G{};
+        G.n = 1;
+        G.sub[0] = 0;
+        G.rowstart[0] = 0;
+        G.rowstart[1] = sub->numw * sub->numz;
+        e = launch_corr(P, N, G, G.rowstart[1], st);
+    }
+    if (e != cudaSuccess) {
+        fprintf(stderr, "jerk_volume_static: %s\n", cudaGetErrorString(e));
+        return JERK_ECUDA;
+    }
+    if (numrs_out)
+        *numrs_out = numrs;
+    if (rlo_out)
+        *rlo_out = sp.rlo;
+    return JERK_OK;
+}

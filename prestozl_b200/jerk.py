@@ -85,7 +85,7 @@ EXPORTS = [
     "jerk_candidate_sigma", "jerk_power_for_sigma", "jerk_insert_hits", "jerk_free",
     "jerk_last_error", "jerk_bank_elements", "jerk_bank_generate", "jerk_device_alloc",
     "jerk_device_free", "jerk_copy_to_host", "jerk_plan_set_profiling", "jerk_plan_reset_stats",
-    "jerk_plan_kernel_stats", "jerk_plan_transfer_stats",
+    "jerk_plan_kernel_stats", "jerk_plan_transfer_stats", "jerk_volume_static",
 ]
 
 
@@ -136,6 +136,9 @@ def lib() -> C.CDLL:
     L.jerk_plan_transfer_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong),
                                            C.POINTER(C.c_longlong)]
     L.jerk_plan_transfer_stats.restype = None
+    L.jerk_volume_static.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.POINTER(Subharm),
+                                     C.c_void_p, C.c_double, C.c_int, C.c_float, C.c_void_p,
+                                     C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.c_void_p]
     _lib = L
     return L
 
@@ -225,6 +228,23 @@ class DeviceBank:
             _check(lib().jerk_copy_to_host(out[i].ctypes.data, self.ptr.value + 8 * (off + int(r) * n),
                                            8 * n))
         return out
+
+
+def volume_static(spectrum_dev: int, numbins: int, lobin: int, sub: dict, kernels_dev: int,
+                  fullrlo: float, corr_uselen: int, nph: float, volume_dev: int,
+                  stream: int = 0) -> Tuple[int, int]:
+    """One subharmonic's ffdot volume for one rstep through the entry point
+    that allocates nothing (jerk_volume_static); all pointers are device
+    addresses the caller owns.  Returns (numrs, rlo); asynchronous on stream."""
+    s = Subharm(sub["numharm"], sub["harmnum"], sub.get("zmax", 0), sub.get("wmax", 0),
+                sub["numz"], sub["numw"], sub["fftlen"], sub["halfwidth"], None)
+    numrs, rlo = C.c_int(0), C.c_longlong(0)
+    rc = lib().jerk_volume_static(spectrum_dev, numbins, lobin, C.byref(s), kernels_dev, fullrlo,
+                                  corr_uselen, nph, volume_dev, C.byref(numrs), C.byref(rlo),
+                                  stream or None)
+    if rc != JERK_OK:
+        raise JerkError(rc, "jerk_volume_static failed (see stderr)")
+    return numrs.value, rlo.value
 
 
 def _spectrum_arg(spectrum):
