@@ -332,25 +332,30 @@ __global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P
     const float *planes = P.planes;
     for (int jj0 = 0; jj0 < numz0; jj0 += kHarmZ) {
         const bool full = jj0 + kHarmZ <= numz0;
-        float v[kHarmZ];
-        {
-            const int4 z = *reinterpret_cast<const int4 *>(hsm + jj0);
-            v[0] = planes[off[0] + z.x];
-            v[1] = planes[off[0] + z.y];
-            v[2] = planes[off[0] + z.z];
-            v[3] = planes[off[0] + z.w];
+        // every gather of the four rows first (independent loads in flight),
+        // then the adds in the reference's order
+        float x[NS][kHarmZ];
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
+            x[s][0] = planes[off[s] + z.x];
+            x[s][1] = planes[off[s] + z.y];
+            x[s][2] = planes[off[s] + z.z];
+            x[s][3] = planes[off[s] + z.w];
         }
+        float v[kHarmZ];
+#pragma unroll
+        for (int u = 0; u < kHarmZ; u++)
+            v[u] = x[0][u];
         int s = 1;
 #pragma unroll
         for (int stage = 0; stage < S; stage++) {
             if (stage > 0) {
 #pragma unroll
                 for (int h = 0; h < (1 << (stage - 1)); h++, s++) {
-                    const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
-                    v[0] = __fadd_rn(v[0], planes[off[s] + z.x]);
-                    v[1] = __fadd_rn(v[1], planes[off[s] + z.y]);
-                    v[2] = __fadd_rn(v[2], planes[off[s] + z.z]);
-                    v[3] = __fadd_rn(v[3], planes[off[s] + z.w]);
+#pragma unroll
+                    for (int u = 0; u < kHarmZ; u++)
+                        v[u] = __fadd_rn(v[u], x[s][u]);
                 }
             }
 #pragma unroll

@@ -685,7 +685,10 @@ struct PendingTiming {
 
 struct jerk_plan {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;   // prep + correlation (and the caller's work)
+    cudaStream_t hstream = nullptr;  // harmonic sums, overlapping the next batch's correlation
+    cudaEvent_t ev_vol[2] = {nullptr, nullptr};   // volumes of buffer i written
+    cudaEvent_t ev_free[2] = {nullptr, nullptr};  // buffer i read by its harmonic sum
     bool own_stream = false;
     jerk_obs obs{};
     int nsubs = 0, maxfft = 0, batch = 8;
@@ -748,7 +751,8 @@ static cudaEvent_t take_event(jerk_plan *p)
 }
 
 // Bracket one launch: returns a token to pass to launch_end.
-static int launch_begin(jerk_plan *p, int cls, double bytes, double flops)
+static int launch_begin(jerk_plan *p, int cls, double bytes, double flops,
+                        cudaStream_t st = nullptr)
 {
     KernelClass &k = p->classes[cls];
     k.launches++;
@@ -757,15 +761,15 @@ static int launch_begin(jerk_plan *p, int cls, double bytes, double flops)
     if (!p->profiling)
         return -1;
     PendingTiming t{cls, take_event(p), take_event(p)};
-    cudaEventRecord(t.start, p->stream);
+    cudaEventRecord(t.start, st ? st : p->stream);
     p->pending.push_back(t);
     return (int)p->pending.size() - 1;
 }
 
-static void launch_end(jerk_plan *p, int token)
+static void launch_end(jerk_plan *p, int token, cudaStream_t st = nullptr)
 {
     if (token >= 0)
-        cudaEventRecord(p->pending[token].stop, p->stream);
+        cudaEventRecord(p->pending[token].stop, st ? st : p->stream);
 }
 
 // after a stream synchronisation: fold the recorded intervals into the classes
@@ -862,6 +866,16 @@ extern "C" void jerk_plan_destroy(jerk_plan *p)
     }
     for (auto e : p->event_pool)
         cudaEventDestroy(e);
+    if (p->hstream) {
+        cudaStreamSynchronize(p->hstream);
+        cudaStreamDestroy(p->hstream);
+    }
+    for (int i = 0; i < 2; i++) {
+        if (p->ev_vol[i])
+            cudaEventDestroy(p->ev_vol[i]);
+        if (p->ev_free[i])
+            cudaEventDestroy(p->ev_free[i]);
+    }
     if (p->own_stream && p->stream)
         cudaStreamDestroy(p->stream);
     cudaSetDevice(cur);
@@ -1080,9 +1094,16 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     JERK_CUDA_B(cudaMemcpyAsync(p->d_wind, wind.data(), sizeof(int) * wind.size(),
                                 cudaMemcpyHostToDevice, p->stream));
     JERK_CUDA_B(cudaMalloc(&p->d_prepped, sizeof(float2) * p->prepped_f2));
-    JERK_CUDA_B(cudaMalloc(&p->d_planes, sizeof(float) * p->plane_floats));
-    JERK_CUDA_B(cudaMalloc(&p->d_rinds, sizeof(uint16_t) * (size_t)p->batch * nsubs *
+    // two volume / rinds buffers: batch k+1's correlation writes one while
+    // batch k's harmonic sum reads the other
+    JERK_CUDA_B(cudaMalloc(&p->d_planes, 2 * sizeof(float) * p->plane_floats));
+    JERK_CUDA_B(cudaMalloc(&p->d_rinds, 2 * sizeof(uint16_t) * (size_t)p->batch * nsubs *
                                             obs->corr_uselen));
+    JERK_CUDA_B(cudaStreamCreateWithFlags(&p->hstream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+        JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_vol[i], cudaEventDisableTiming));
+        JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_free[i], cudaEventDisableTiming));
+    }
     JERK_CUDA_B(cudaMalloc(&p->d_hit_count, sizeof(unsigned int)));
     JERK_CUDA_B(cudaMalloc(&p->d_status, sizeof(unsigned int)));
     JERK_CUDA_B(cudaMemsetAsync(p->d_status, 0, sizeof(unsigned int), p->stream));
@@ -1208,13 +1229,24 @@ static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, lo
 {
     unsigned int status = 0;
     SearchDev a = make_args(p, spec);
+    const size_t rinds_per_buf = (size_t)p->batch * p->nsubs * p->obs.corr_uselen;
     JERK_CUDA(cudaMemsetAsync(p->d_hit_count, 0, sizeof(unsigned int), p->stream));
-    for (long long k = first; k < first + count; k += p->batch) {
+    bool used[2] = {false, false};
+    long long nbatch = 0;
+    for (long long k = first; k < first + count; k += p->batch, nbatch++) {
+        const int i = (int)(nbatch & 1);
         a.first_rstep = k;
         a.nb = (int)std::min<long long>(p->batch, first + count - k);
+        a.planes = p->d_planes + (size_t)i * p->plane_floats;
+        a.rinds = p->d_rinds + (size_t)i * rinds_per_buf;
+        // buffer i is free once the harmonic sum two batches back has read it
+        if (used[i])
+            JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
         int rc = run_volumes(p, a);
         if (rc != JERK_OK)
             return rc;
+        JERK_CUDA(cudaEventRecord(p->ev_vol[i], p->stream));
+        JERK_CUDA(cudaStreamWaitEvent(p->hstream, p->ev_vol[i], 0));
         // algorithmic traffic: every volume of the batch read once
         double bytes = 0, flops = 0;
         const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
@@ -1225,12 +1257,18 @@ static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, lo
             bytes += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
         }
         flops = npts * p->nsubs;
-        const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops);
-        cudaError_t e = launch_harmsum(a, p->stream);
-        launch_end(p, tok);
+        const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops, p->hstream);
+        cudaError_t e = launch_harmsum(a, p->hstream);
+        launch_end(p, tok, p->hstream);
         if (e != cudaSuccess)
             return cuda_fail(e, "harmsum_kernel");
+        JERK_CUDA(cudaEventRecord(p->ev_free[i], p->hstream));
+        used[i] = true;
     }
+    // join: the caller's stream sees every harmonic sum done
+    for (int i = 0; i < 2; i++)
+        if (used[i])
+            JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
     JERK_CUDA(cudaMemcpyAsync(nhits_out, p->d_hit_count, sizeof(unsigned int),
                               cudaMemcpyDeviceToHost, p->stream));
     JERK_CUDA(cudaMemcpyAsync(&status, p->d_status, sizeof(unsigned int),
