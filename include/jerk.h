@@ -127,6 +127,20 @@ int jerk_search(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
                 long long first_rstep, long long num_rsteps, jerk_cand **cands,
                 long long *ncands, jerk_hits *hits);
 
+/* The same search in two halves, so a host thread can keep several plans
+ * busy: jerk_search_async stages the spectrum and enqueues every batch on the
+ * plan's streams, then returns; jerk_search_ready reports (without blocking)
+ * whether the device work is done (1), not yet (0) or failed (< 0);
+ * jerk_search_collect waits for it and builds the candidate list.  One search
+ * in flight per plan; a host spectrum must stay valid until collect. */
+int jerk_search_async(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
+                      long long first_rstep, long long num_rsteps);
+int jerk_search_ready(jerk_plan *plan);
+int jerk_search_collect(jerk_plan *plan, jerk_cand **cands, long long *ncands, jerk_hits *hits);
+
+/* Device memory the plan holds (volumes, tables, hit buffer, its own bank). */
+long long jerk_plan_device_bytes(const jerk_plan *plan);
+
 /* Number of rsteps of the full search. */
 long long jerk_num_rsteps(const jerk_plan *plan);
 
@@ -183,6 +197,54 @@ int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
                        const jerk_subharm *sub, const void *kernels, double fullrlo,
                        int corr_uselen, float nph, float *volume, int *numrs, long long *rlo,
                        void *stream);
+
+/* The served form: a request loop on one GPU (continuous batching).
+ * Submitted spectra wait in a queue; a worker thread that owns the device
+ * admits them while fewer than max_active searches run and their device
+ * footprint fits hbm_budget_bytes, keeps the admitted searches in flight
+ * together on their own streams, and queues each finished candidate list for
+ * jerk_server_poll.  Kernel banks are generated once per search geometry and
+ * shared; idle plans of the same geometry are reused.  A result equals
+ * jerk_search's for the same spectrum and parameters.  (The reference's
+ * counterpart is the process pool of bin/accelsearch_pipeline_cu.py.) */
+typedef struct jerk_server jerk_server;
+
+typedef struct jerk_server_config {
+    long long hbm_budget_bytes;  /* admission budget; 0 = 85% of free device memory */
+    int max_active;              /* searches in flight at once; 0 = 3 */
+    int batch_rsteps;            /* rsteps per batch of each plan; 0 = 16 */
+    int device;                  /* CUDA device the worker owns */
+} jerk_server_config;
+
+typedef struct jerk_request {
+    const void *spectrum;        /* numbins complex64; valid until its result is polled */
+    int on_device;               /* spectrum is a device pointer */
+    long long numbins;
+    long long N;                 /* time samples (the .inf's N) */
+    double dt;
+    int zmax, wmax, wmax_given, numharm;
+    float sigma;
+    double flo, fhi;             /* accelsearch's -flo / -fhi (defaults 1, 10000) */
+    long long tag;               /* the caller's id, returned with the result */
+} jerk_request;
+
+typedef struct jerk_result {
+    long long tag;
+    int status;                  /* JERK_OK or the error of this request */
+    jerk_cand *cands;            /* free with jerk_free */
+    long long ncands;
+    double t_submit, t_start, t_done;  /* seconds on a steady clock */
+} jerk_result;
+
+int jerk_server_create(jerk_server **server, const jerk_server_config *cfg);
+int jerk_server_submit(jerk_server *server, const jerk_request *req);
+/* Next finished request within timeout_ms: JERK_OK with *out filled, or
+ * JERK_TIMEOUT. */
+int jerk_server_poll(jerk_server *server, jerk_result *out, int timeout_ms);
+/* out[6]: submitted, finished, failed, queued, peak device bytes, budget. */
+void jerk_server_stats(jerk_server *server, long long *out);
+/* Finishes every submitted request, then stops; unpolled results are freed. */
+void jerk_server_destroy(jerk_server *server);
 
 /* Statistics (host, double precision). */
 double jerk_candidate_sigma(double power, int numsum, double numtrials);

@@ -717,6 +717,12 @@ struct jerk_plan {
     unsigned int *d_status = nullptr;
     long long max_hits = 0;
     long long plane_floats = 0, prepped_f2 = 0;
+    // asynchronous search in flight (jerk_search_async / jerk_search_collect)
+    bool in_flight = false;
+    const float2 *inflight_spec = nullptr;
+    long long inflight_first = 0, inflight_count = 0;
+    unsigned int *h_counts = nullptr;  // pinned: hit count, status
+    cudaEvent_t ev_done = nullptr;
     // instrumentation
     bool profiling = false;
     std::vector<KernelClass> classes;
@@ -870,6 +876,10 @@ extern "C" void jerk_plan_destroy(jerk_plan *p)
         cudaStreamSynchronize(p->hstream);
         cudaStreamDestroy(p->hstream);
     }
+    if (p->ev_done)
+        cudaEventDestroy(p->ev_done);
+    if (p->h_counts)
+        cudaFreeHost(p->h_counts);
     for (int i = 0; i < 2; i++) {
         if (p->ev_vol[i])
             cudaEventDestroy(p->ev_vol[i]);
@@ -1100,6 +1110,8 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     JERK_CUDA_B(cudaMalloc(&p->d_rinds, 2 * sizeof(uint16_t) * (size_t)p->batch * nsubs *
                                             obs->corr_uselen));
     JERK_CUDA_B(cudaStreamCreateWithFlags(&p->hstream, cudaStreamNonBlocking));
+    JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming));
+    JERK_CUDA_B(cudaHostAlloc(&p->h_counts, 2 * sizeof(unsigned int), cudaHostAllocDefault));
     for (int i = 0; i < 2; i++) {
         JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_vol[i], cudaEventDisableTiming));
         JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_free[i], cudaEventDisableTiming));
@@ -1224,10 +1236,9 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
     return JERK_OK;
 }
 
-static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, long long count,
-                           unsigned int *nhits_out)
+// Enqueue one search pass on the plan's streams (no host synchronisation).
+static int enqueue_search_pass(jerk_plan *p, const float2 *spec, long long first, long long count)
 {
-    unsigned int status = 0;
     SearchDev a = make_args(p, spec);
     const size_t rinds_per_buf = (size_t)p->batch * p->nsubs * p->obs.corr_uselen;
     JERK_CUDA(cudaMemsetAsync(p->d_hit_count, 0, sizeof(unsigned int), p->stream));
@@ -1269,50 +1280,106 @@ static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, lo
     for (int i = 0; i < 2; i++)
         if (used[i])
             JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
-    JERK_CUDA(cudaMemcpyAsync(nhits_out, p->d_hit_count, sizeof(unsigned int),
+    JERK_CUDA(cudaMemcpyAsync(p->h_counts, p->d_hit_count, sizeof(unsigned int),
                               cudaMemcpyDeviceToHost, p->stream));
-    JERK_CUDA(cudaMemcpyAsync(&status, p->d_status, sizeof(unsigned int),
+    JERK_CUDA(cudaMemcpyAsync(p->h_counts + 1, p->d_status, sizeof(unsigned int),
                               cudaMemcpyDeviceToHost, p->stream));
-    JERK_CUDA(cudaStreamSynchronize(p->stream));
-    collect_timings(p);
-    p->d2h_bytes += 2 * sizeof(unsigned int);
-    if (status)
-        return fail(JERK_EINVAL, "harmonic sum: a subharmonic r index left its row");
+    JERK_CUDA(cudaEventRecord(p->ev_done, p->stream));
     return JERK_OK;
 }
 
-extern "C" int jerk_search(jerk_plan *p, const void *spectrum, int spectrum_on_device,
-                           long long first_rstep, long long num_rsteps, jerk_cand **cands,
-                           long long *ncands, jerk_hits *hits)
+// Wait for an enqueued pass and read its hit count.
+static int finish_search_pass(jerk_plan *p, unsigned int *nhits_out)
 {
-    if (!p || !spectrum)
-        return fail(JERK_EINVAL, "jerk_search: null argument");
+    JERK_CUDA(cudaEventSynchronize(p->ev_done));
+    collect_timings(p);
+    p->d2h_bytes += 2 * sizeof(unsigned int);
+    if (p->h_counts[1])
+        return fail(JERK_EINVAL, "harmonic sum: a subharmonic r index left its row");
+    *nhits_out = p->h_counts[0];
+    return JERK_OK;
+}
+
+static int run_search_pass(jerk_plan *p, const float2 *spec, long long first, long long count,
+                           unsigned int *nhits_out)
+{
+    int rc = enqueue_search_pass(p, spec, first, count);
+    if (rc != JERK_OK)
+        return rc;
+    return finish_search_pass(p, nhits_out);
+}
+
+static int check_range(const jerk_plan *p, long long first_rstep, long long num_rsteps,
+                       long long *count)
+{
     if (first_rstep < 0 || first_rstep > p->nrsteps)
         return fail(JERK_EINVAL, "jerk_search: first_rstep out of range");
-    long long count = p->nrsteps - first_rstep;
-    if (num_rsteps > 0 && num_rsteps < count)
-        count = num_rsteps;
+    *count = p->nrsteps - first_rstep;
+    if (num_rsteps > 0 && num_rsteps < *count)
+        *count = num_rsteps;
+    return JERK_OK;
+}
+
+extern "C" int jerk_search_async(jerk_plan *p, const void *spectrum, int spectrum_on_device,
+                                 long long first_rstep, long long num_rsteps)
+{
+    if (!p || !spectrum)
+        return fail(JERK_EINVAL, "jerk_search_async: null argument");
+    if (p->in_flight)
+        return fail(JERK_EINVAL, "jerk_search_async: a search is already in flight on this plan");
+    long long count = 0;
+    int rc = check_range(p, first_rstep, num_rsteps, &count);
+    if (rc != JERK_OK)
+        return rc;
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != p->device)
         JERK_CUDA(cudaSetDevice(p->device));
     const float2 *spec = nullptr;
-    int rc = stage_spectrum(p, spectrum, spectrum_on_device, &spec);
+    rc = stage_spectrum(p, spectrum, spectrum_on_device, &spec);
     if (rc != JERK_OK)
         return rc;
+    rc = enqueue_search_pass(p, spec, first_rstep, count);
+    if (rc != JERK_OK)
+        return rc;
+    p->in_flight = true;
+    p->inflight_spec = spec;
+    p->inflight_first = first_rstep;
+    p->inflight_count = count;
+    return JERK_OK;
+}
 
+extern "C" int jerk_search_ready(jerk_plan *p)
+{
+    if (!p || !p->in_flight)
+        return 1;
+    const cudaError_t e = cudaEventQuery(p->ev_done);
+    if (e == cudaSuccess)
+        return 1;
+    if (e == cudaErrorNotReady)
+        return 0;
+    return cuda_fail(e, "jerk_search_ready");
+}
+
+extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *ncands,
+                                   jerk_hits *hits)
+{
+    if (!p || !p->in_flight)
+        return fail(JERK_EINVAL, "jerk_search_collect: no search in flight");
+    p->in_flight = false;
     unsigned int nh = 0;
-    for (int attempt = 0;; attempt++) {
-        rc = run_search_pass(p, spec, first_rstep, count, &nh);
-        if (rc != JERK_OK)
-            return rc;
-        if ((long long)nh <= p->max_hits)
-            break;
+    int rc = finish_search_pass(p, &nh);
+    if (rc != JERK_OK)
+        return rc;
+    for (int attempt = 0; (long long)nh > p->max_hits; attempt++) {
         // overflow: the counter kept counting, so one retry with the exact
         // size always suffices
         if (attempt > 2)
             return fail(JERK_OVERFLOW, "hit buffer overflow persisted");
         rc = alloc_hits(p, (long long)nh + (nh >> 3) + 1024);
+        if (rc != JERK_OK)
+            return rc;
+        rc = run_search_pass(p, p->inflight_spec, p->inflight_first, p->inflight_count, &nh);
         if (rc != JERK_OK)
             return rc;
     }
@@ -1373,6 +1440,29 @@ extern "C" int jerk_search(jerk_plan *p, const void *spectrum, int spectrum_on_d
     if (ncands)
         *ncands = n;
     return JERK_OK;
+}
+
+extern "C" int jerk_search(jerk_plan *p, const void *spectrum, int spectrum_on_device,
+                           long long first_rstep, long long num_rsteps, jerk_cand **cands,
+                           long long *ncands, jerk_hits *hits)
+{
+    int rc = jerk_search_async(p, spectrum, spectrum_on_device, first_rstep, num_rsteps);
+    if (rc != JERK_OK)
+        return rc;
+    return jerk_search_collect(p, cands, ncands, hits);
+}
+
+extern "C" long long jerk_plan_device_bytes(const jerk_plan *p)
+{
+    if (!p)
+        return 0;
+    return (long long)(2 * sizeof(float) * p->plane_floats +
+                       2 * sizeof(uint16_t) * (size_t)p->batch * p->nsubs * p->obs.corr_uselen +
+                       sizeof(float2) * p->prepped_f2 +
+                       (sizeof(unsigned long long) + sizeof(float)) * p->max_hits +
+                       sizeof(StepDev) * p->hsteps.size() + sizeof(float2) * p->spec_cap +
+                       (p->own_bank ? sizeof(float2) * jerk_bank_elements(p->subs.data(), p->nsubs)
+                                    : 0));
 }
 
 extern "C" int jerk_debug_volume(jerk_plan *p, const void *spectrum, int spectrum_on_device,

@@ -68,6 +68,24 @@ class KernelStat(C.Structure):
                 ("bytes", C.c_double), ("flops", C.c_double)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_longlong), ("max_active", C.c_int),
+                ("batch_rsteps", C.c_int), ("device", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("spectrum", C.c_void_p), ("on_device", C.c_int), ("numbins", C.c_longlong),
+                ("N", C.c_longlong), ("dt", C.c_double), ("zmax", C.c_int), ("wmax", C.c_int),
+                ("wmax_given", C.c_int), ("numharm", C.c_int), ("sigma", C.c_float),
+                ("flo", C.c_double), ("fhi", C.c_double), ("tag", C.c_longlong)]
+
+
+class Result(C.Structure):
+    _fields_ = [("tag", C.c_longlong), ("status", C.c_int), ("cands", C.POINTER(Cand)),
+                ("ncands", C.c_longlong), ("t_submit", C.c_double), ("t_start", C.c_double),
+                ("t_done", C.c_double)]
+
+
 class Hits(C.Structure):
     _fields_ = [("count", C.c_longlong), ("keys", C.POINTER(C.c_ulonglong)),
                 ("powers", C.POINTER(C.c_float))]
@@ -86,6 +104,9 @@ EXPORTS = [
     "jerk_last_error", "jerk_bank_elements", "jerk_bank_generate", "jerk_device_alloc",
     "jerk_device_free", "jerk_copy_to_host", "jerk_plan_set_profiling", "jerk_plan_reset_stats",
     "jerk_plan_kernel_stats", "jerk_plan_transfer_stats", "jerk_volume_static",
+    "jerk_search_async", "jerk_search_ready", "jerk_search_collect", "jerk_plan_device_bytes",
+    "jerk_server_create", "jerk_server_submit", "jerk_server_poll", "jerk_server_stats",
+    "jerk_server_destroy",
 ]
 
 
@@ -136,6 +157,19 @@ def lib() -> C.CDLL:
     L.jerk_plan_transfer_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong),
                                            C.POINTER(C.c_longlong)]
     L.jerk_plan_transfer_stats.restype = None
+    L.jerk_search_async.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_longlong]
+    L.jerk_search_ready.argtypes = [C.c_void_p]
+    L.jerk_search_collect.argtypes = [C.c_void_p, C.POINTER(C.POINTER(Cand)),
+                                      C.POINTER(C.c_longlong), C.POINTER(Hits)]
+    L.jerk_plan_device_bytes.restype = C.c_longlong
+    L.jerk_plan_device_bytes.argtypes = [C.c_void_p]
+    L.jerk_server_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(ServerConfig)]
+    L.jerk_server_submit.argtypes = [C.c_void_p, C.POINTER(Request)]
+    L.jerk_server_poll.argtypes = [C.c_void_p, C.POINTER(Result), C.c_int]
+    L.jerk_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    L.jerk_server_stats.restype = None
+    L.jerk_server_destroy.argtypes = [C.c_void_p]
+    L.jerk_server_destroy.restype = None
     L.jerk_volume_static.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.POINTER(Subharm),
                                      C.c_void_p, C.c_double, C.c_int, C.c_float, C.c_void_p,
                                      C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.c_void_p]
@@ -360,6 +394,73 @@ class JerkPlan:
         ii = k % numw; k //= numw
         st = k % S; rs = k // S
         return rs, st, ii, jj, kk
+
+
+def _cands_array(ptr, n: int) -> np.ndarray:
+    nb = n * CAND_DTYPE.itemsize
+    out = np.frombuffer(C.string_at(ptr, nb), dtype=CAND_DTYPE).copy() if nb else \
+        np.zeros(0, dtype=CAND_DTYPE)
+    lib().jerk_free(ptr)
+    return out
+
+
+class JerkServer:
+    """The served form (jerk_server_*): submit spectra as they arrive, poll
+    finished candidate lists.  Spectra (numpy arrays on the host, or CUDA
+    tensors) are kept alive here until their result has been polled."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_active: int = 0, batch: int = 0,
+                 device: int = 0):
+        cfg = ServerConfig(hbm_budget_bytes, max_active, batch, device)
+        self._s = C.c_void_p()
+        _check(lib().jerk_server_create(C.byref(self._s), C.byref(cfg)))
+        self._keep = {}
+        self._next = 0
+
+    def submit(self, spectrum, N: int, dt: float, zmax: int, wmax: int, numharm: int,
+               sigma: float, wmax_given: bool = True, flo: float = 1.0, fhi: float = 10000.0,
+               tag: Optional[int] = None) -> int:
+        ptr, dev, keep = _spectrum_arg(spectrum)
+        numbins = int(spectrum.shape[0]) if dev else len(keep)
+        if tag is None:
+            tag = self._next
+        self._next = max(self._next, tag) + 1
+        self._keep[tag] = keep
+        req = Request(ptr, dev, numbins, N, dt, zmax, wmax, int(wmax_given), numharm, sigma,
+                      flo, fhi, tag)
+        _check(lib().jerk_server_submit(self._s, C.byref(req)))
+        return tag
+
+    def poll(self, timeout_ms: int = 1000):
+        """(tag, candidates, times dict) of the next finished request, or None."""
+        r = Result()
+        rc = lib().jerk_server_poll(self._s, C.byref(r), timeout_ms)
+        if rc == JERK_TIMEOUT:
+            return None
+        _check(rc)
+        self._keep.pop(r.tag, None)
+        if r.status != JERK_OK:
+            raise JerkError(r.status, f"request {r.tag} failed")
+        cands = _cands_array(r.cands, r.ncands)
+        return r.tag, cands, {"submit": r.t_submit, "start": r.t_start, "done": r.t_done}
+
+    def stats(self) -> dict:
+        a = (C.c_longlong * 6)()
+        lib().jerk_server_stats(self._s, a)
+        return dict(zip(["submitted", "finished", "failed", "queued", "peak_bytes", "budget"],
+                        list(a)))
+
+    def close(self) -> None:
+        if self._s:
+            lib().jerk_server_destroy(self._s)
+            self._s = C.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def obs_from_refobs(ro) -> Obs:

@@ -1,0 +1,76 @@
+"""Multi-GPU: one process per GPU, spectra sharded across ranks.
+
+The jerk search has no data-path exchange: spectra (and, for one very long
+spectrum, rstep ranges) are independent, and the kernel bank is replicated.
+Ranks only agree on timing (the max over ranks) and, for a job that wants
+one list of results, hand their per-spectrum candidate lists to rank 0 -- the
+host merge.  Everything here is torch.distributed plumbing that works with the
+"nccl" backend on GPUs and "gloo" on CPUs.
+"""
+
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+
+@dataclass(frozen=True)
+class RankEnv:
+    rank: int
+    world: int
+    local: int
+
+
+def rank_env() -> RankEnv:
+    return RankEnv(int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+                   int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def shard(items: Sequence, rank: int, world: int) -> List:
+    """Round-robin share of a job's spectra for one rank (every item exactly
+    once over all ranks)."""
+    return [x for i, x in enumerate(items) if i % world == rank]
+
+
+def rstep_ranges(nrsteps: int, world: int) -> List[Tuple[int, int]]:
+    """Contiguous (first, count) rstep ranges covering one spectrum, one per
+    rank, for a spectrum searched by several GPUs."""
+    base, extra = divmod(nrsteps, world)
+    out, first = [], 0
+    for r in range(world):
+        n = base + (1 if r < extra else 0)
+        out.append((first, n))
+        first += n
+    return out
+
+
+def max_over_ranks(value: float, dist=None, device: Optional[str] = None) -> float:
+    """The largest value over ranks (a job's time is its slowest rank's)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gather_results(local: Dict[int, list], dist=None) -> Optional[Dict[int, list]]:
+    """Per-spectrum results of all ranks on rank 0 (None elsewhere).  Keys are
+    global spectrum ids; a rank's lists are merged unchanged (each spectrum is
+    searched by exactly one rank, so nothing needs re-ordering)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return dict(local)
+    world = dist.get_world_size()
+    parts = [None] * world if dist.get_rank() == 0 else None
+    dist.gather_object(local, parts, dst=0)
+    if dist.get_rank() != 0:
+        return None
+    merged: Dict[int, list] = {}
+    for p in parts:
+        for k, v in p.items():
+            if k in merged:
+                raise ValueError(f"spectrum {k} searched by two ranks")
+            merged[k] = v
+    return merged

@@ -1,0 +1,82 @@
+"""The served form: spectra of uneven length and uneven (zmax, wmax, numharm)
+submitted together must each give exactly the candidate list they give when
+searched alone (same kernels, same inputs -- bitwise equal), with banks
+shared between requests of equal geometry and admission held to an HBM
+budget."""
+
+import numpy as np
+import pytest
+
+from prestozl_b200 import build, jerk, synth
+
+pytestmark = pytest.mark.gpu
+
+# (N, dt, zmax, wmax, numharm, sigma, seed)
+MIX = [
+    (1 << 20, 64e-6, 20, 60, 8, 2.0, 1),
+    (1 << 19, 64e-6, 50, 160, 4, 2.5, 2),
+    (1 << 20, 64e-6, 20, 60, 8, 2.0, 3),     # shares the first request's bank
+    (1 << 18, 128e-6, 100, 0, 16, 3.0, 4),   # -wmax 0
+    (1 << 20, 64e-6, 10, 40, 2, 2.0, 5),
+]
+
+
+def spectra():
+    out = []
+    for N, dt, z, w, nh, sig, seed in MIX:
+        rng = np.random.default_rng(seed)
+        ps = synth.random_pulsars(rng, 2, zmax=z * 0.8, wmax=max(w, 1) * 0.8, fmax=200.0)
+        ts = synth.timeseries(N, dt, ps, seed)
+        out.append(synth.presto_fft(ts))
+    return out
+
+
+def alone(spec, N, dt, z, w, nh, sig):
+    obs, fftlen, _ = jerk.obs_from_params(len(spec), N, dt, z, w, nh, sig)
+    subs = jerk.subharm_sizes(obs, fftlen)
+    bank = jerk.DeviceBank(subs)
+    plan = jerk.JerkPlan(obs, subs, batch=16, device_bank=bank.ptr.value)
+    c = plan.search(spec)
+    plan.close()
+    bank.close()
+    return c
+
+
+def test_results_alone_equal_results_in_the_mix():
+    build.build()
+    specs = spectra()
+    want = [alone(s, N, dt, z, w, nh, sig) for s, (N, dt, z, w, nh, sig, _) in zip(specs, MIX)]
+    srv = jerk.JerkServer(max_active=3, batch=16)
+    for i, (s, (N, dt, z, w, nh, sig, _)) in enumerate(zip(specs, MIX)):
+        srv.submit(s, N, dt, z, w, nh, sig, tag=i)
+    got = {}
+    while len(got) < len(MIX):
+        r = srv.poll(60000)
+        assert r is not None, "server stalled"
+        tag, cands, t = r
+        assert t["submit"] <= t["start"] <= t["done"]
+        got[tag] = cands
+    st = srv.stats()
+    srv.close()
+    assert st["finished"] == len(MIX) and st["failed"] == 0
+    for i in range(len(MIX)):
+        assert np.array_equal(got[i], want[i]), i
+    assert any(len(w) for w in want)
+
+
+def test_admission_under_a_small_budget_still_finishes_everything():
+    build.build()
+    specs = spectra()[:3]
+    # room for about one request at a time (each needs ~130 MB here)
+    srv = jerk.JerkServer(hbm_budget_bytes=300 << 20, max_active=3, batch=4)
+    for i, (s, (N, dt, z, w, nh, sig, _)) in enumerate(zip(specs, MIX)):
+        srv.submit(s, N, dt, z, w, nh, sig, tag=i)
+    tags = []
+    while len(tags) < 3:
+        r = srv.poll(60000)
+        assert r is not None
+        tags.append(r[0])
+    st = srv.stats()
+    srv.close()
+    assert sorted(tags) == [0, 1, 2] and st["failed"] == 0
+    assert 0 < st["peak_bytes"] <= st["budget"]

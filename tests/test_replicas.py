@@ -1,0 +1,67 @@
+"""The multi-rank path on CPU: two gloo ranks shard a job's spectra, agree on
+the max-over-ranks time and merge their per-spectrum results on rank 0 --
+the same calls bench.py and the service make over NCCL on GPUs."""
+
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from prestozl_b200 import replicas
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    env = replicas.rank_env()
+    ids = list(range(7))
+    mine = replicas.shard(ids, env.rank, env.world)
+    # each rank "searches" its spectra: results keyed by spectrum id
+    local = {i: [(float(i), env.rank)] for i in mine}
+    t = replicas.max_over_ranks(10.0 + env.rank, dist)
+    merged = replicas.gather_results(local, dist)
+    q.put((env.rank, mine, t, merged))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_shard_time_and_merge():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in range(world):
+        r, mine, t, merged = q.get(timeout=120)
+        out[r] = (mine, t, merged)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert sorted(out[0][0] + out[1][0]) == list(range(7))
+    assert not set(out[0][0]) & set(out[1][0])
+    assert out[0][1] == out[1][1] == 11.0
+    merged = out[0][2]
+    assert sorted(merged) == list(range(7))
+    assert all(merged[i][0][1] == i % 2 for i in range(7))
+    assert out[1][2] is None
+
+
+def test_rstep_ranges_cover_a_spectrum():
+    for n, w in ((23364, 8), (5, 8), (100, 3)):
+        rr = replicas.rstep_ranges(n, w)
+        assert sum(c for _, c in rr) == n
+        assert all(rr[i][0] + rr[i][1] == rr[i + 1][0] for i in range(w - 1))
