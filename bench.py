@@ -207,19 +207,47 @@ def _count_rsteps(obs) -> int:
 
 # --------------------------------------------------------------------------
 
+def run_served(srv, spectra, dev: bool, device_events: bool = True):
+    """Submit every spectrum at once to the server and wait for all results.
+    Returns (job seconds on the device timeline, per-request service and
+    queueing latencies in ms, candidates per spectrum)."""
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for i, sp in enumerate(spectra):
+        srv.submit(sp, N_SAMPLES, DT, ZMAX, WMAX, NUMHARM, SIGMA, tag=i)
+    service, total, ncand = [], [], []
+    for _ in spectra:
+        r = srv.poll(600000)
+        if r is None:
+            raise RuntimeError("served search stalled")
+        tag, cands, t = r
+        service.append((t["done"] - t["start"]) * 1000.0)
+        total.append((t["done"] - t["submit"]) * 1000.0)
+        ncand.append(len(cands))
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1000.0, service, total, ncand
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=4,
+                    help="spectra per timed job (plain: sequential searches; served: one burst)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=16, help="rsteps per batch")
+    ap.add_argument("--batch", type=int, default=32, help="rsteps per batch")
+    ap.add_argument("--max-active", type=int, default=3, help="served: searches in flight")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--rsteps", type=int, default=0,
                     help="search only the first R rsteps of each spectrum (profiling runs; "
-                         "the line is then marked partial)")
+                         "the line is then marked partial and the served legs are skipped)")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -228,9 +256,10 @@ def main():
 
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from prestozl_b200 import replicas
+
+    env = replicas.rank_env()
+    rank, world, local = env.rank, env.world, env.local
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -246,114 +275,183 @@ def main():
     bank = jerk.DeviceBank(subs)
     plan = jerk.JerkPlan(obs, subs, batch=args.batch, device_bank=bank.ptr.value)
     nrsteps = plan.num_rsteps
+    nsearch = args.rsteps if args.rsteps > 0 else 0
+    served = not args.no_served and not nsearch
 
-    # two resident spectra per rank, alternated (each is larger than L2)
-    specs = [make_spectrum(1000 * rank + i, "cuda") for i in range(2)]
+    # this rank's spectra, resident in HBM (each larger than L2)
+    nspec = max(2, args.steps)
+    specs = [make_spectrum(1000 * rank + i, "cuda") for i in range(nspec)]
     torch.cuda.synchronize()
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    nsearch = args.rsteps if args.rsteps > 0 else 0
-
     for i in range(args.warmup):
-        plan.search(specs[i % 2], 0, nsearch)
+        plan.search(specs[i % nspec], 0, nsearch)
     torch.cuda.synchronize()
 
-    plan.reset_stats()
-    plan.set_profiling(True)
+    # ---- plain: one spectrum per search call, sequentially
     sampler = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    step_ms = []
-    ncands = []
+    step_ms, ncands = [], []
     t_all0 = time.perf_counter()
     for i in range(args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        c = plan.search(specs[i % 2], 0, nsearch)
+        c = plan.search(specs[i % nspec], 0, nsearch)
         e1.record()
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         ncands.append(len(c))
     torch.cuda.synchronize()
     barrier()
-    wall = time.perf_counter() - t_all0
+    plain_wall = time.perf_counter() - t_all0
+    plain_s = replicas.max_over_ranks(sum(step_ms) / 1000.0, dist, "cuda")
+    plain_value = world * args.steps / plain_s * 3600.0
+
+    # ---- plain drop-in: what accelsearch_GPU does per spectrum -- upload the
+    # host kernel bank, allocate a plan (-batchsize 8), copy the host spectrum,
+    # search, build the list, free everything
+    dropin = None
+    if served:
+        host_subs = []
+        for i, sb in enumerate(subs):
+            d = dict(sb)
+            d["kern"] = bank.rows(subs, i, range(sb["numw"] * sb["numz"])).reshape(
+                sb["numw"], sb["numz"], sb["fftlen"])
+            host_subs.append(d)
+        hspec = [specs[i % nspec].cpu().numpy() for i in range(2)]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for hs in hspec:
+            p1 = jerk.JerkPlan(obs, host_subs, batch=8)
+            p1.search(hs)
+            p1.close()
+        e1.record()
+        torch.cuda.synchronize()
+        dropin_s = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0, dist, "cuda")
+        dropin = {"value": world * len(hspec) / dropin_s * 3600.0,
+                  "ms_per_spectrum": dropin_s * 1000.0 / len(hspec), "batch_rsteps": 8}
+        del host_subs
+
+    # ---- served: the request loop, every spectrum of the job submitted at once
+    served_info = None
+    if served:
+        srv = jerk.JerkServer(max_active=args.max_active, batch=args.batch, device=local)
+        run_served(srv, specs[:1], True)  # warm: bank + plans
+        barrier()
+        job_s, service, total, ncand_s = run_served(srv, specs[: args.steps], True)
+        barrier()
+        srv.close()
+        job_s = replicas.max_over_ranks(job_s, dist, "cuda")
+        served_info = {"value": world * args.steps / job_s * 3600.0, "job_s": job_s,
+                       "service_ms": service, "queue_and_service_ms": total,
+                       "candidates": ncand_s}
     clocks = sampler.stop()
+
+    # ---- e2e: spectra in pinned host memory through the public API
+    e2e_steps = args.e2e_steps or (args.steps if served else max(1, min(args.steps, 2)))
+    host = [specs[i % nspec].cpu().pin_memory() for i in range(e2e_steps)]
+    hnp = [h.numpy() for h in host]
+    barrier()
+    if served:
+        srv = jerk.JerkServer(max_active=args.max_active, batch=args.batch, device=local)
+        run_served(srv, hnp[:1], False)
+        e2e_s, _, _, _ = run_served(srv, hnp, False)
+        srv.close()
+        h2d = len(hnp) * hnp[0].nbytes
+        d2h = None
+    else:
+        plan.reset_stats()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(e2e_steps):
+            plan.search(hnp[i], 0, nsearch)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_s = e0.elapsed_time(e1) / 1000.0
+        h2d, d2h = plan.transfer_stats()
+    e2e_s = replicas.max_over_ranks(e2e_s, dist, "cuda")
+    e2e_value = world * e2e_steps / e2e_s * 3600.0
+
+    # ---- roofline: one profiled search (CUDA events around every launch)
+    plan.reset_stats()
+    plan.set_profiling(True)
+    plan.search(specs[0], 0, nsearch)
+    torch.cuda.synchronize()
     plan.set_profiling(False)
     kstats = plan.kernel_stats()
-
-    total_ms = float(sum(step_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps / (total_ms / 1000.0) * 3600.0
-
-    # e2e: pinned host spectrum through the C ABI, copy-in and read-back timed
-    e2e_steps = args.e2e_steps or max(1, min(args.steps, 2))
-    host = [s.cpu().pin_memory() for s in specs]
-    hnp = [h.numpy() for h in host]
-    plan.reset_stats()
-    barrier()
-    torch.cuda.synchronize()
-    e2e_ms = []
-    for i in range(e2e_steps):
-        t0 = time.perf_counter()
-        plan.search(hnp[i % 2], 0, nsearch)
-        torch.cuda.synchronize()
-        e2e_ms.append((time.perf_counter() - t0) * 1000.0)
-    h2d, d2h = plan.transfer_stats()
-    e2e_total = float(sum(e2e_ms))
-    if dist is not None:
-        t = torch.tensor([e2e_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * e2e_steps / (e2e_total / 1000.0) * 3600.0
-
-    # roofline of the dominant kernel class
+    _, prof_d2h = plan.transfer_stats()
+    if d2h is None:
+        d2h = prof_d2h * e2e_steps
     dom = max(kstats.items(), key=lambda kv: kv[1]["ms"])
     dname, d = dom
     launches = max(d["launches"], 1)
     per_launch_s = d["ms"] / 1000.0 / launches
     achieved = d["bytes"] / launches / per_launch_s / 1e9
     peak, peak_kind = peaks()
-    launches_total = sum(v["launches"] for v in kstats.values())
+    launches_per_spectrum = sum(v["launches"] for v in kstats.values())
+    timed_spectra = args.steps * (2 if served else 1)
 
+    value = served_info["value"] if served else plain_value
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "ms_per_step": (served_info["job_s"] * 1000.0 / args.steps) if served
+            else statistics.mean(step_ms),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD if not nsearch else
                        f"{WORKLOAD} (PARTIAL: first {nsearch} rsteps per spectrum)",
-                       "numbins": N_SAMPLES // 2,
-                       "rsteps_per_spectrum": nrsteps, "batch_rsteps": args.batch,
-                       "form": "plain (one spectrum per search call)",
-                       "l2": "inputs larger than L2 (128 MiB spectrum, ~GB volumes per batch)",
+                       "numbins": N_SAMPLES // 2, "rsteps_per_spectrum": nrsteps,
+                       "batch_rsteps": args.batch,
+                       "form": ("served: one request loop per GPU, all step spectra submitted "
+                                f"at once, {args.max_active} in flight, shared resident bank")
+                       if served else "plain: one spectrum per search call",
+                       "timing": "CUDA events on the device timeline around the whole job "
+                                 "(served) or each search (plain); max over ranks",
+                       "l2": "inputs larger than L2 (128 MiB spectra, GB-sized volumes), no flush",
                        "parallelism": f"replicas x{world}"},
-            "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
-                           "p99": float(np.percentile(step_ms, 99))},
+            "plain": {"value": plain_value, "ms_per_spectrum": statistics.mean(step_ms),
+                      "p50_ms": float(np.percentile(step_ms, 50)),
+                      "p99_ms": float(np.percentile(step_ms, 99))},
+            "latency_ms": ({"p50": float(np.percentile(served_info["service_ms"], 50)),
+                            "p99": float(np.percentile(served_info["service_ms"], 99)),
+                            "p50_with_queue": float(np.percentile(
+                                served_info["queue_and_service_ms"], 50)),
+                            "p99_with_queue": float(np.percentile(
+                                served_info["queue_and_service_ms"], 99))}
+                           if served else
+                           {"p50": float(np.percentile(step_ms, 50)),
+                            "p99": float(np.percentile(step_ms, 99))}),
             "e2e": {"value": e2e_value, "unit": UNIT,
-                    "h2d_bytes_per_step": h2d // e2e_steps,
-                    "d2h_bytes_per_step": d2h // e2e_steps},
+                    "h2d_bytes_per_step": int(h2d // e2e_steps),
+                    "d2h_bytes_per_step": int(d2h // e2e_steps)},
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": None,
-                         "fp32_tflops": d["flops"] / launches / per_launch_s / 1e12},
+                         "fp32_tflops": d["flops"] / launches / per_launch_s / 1e12,
+                         "note": "corr kernels are FP32/shared-memory bound (see DESIGN.md)"},
             "kernels": {k: {"launches": v["launches"], "ms": v["ms"],
                             "share": v["ms"] / max(sum(x["ms"] for x in kstats.values()), 1e-9),
                             "gbs": v["bytes"] / max(v["ms"], 1e-9) / 1e6,
                             "tflops": v["flops"] / max(v["ms"], 1e-9) / 1e9}
                         for k, v in kstats.items()},
-            "gpu_launches": launches_total,
+            "gpu_launches": launches_per_spectrum * timed_spectra,
             "clocks": clocks,
-            "wall_s": wall,
+            "wall_s": plain_wall,
             "candidates_per_spectrum": ncands,
         }
+        if served:
+            line["plain_dropin"] = dropin
+            line["speedup_vs_plain"] = value / plain_value
+            line["speedup_vs_plain_dropin"] = value / dropin["value"]
         if world == 1 and not args.no_cpu_baseline and not nsearch:
             try:
                 from oracle import bindings as ob
