@@ -66,9 +66,22 @@ CAND_DTYPE = np.dtype([("power", np.float32), ("sigma", np.float32), ("numharm",
 _reflib = None
 
 
+def _quiet_wisdom() -> None:
+    """The reference's FFT wrapper (src/fftcalls.c:13-35) reads a wisdom file
+    from $PRESTO/lib and prints a warning to stdout when it is missing; point
+    PRESTO at an empty one so the reference prints nothing."""
+    d = os.path.join(REF_DIR, "presto_home")
+    f = os.path.join(d, "lib", "fftw_wisdom.txt")
+    if not os.path.exists(f):
+        os.makedirs(os.path.dirname(f), exist_ok=True)
+        open(f, "w").close()
+    os.environ["PRESTO"] = d
+
+
 def _ref():
     global _reflib
     if _reflib is None:
+        _quiet_wisdom()
         lib = C.CDLL(REF_LIB)
         lib.ref_open.restype = C.c_void_p
         lib.ref_open.argtypes = [C.c_int, C.POINTER(C.c_char_p)]

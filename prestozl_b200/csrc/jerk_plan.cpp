@@ -1240,6 +1240,9 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
 static int enqueue_search_pass(jerk_plan *p, const float2 *spec, long long first, long long count)
 {
     SearchDev a = make_args(p, spec);
+    // profiling times every launch alone: the harmonic sums then run on the
+    // main stream instead of overlapping the next batch's correlation
+    cudaStream_t hs = p->profiling ? p->stream : p->hstream;
     const size_t rinds_per_buf = (size_t)p->batch * p->nsubs * p->obs.corr_uselen;
     JERK_CUDA(cudaMemsetAsync(p->d_hit_count, 0, sizeof(unsigned int), p->stream));
     bool used[2] = {false, false};
@@ -1257,7 +1260,7 @@ static int enqueue_search_pass(jerk_plan *p, const float2 *spec, long long first
         if (rc != JERK_OK)
             return rc;
         JERK_CUDA(cudaEventRecord(p->ev_vol[i], p->stream));
-        JERK_CUDA(cudaStreamWaitEvent(p->hstream, p->ev_vol[i], 0));
+        JERK_CUDA(cudaStreamWaitEvent(hs, p->ev_vol[i], 0));
         // algorithmic traffic: every volume of the batch read once
         double bytes = 0, flops = 0;
         const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
@@ -1268,12 +1271,12 @@ static int enqueue_search_pass(jerk_plan *p, const float2 *spec, long long first
             bytes += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
         }
         flops = npts * p->nsubs;
-        const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops, p->hstream);
-        cudaError_t e = launch_harmsum(a, p->hstream);
-        launch_end(p, tok, p->hstream);
+        const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops, hs);
+        cudaError_t e = launch_harmsum(a, hs);
+        launch_end(p, tok, hs);
         if (e != cudaSuccess)
             return cuda_fail(e, "harmsum_kernel");
-        JERK_CUDA(cudaEventRecord(p->ev_free[i], p->hstream));
+        JERK_CUDA(cudaEventRecord(p->ev_free[i], hs));
         used[i] = true;
     }
     // join: the caller's stream sees every harmonic sum done

@@ -17,7 +17,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libjerk.so")
+LIB_PATH = os.environ.get("JERK_LIB", os.path.join(HERE, "lib", "libjerk.so"))
 
 JERK_OK = 0
 JERK_OVERFLOW = 1
