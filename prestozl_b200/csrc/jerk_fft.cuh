@@ -215,6 +215,24 @@ __host__ __device__ __forceinline__ constexpr int pad(int i) { return i ^ ((i >>
 template <int N>
 __host__ __device__ constexpr int fft_buf_len() { return N; }
 
+template <int X>
+struct IsPow2 {
+    static constexpr bool value = X > 0 && (X & (X - 1)) == 0;
+};
+
+// Swizzled address of element base + c, where base and the constant c have
+// no set bits in common (base < 2^k <= lowest set bit of c, as for
+// j + r * NB with j < NB, or idxD + r * Ns with j % Ns < Ns): then
+//   pad(base + c) = pad(base) ^ (c ^ ((c >> 4) & 15))
+// = (pad(base) ^ lo) + hi with compile-time lo (bits 0-3) and hi (bits >= 4),
+// so each access costs at most one XOR with an immediate.
+__device__ __forceinline__ int pad_add(int pbase, int c)
+{
+    const int lo = ((c >> 4) & 15) ^ (c & 15);
+    const int hi = c & ~15;
+    return (pbase ^ lo) + hi;
+}
+
 // One middle stage, in place in buf.  Every thread of the block must call it
 // (it holds two barriers); only threads with act == true (tid < T) work.
 template <int N, int SIGN, int T, int Ns, int R>
@@ -228,9 +246,16 @@ __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw,
         for (int p = 0; p < PER; p++) {
             const int j = tid + p * T;
             if (NB % T == 0 || j < NB) {
+                if constexpr (IsPow2<NB>::value && NB >= 16) {
+                    const int pj = pad(j);
 #pragma unroll
-                for (int r = 0; r < R; r++)
-                    v[p][r] = buf[pad(j + r * NB)];
+                    for (int r = 0; r < R; r++)
+                        v[p][r] = buf[pad_add(pj, r * NB)];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                        v[p][r] = buf[pad(j + r * NB)];
+                }
             }
         }
     }
@@ -248,9 +273,16 @@ __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw,
                 }
                 Dft<R, SIGN>::run(v[p]);
                 const int idxD = (j / Ns) * Ns * R + k;
+                if constexpr (IsPow2<Ns>::value && IsPow2<R>::value) {
+                    const int pd = pad(idxD);
 #pragma unroll
-                for (int r = 0; r < R; r++)
-                    buf[pad(idxD + r * Ns)] = v[p][r];
+                    for (int r = 0; r < R; r++)
+                        buf[pad_add(pd, r * Ns)] = v[p][r];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                        buf[pad(idxD + r * Ns)] = v[p][r];
+                }
             }
         }
     }
@@ -273,9 +305,16 @@ __device__ __forceinline__ void fft_stage_last(const float2 *buf, const float2 *
         const int j = tid + p * T;
         if (NB % T == 0 || j < NB) {
             float2 v[R];
+            if constexpr (IsPow2<NB>::value && NB >= 16) {
+                const int pj = pad(j);
 #pragma unroll
-            for (int r = 0; r < R; r++)
-                v[r] = buf[pad(j + r * NB)];
+                for (int r = 0; r < R; r++)
+                    v[r] = buf[pad_add(pj, r * NB)];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    v[r] = buf[pad(j + r * NB)];
+            }
 #pragma unroll
             for (int r = 1; r < R; r++)
                 v[r] = cmul(v[r], twiddle<SIGN>(tw, r * Ns + j));
@@ -338,9 +377,16 @@ __device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid
         for (int r = 0; r < R0; r++)
             v[r] = in(r);
         Dft<R0, SIGN>::run(v);
+        if constexpr (IsPow2<R0>::value) {
+            const int pd = pad(tid * R0);
 #pragma unroll
-        for (int r = 0; r < R0; r++)
-            buf[pad(tid * R0 + r)] = v[r];
+            for (int r = 0; r < R0; r++)
+                buf[pad_add(pd, r)] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R0; r++)
+                buf[pad(tid * R0 + r)] = v[r];
+        }
     }
     __syncthreads();
     FftTail<N, SIGN, T, 1, R0>::run(buf, tw, tid, act, out);
