@@ -277,7 +277,7 @@ size_t harmsum_smem_bytes(int nsubs, int numz0)
 // value is compared with that stage's cutoff.  Offsets are 32-bit (the
 // batch's volumes hold fewer than 2^32 floats; checked on the host).
 template <int S>
-__global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P)
+__global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 3 : 2) harmsum_kernel(const SearchDev P)
 {
     constexpr int NS = 1 << (S - 1);
     extern __shared__ int hsm[];
@@ -330,34 +330,67 @@ __global__ void __launch_bounds__(kHarmThreads) harmsum_kernel(const SearchDev P
         cut[st] = P.powcut[st];
 
     const float *planes = P.planes;
+    // subharmonics [0, NA) belong to stages 0 .. S-2, [NA, NS) to the last
+    constexpr int NA = NS > 1 ? NS / 2 : 1;
     for (int jj0 = 0; jj0 < numz0; jj0 += kHarmZ) {
         const bool full = jj0 + kHarmZ <= numz0;
-        // every gather of the four rows first (independent loads in flight),
-        // then the adds in the reference's order
-        float x[NS][kHarmZ];
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-            const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
-            x[s][0] = planes[off[s] + z.x];
-            x[s][1] = planes[off[s] + z.y];
-            x[s][2] = planes[off[s] + z.z];
-            x[s][3] = planes[off[s] + z.w];
-        }
         float v[kHarmZ];
+        // phase 1: every gather of stages 0 .. S-2 for the four rows in flight
+        // at once, then the adds in the reference's order
+        {
+            float x[NA][kHarmZ];
 #pragma unroll
-        for (int u = 0; u < kHarmZ; u++)
-            v[u] = x[0][u];
-        int s = 1;
+            for (int s = 0; s < NA; s++) {
+                const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
+                x[s][0] = planes[off[s] + z.x];
+                x[s][1] = planes[off[s] + z.y];
+                x[s][2] = planes[off[s] + z.z];
+                x[s][3] = planes[off[s] + z.w];
+            }
 #pragma unroll
-        for (int stage = 0; stage < S; stage++) {
-            if (stage > 0) {
+            for (int u = 0; u < kHarmZ; u++)
+                v[u] = x[0][u];
+            int s = 1;
 #pragma unroll
-                for (int h = 0; h < (1 << (stage - 1)); h++, s++) {
+            for (int stage = 0; stage < (S > 1 ? S - 1 : 1); stage++) {
+                if (stage > 0) {
 #pragma unroll
-                    for (int u = 0; u < kHarmZ; u++)
-                        v[u] = __fadd_rn(v[u], x[s][u]);
+                    for (int h = 0; h < (1 << (stage - 1)); h++, s++) {
+#pragma unroll
+                        for (int u = 0; u < kHarmZ; u++)
+                            v[u] = __fadd_rn(v[u], x[s][u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kHarmZ; u++) {
+                    const bool hit = valid && (full || jj0 + u < numz0) && v[u] > cut[stage];
+                    if (__any_sync(0xffffffffu, hit)) {
+                        const unsigned long long key =
+                            ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) * numz0 +
+                             (jj0 + u)) * P.corr_uselen + kk;
+                        record_hits(P, hit, lane, key, v[u]);
+                    }
                 }
             }
+        }
+        // phase 2: the last stage's subharmonics
+        if constexpr (S > 1) {
+            float x[NS - NA][kHarmZ];
+#pragma unroll
+            for (int s = NA; s < NS; s++) {
+                const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
+                x[s - NA][0] = planes[off[s] + z.x];
+                x[s - NA][1] = planes[off[s] + z.y];
+                x[s - NA][2] = planes[off[s] + z.z];
+                x[s - NA][3] = planes[off[s] + z.w];
+            }
+#pragma unroll
+            for (int s = NA; s < NS; s++) {
+#pragma unroll
+                for (int u = 0; u < kHarmZ; u++)
+                    v[u] = __fadd_rn(v[u], x[s - NA][u]);
+            }
+            constexpr int stage = S - 1;
 #pragma unroll
             for (int u = 0; u < kHarmZ; u++) {
                 const bool hit = valid && (full || jj0 + u < numz0) && v[u] > cut[stage];
