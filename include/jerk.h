@@ -127,14 +127,17 @@ int jerk_search(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
                 long long first_rstep, long long num_rsteps, jerk_cand **cands,
                 long long *ncands, jerk_hits *hits);
 
-/* The same search in two halves, so a host thread can keep several plans
- * busy: jerk_search_async stages the spectrum and enqueues every batch on the
- * plan's streams, then returns; jerk_search_ready reports (without blocking)
- * whether the device work is done (1), not yet (0) or failed (< 0);
- * jerk_search_collect waits for it and builds the candidate list.  One search
- * in flight per plan; a host spectrum must stay valid until collect. */
+/* The same search in parts, so one host thread can keep several plans busy:
+ * jerk_search_async stages the spectrum and enqueues the first few batches;
+ * jerk_search_advance(plan, ahead) enqueues more while fewer than `ahead`
+ * batches are queued or running (returns 1 while batches remain, 0 once all
+ * are enqueued); jerk_search_ready reports without blocking whether all the
+ * device work is done (1), not yet (0) or failed (< 0); jerk_search_collect
+ * enqueues whatever remains, waits, and builds the candidate list.  One
+ * search in flight per plan; a host spectrum must stay valid until collect. */
 int jerk_search_async(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
                       long long first_rstep, long long num_rsteps);
+int jerk_search_advance(jerk_plan *plan, int ahead);
 int jerk_search_ready(jerk_plan *plan);
 int jerk_search_collect(jerk_plan *plan, jerk_cand **cands, long long *ncands, jerk_hits *hits);
 
@@ -214,6 +217,9 @@ typedef struct jerk_server_config {
     int max_active;              /* searches in flight at once; 0 = 3 */
     int batch_rsteps;            /* rsteps per batch of each plan; 0 = 16 */
     int device;                  /* CUDA device the worker owns */
+    int batches_ahead;           /* batches each search keeps queued; 0 = 3 */
+    double queue_timeout_s;      /* a request not admitted within this fails
+                                    with JERK_TIMEOUT; 0 = never */
 } jerk_server_config;
 
 typedef struct jerk_request {

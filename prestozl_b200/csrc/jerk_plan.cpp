@@ -717,6 +717,16 @@ struct jerk_plan {
     unsigned int *d_status = nullptr;
     long long max_hits = 0;
     long long plane_floats = 0, prepped_f2 = 0;
+    // a search pass being enqueued batch by batch
+    struct Pass {
+        SearchDev a{};
+        cudaStream_t hs = nullptr;
+        long long first = 0, count = 0, next = 0, nbatch = 0, ndone = 0;
+        bool used[2] = {false, false};
+        bool all_enqueued = false;
+    } pass;
+    static constexpr int kRing = 16;
+    cudaEvent_t ev_batch[kRing] = {};  // harmonic sum of batch n done (n % kRing)
     // asynchronous search in flight (jerk_search_async / jerk_search_collect)
     bool in_flight = false;
     const float2 *inflight_spec = nullptr;
@@ -878,6 +888,9 @@ extern "C" void jerk_plan_destroy(jerk_plan *p)
     }
     if (p->ev_done)
         cudaEventDestroy(p->ev_done);
+    for (int i = 0; i < jerk_plan::kRing; i++)
+        if (p->ev_batch[i])
+            cudaEventDestroy(p->ev_batch[i]);
     if (p->h_counts)
         cudaFreeHost(p->h_counts);
     for (int i = 0; i < 2; i++) {
@@ -1111,6 +1124,8 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
                                             obs->corr_uselen));
     JERK_CUDA_B(cudaStreamCreateWithFlags(&p->hstream, cudaStreamNonBlocking));
     JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming));
+    for (int i = 0; i < jerk_plan::kRing; i++)
+        JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_batch[i], cudaEventDisableTiming));
     JERK_CUDA_B(cudaHostAlloc(&p->h_counts, 2 * sizeof(unsigned int), cudaHostAllocDefault));
     for (int i = 0; i < 2; i++) {
         JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_vol[i], cudaEventDisableTiming));
@@ -1236,59 +1251,123 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
     return JERK_OK;
 }
 
-// Enqueue one search pass on the plan's streams (no host synchronisation).
-static int enqueue_search_pass(jerk_plan *p, const float2 *spec, long long first, long long count)
+// A search pass is enqueued batch by batch, so a host thread driving several
+// plans can keep each a few batches ahead of the device instead of filling
+// the launch queue with one whole spectrum.
+
+static int pass_begin(jerk_plan *p, const float2 *spec, long long first, long long count)
 {
-    SearchDev a = make_args(p, spec);
+    jerk_plan::Pass &ps = p->pass;
+    ps = jerk_plan::Pass();
+    ps.a = make_args(p, spec);
     // profiling times every launch alone: the harmonic sums then run on the
     // main stream instead of overlapping the next batch's correlation
-    cudaStream_t hs = p->profiling ? p->stream : p->hstream;
-    const size_t rinds_per_buf = (size_t)p->batch * p->nsubs * p->obs.corr_uselen;
+    ps.hs = p->profiling ? p->stream : p->hstream;
+    ps.first = first;
+    ps.count = count;
+    ps.next = first;
     JERK_CUDA(cudaMemsetAsync(p->d_hit_count, 0, sizeof(unsigned int), p->stream));
-    bool used[2] = {false, false};
-    long long nbatch = 0;
-    for (long long k = first; k < first + count; k += p->batch, nbatch++) {
-        const int i = (int)(nbatch & 1);
-        a.first_rstep = k;
-        a.nb = (int)std::min<long long>(p->batch, first + count - k);
-        a.planes = p->d_planes + (size_t)i * p->plane_floats;
-        a.rinds = p->d_rinds + (size_t)i * rinds_per_buf;
-        // buffer i is free once the harmonic sum two batches back has read it
-        if (used[i])
-            JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
-        int rc = run_volumes(p, a);
-        if (rc != JERK_OK)
-            return rc;
-        JERK_CUDA(cudaEventRecord(p->ev_vol[i], p->stream));
-        JERK_CUDA(cudaStreamWaitEvent(hs, p->ev_vol[i], 0));
-        // algorithmic traffic: every volume of the batch read once
-        double bytes = 0, flops = 0;
-        const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
-        for (int s = 0; s < p->nsubs; s++) {
-            double numrs = 0;
-            for (int b = 0; b < a.nb; b++)
-                numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
-            bytes += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
-        }
-        flops = npts * p->nsubs;
-        const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops, hs);
-        cudaError_t e = launch_harmsum(a, hs);
-        launch_end(p, tok, hs);
-        if (e != cudaSuccess)
-            return cuda_fail(e, "harmsum_kernel");
-        JERK_CUDA(cudaEventRecord(p->ev_free[i], hs));
-        used[i] = true;
+    return JERK_OK;
+}
+
+// Batches whose harmonic sums have finished (non-blocking).
+static long long pass_done_batches(jerk_plan *p)
+{
+    jerk_plan::Pass &ps = p->pass;
+    while (ps.ndone < ps.nbatch && cudaEventQuery(p->ev_batch[ps.ndone % jerk_plan::kRing]) ==
+                                       cudaSuccess)
+        ps.ndone++;
+    return ps.ndone;
+}
+
+static int pass_enqueue_one(jerk_plan *p)
+{
+    jerk_plan::Pass &ps = p->pass;
+    SearchDev &a = ps.a;
+    cudaStream_t hs = ps.hs;
+    const size_t rinds_per_buf = (size_t)p->batch * p->nsubs * p->obs.corr_uselen;
+    const int i = (int)(ps.nbatch & 1);
+    const long long k = ps.next;
+    a.first_rstep = k;
+    a.nb = (int)std::min<long long>(p->batch, ps.first + ps.count - k);
+    a.planes = p->d_planes + (size_t)i * p->plane_floats;
+    a.rinds = p->d_rinds + (size_t)i * rinds_per_buf;
+    // buffer i is free once the harmonic sum two batches back has read it
+    if (ps.used[i])
+        JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
+    int rc = run_volumes(p, a);
+    if (rc != JERK_OK)
+        return rc;
+    JERK_CUDA(cudaEventRecord(p->ev_vol[i], p->stream));
+    JERK_CUDA(cudaStreamWaitEvent(hs, p->ev_vol[i], 0));
+    // algorithmic traffic: every volume of the batch read once
+    double bytes = 0, flops = 0;
+    const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
+    for (int s = 0; s < p->nsubs; s++) {
+        double numrs = 0;
+        for (int b = 0; b < a.nb; b++)
+            numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
+        bytes += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
     }
+    flops = npts * p->nsubs;
+    const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops, hs);
+    cudaError_t e = launch_harmsum(a, hs);
+    launch_end(p, tok, hs);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "harmsum_kernel");
+    JERK_CUDA(cudaEventRecord(p->ev_free[i], hs));
+    JERK_CUDA(cudaEventRecord(p->ev_batch[ps.nbatch % jerk_plan::kRing], hs));
+    ps.used[i] = true;
+    ps.next += a.nb;
+    ps.nbatch++;
+    return JERK_OK;
+}
+
+static int pass_finish_enqueue(jerk_plan *p)
+{
+    jerk_plan::Pass &ps = p->pass;
     // join: the caller's stream sees every harmonic sum done
     for (int i = 0; i < 2; i++)
-        if (used[i])
+        if (ps.used[i])
             JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
     JERK_CUDA(cudaMemcpyAsync(p->h_counts, p->d_hit_count, sizeof(unsigned int),
                               cudaMemcpyDeviceToHost, p->stream));
     JERK_CUDA(cudaMemcpyAsync(p->h_counts + 1, p->d_status, sizeof(unsigned int),
                               cudaMemcpyDeviceToHost, p->stream));
     JERK_CUDA(cudaEventRecord(p->ev_done, p->stream));
+    ps.all_enqueued = true;
     return JERK_OK;
+}
+
+// Enqueue batches until `ahead` of them are queued or running beyond those
+// finished (ahead <= 0: all of them).  Returns 1 while batches remain to be
+// enqueued, 0 once the pass is fully enqueued, < 0 on error.
+static int pass_advance(jerk_plan *p, int ahead)
+{
+    jerk_plan::Pass &ps = p->pass;
+    if (ps.all_enqueued)
+        return 0;
+    const int limit = ahead <= 0 ? 1 << 30 : std::min(ahead, jerk_plan::kRing - 2);
+    while (ps.next < ps.first + ps.count) {
+        if (ps.nbatch - pass_done_batches(p) >= limit)
+            return 1;
+        int rc = pass_enqueue_one(p);
+        if (rc != JERK_OK)
+            return rc;
+    }
+    int rc = pass_finish_enqueue(p);
+    return rc == JERK_OK ? 0 : rc;
+}
+
+// Enqueue one whole search pass (no host synchronisation beyond the
+// bookkeeping of pass_advance).
+static int enqueue_search_pass(jerk_plan *p, const float2 *spec, long long first, long long count)
+{
+    int rc = pass_begin(p, spec, first, count);
+    if (rc != JERK_OK)
+        return rc;
+    rc = pass_advance(p, 0);
+    return rc < 0 ? rc : JERK_OK;
 }
 
 // Wait for an enqueued pass and read its hit count.
@@ -1342,8 +1421,10 @@ extern "C" int jerk_search_async(jerk_plan *p, const void *spectrum, int spectru
     rc = stage_spectrum(p, spectrum, spectrum_on_device, &spec);
     if (rc != JERK_OK)
         return rc;
-    rc = enqueue_search_pass(p, spec, first_rstep, count);
-    if (rc != JERK_OK)
+    rc = pass_begin(p, spec, first_rstep, count);
+    if (rc == JERK_OK)
+        rc = pass_advance(p, 4);
+    if (rc < 0)
         return rc;
     p->in_flight = true;
     p->inflight_spec = spec;
@@ -1352,10 +1433,19 @@ extern "C" int jerk_search_async(jerk_plan *p, const void *spectrum, int spectru
     return JERK_OK;
 }
 
+extern "C" int jerk_search_advance(jerk_plan *p, int ahead)
+{
+    if (!p || !p->in_flight)
+        return 0;
+    return pass_advance(p, ahead);
+}
+
 extern "C" int jerk_search_ready(jerk_plan *p)
 {
     if (!p || !p->in_flight)
         return 1;
+    if (!p->pass.all_enqueued)
+        return 0;
     const cudaError_t e = cudaEventQuery(p->ev_done);
     if (e == cudaSuccess)
         return 1;
@@ -1371,7 +1461,10 @@ extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *n
         return fail(JERK_EINVAL, "jerk_search_collect: no search in flight");
     p->in_flight = false;
     unsigned int nh = 0;
-    int rc = finish_search_pass(p, &nh);
+    int rc = pass_advance(p, 0);  // whatever is not enqueued yet
+    if (rc < 0)
+        return rc;
+    rc = finish_search_pass(p, &nh);
     if (rc != JERK_OK)
         return rc;
     for (int attempt = 0; (long long)nh > p->max_hits; attempt++) {

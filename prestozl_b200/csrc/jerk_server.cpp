@@ -219,6 +219,15 @@ static bool admit(jerk_server *s, const Pending &pd)
     const long long bank_bytes =
         have_bank ? 0 : 8 * jerk_bank_elements(sl.geo.subs.data(), (int)sl.geo.subs.size());
     const long long need = (sl.plan ? 0 : plan_footprint(sl.geo, s->cfg.batch_rsteps)) + bank_bytes;
+    if (need > s->cfg.hbm_budget_bytes) {
+        // can never fit, even alone: fail this request, keep serving the rest
+        if (sl.plan)
+            s->idle.push_back(IdlePlan{sl.plan, sl.geo.obs, sl.key, sl.bytes});
+        if (have_bank)
+            release_bank(s, sl.key);
+        finish(s, pd.req, pd.t_submit, now_s(), JERK_ENOMEM, nullptr, 0);
+        return true;
+    }
     if (s->bytes_in_use + need > s->cfg.hbm_budget_bytes) {
         make_room(s, need);
         if (s->bytes_in_use + need > s->cfg.hbm_budget_bytes && !s->active.empty()) {
@@ -281,6 +290,24 @@ static void worker_main(jerk_server *s)
 {
     cudaSetDevice(s->cfg.device);
     for (;;) {
+        // requests that waited in the queue longer than allowed fail
+        if (s->cfg.queue_timeout_s > 0) {
+            std::vector<Pending> expired;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                const double t = now_s();
+                for (auto it = s->pending.begin(); it != s->pending.end();) {
+                    if (t - it->t_submit > s->cfg.queue_timeout_s) {
+                        expired.push_back(*it);
+                        it = s->pending.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+            }
+            for (auto &pd : expired)
+                finish(s, pd.req, pd.t_submit, now_s(), JERK_TIMEOUT, nullptr, 0);
+        }
         // admission
         for (;;) {
             Pending pd;
@@ -297,8 +324,15 @@ static void worker_main(jerk_server *s)
             std::lock_guard<std::mutex> lk(s->mu);
             s->pending.pop_front();
         }
-        // completions
+        // keep every active search a few batches ahead of the device, round
+        // robin, so their kernels interleave instead of queueing one behind
+        // another
         bool progressed = false;
+        for (auto &sl : s->active) {
+            const int adv = jerk_search_advance(sl.plan, s->cfg.batches_ahead);
+            (void)adv;  // errors surface through jerk_search_ready below
+        }
+        // completions
         for (size_t i = 0; i < s->active.size();) {
             Slot &sl = s->active[i];
             const int ready = jerk_search_ready(sl.plan);
@@ -342,6 +376,8 @@ extern "C" int jerk_server_create(jerk_server **out, const jerk_server_config *c
         s->cfg.max_active = 3;
     if (s->cfg.batch_rsteps <= 0)
         s->cfg.batch_rsteps = 16;
+    if (s->cfg.batches_ahead <= 0)
+        s->cfg.batches_ahead = 3;
     if (s->cfg.hbm_budget_bytes <= 0) {
         size_t fr = 0, tot = 0;
         cudaSetDevice(s->cfg.device);

@@ -70,7 +70,8 @@ class KernelStat(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_longlong), ("max_active", C.c_int),
-                ("batch_rsteps", C.c_int), ("device", C.c_int)]
+                ("batch_rsteps", C.c_int), ("device", C.c_int), ("batches_ahead", C.c_int),
+                ("queue_timeout_s", C.c_double)]
 
 
 class Request(C.Structure):
@@ -104,7 +105,7 @@ EXPORTS = [
     "jerk_last_error", "jerk_bank_elements", "jerk_bank_generate", "jerk_device_alloc",
     "jerk_device_free", "jerk_copy_to_host", "jerk_plan_set_profiling", "jerk_plan_reset_stats",
     "jerk_plan_kernel_stats", "jerk_plan_transfer_stats", "jerk_volume_static",
-    "jerk_search_async", "jerk_search_ready", "jerk_search_collect", "jerk_plan_device_bytes",
+    "jerk_search_async", "jerk_search_advance", "jerk_search_ready", "jerk_search_collect", "jerk_plan_device_bytes",
     "jerk_server_create", "jerk_server_submit", "jerk_server_poll", "jerk_server_stats",
     "jerk_server_destroy",
 ]
@@ -159,6 +160,7 @@ def lib() -> C.CDLL:
     L.jerk_plan_transfer_stats.restype = None
     L.jerk_search_async.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_longlong]
     L.jerk_search_ready.argtypes = [C.c_void_p]
+    L.jerk_search_advance.argtypes = [C.c_void_p, C.c_int]
     L.jerk_search_collect.argtypes = [C.c_void_p, C.POINTER(C.POINTER(Cand)),
                                       C.POINTER(C.c_longlong), C.POINTER(Hits)]
     L.jerk_plan_device_bytes.restype = C.c_longlong
@@ -410,8 +412,9 @@ class JerkServer:
     tensors) are kept alive here until their result has been polled."""
 
     def __init__(self, hbm_budget_bytes: int = 0, max_active: int = 0, batch: int = 0,
-                 device: int = 0):
-        cfg = ServerConfig(hbm_budget_bytes, max_active, batch, device)
+                 device: int = 0, batches_ahead: int = 0, queue_timeout_s: float = 0.0):
+        cfg = ServerConfig(hbm_budget_bytes, max_active, batch, device, batches_ahead,
+                           queue_timeout_s)
         self._s = C.c_void_p()
         _check(lib().jerk_server_create(C.byref(self._s), C.byref(cfg)))
         self._keep = {}

@@ -80,3 +80,35 @@ def test_admission_under_a_small_budget_still_finishes_everything():
     srv.close()
     assert sorted(tags) == [0, 1, 2] and st["failed"] == 0
     assert 0 < st["peak_bytes"] <= st["budget"]
+
+
+def test_requests_that_cannot_fit_or_wait_too_long_fail_alone():
+    """Fault handling on the host: a request larger than the whole budget and
+    requests left waiting past the queue deadline come back as errors while
+    the loop keeps serving the others."""
+    build.build()
+    specs = spectra()
+    # budget too small for any request: every one fails with ENOMEM
+    srv = jerk.JerkServer(hbm_budget_bytes=16 << 20, max_active=2, batch=4)
+    srv.submit(specs[0], *MIX[0][:6], tag=0)
+    with pytest.raises(jerk.JerkError) as ei:
+        srv.poll(60000)
+    assert ei.value.code == jerk.JERK_ENOMEM
+    srv.close()
+    # one slot and a short deadline: the request queued behind a long one
+    # times out, the long one still finishes
+    srv = jerk.JerkServer(max_active=1, batch=4, queue_timeout_s=0.05)
+    srv.submit(specs[0], *MIX[0][:6], tag=0)
+    srv.submit(specs[2], *MIX[2][:6], tag=1)
+    outcomes = {}
+    for _ in range(2):
+        try:
+            tag, cands, _ = srv.poll(60000)
+            outcomes[tag] = "ok"
+        except jerk.JerkError as e:
+            outcomes["err"] = e.code
+    st = srv.stats()
+    srv.close()
+    assert outcomes.get(0) == "ok"
+    assert outcomes.get("err") == jerk.JERK_TIMEOUT
+    assert st["failed"] == 1
