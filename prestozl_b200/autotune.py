@@ -1,0 +1,96 @@
+"""Autotuning of rsteps per launch (the batch size B) per search geometry.
+
+B trades kernel-bank reuse (each kernel row is read from HBM once per batch
+and kept in registers for B rsteps) against the size of the double-buffered
+ffdot volumes (2 x B x ~160 MB at -zmax 200 -wmax 300 -numharm 16) and the
+granularity of the overlap between a batch's harmonic sums and the next
+batch's correlations.  The best B depends on the geometry (fftlen, numz,
+numw, stages, corr_uselen), so it is measured once on a short partial search
+and cached in a JSON file (``$JERK_TUNE_CACHE``, default
+``~/.cache/prestozl_b200/autotune.json``).
+
+The FFT radix plans are fixed per fftlen (``csrc/jerk_fft.cuh``) and the
+kernels' tile shapes are compile-time; B is the run-time knob.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+from typing import Dict, Optional, Sequence
+
+from . import jerk
+
+DEFAULT_CANDIDATES = (8, 16, 32, 64)
+
+
+def cache_path() -> str:
+    return os.environ.get("JERK_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "prestozl_b200",
+                                       "autotune.json"))
+
+
+def geometry_key(obs: jerk.Obs, subs: Sequence[dict]) -> str:
+    f = subs[0]
+    return (f"fftlen={f['fftlen']}:numz={f['numz']}:numw={f['numw']}:"
+            f"stages={obs.numharmstages}:uselen={obs.corr_uselen}")
+
+
+def _load() -> Dict[str, dict]:
+    try:
+        with open(cache_path()) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(db: Dict[str, dict]) -> None:
+    path = cache_path()
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as fh:
+        json.dump(db, fh, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def cached_batch(obs: jerk.Obs, subs: Sequence[dict]) -> Optional[int]:
+    e = _load().get(geometry_key(obs, subs))
+    return int(e["batch_rsteps"]) if e else None
+
+
+def tune(obs: jerk.Obs, subs: Sequence[dict], bank_ptr: int, spectrum,
+         candidates: Sequence[int] = DEFAULT_CANDIDATES, rsteps: int = 1024,
+         use_cache: bool = True) -> dict:
+    """Time a partial search of ``rsteps`` rsteps for each candidate B (the
+    spectrum may be a CUDA tensor or a host array) and cache the fastest."""
+    import torch
+
+    key = geometry_key(obs, subs)
+    db = _load() if use_cache else {}
+    if use_cache and key in db:
+        return db[key]
+    times = {}
+    for B in candidates:
+        try:
+            plan = jerk.JerkPlan(obs, subs, batch=B, device_bank=bank_ptr)
+        except jerk.JerkError:
+            continue  # e.g. volumes beyond 32-bit offsets, or out of memory
+        n = min(rsteps, plan.num_rsteps)
+        plan.search(spectrum, 0, max(B, n // 4))  # warm
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.search(spectrum, 0, n)
+        e1.record()
+        torch.cuda.synchronize()
+        times[B] = e0.elapsed_time(e1) / n
+        plan.close()
+    if not times:
+        raise RuntimeError("no batch size could be planned")
+    best = min(times, key=times.get)
+    entry = {"batch_rsteps": best, "ms_per_rstep": {str(k): v for k, v in times.items()},
+             "rsteps_timed": rsteps}
+    if use_cache:
+        db[key] = entry
+        _store(db)
+    return entry

@@ -363,9 +363,12 @@ struct FftTail<N, SIGN, T, I, Ns, false> {
 // the threads that computed them; the caller must __syncthreads() before
 // buf is written again.  buf holds fft_buf_len<N>() float2; tw holds the
 // per-stage tables of FftPlan<N> (fft_stage_twiddles on the host).
-template <int N, int SIGN, class In, class Out>
+//
+// mid() is called by every thread right after the first-stage barrier, when
+// no thread will call in() again (the caller may then refill in()'s source).
+template <int N, int SIGN, class In, class Out, class Mid>
 __device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid, In &in,
-                                          Out &out)
+                                          Out &out, Mid &&mid)
 {
     using P = FftPlan<N>;
     constexpr int R0 = P::R0;
@@ -389,7 +392,15 @@ __device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid
         }
     }
     __syncthreads();
+    mid();
     FftTail<N, SIGN, T, 1, R0>::run(buf, tw, tid, act, out);
+}
+
+template <int N, int SIGN, class In, class Out>
+__device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid, In &in,
+                                          Out &out)
+{
+    fft_block<N, SIGN>(buf, tw, tid, in, out, [] {});
 }
 
 // Host: the per-stage twiddle tables of FftPlan<N>, forward sign, computed

@@ -126,13 +126,23 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
     }
     __syncthreads();
 
-    // spread_no_pad (data at even interbins) + forward FFT (sign -1)
+    // spread_no_pad (data at even interbins) + forward FFT (sign -1).  For a
+    // power-of-two fftlen the chunk is scaled by 1/fftlen here, exactly (a
+    // power of two), so the correlation's |y|^2 already carries the
+    // reference's 1/fftlen^2 and needs no multiply; other lengths keep it.
     float2 *outp = P.prepped + sd.data_off + (long long)b * N;
     auto in = [&](int r) -> float2 {
         const int m = tid + r * (N / R0);
         return (m & 1) ? make_float2(0.f, 0.f) : data[m >> 1];
     };
-    auto out = [&](int m, float2 y) { outp[m] = y; };
+    auto out = [&](int m, float2 y) {
+        if constexpr (IsPow2<N>::value) {
+            constexpr float inv = 1.0f / (float)N;
+            y.x = __fmul_rn(y.x, inv);
+            y.y = __fmul_rn(y.y, inv);
+        }
+        outp[m] = y;
+    };
     fft_block<N, -1>(buf, tw, tid, in, out);
 
     // rinds: fundamental r -> subharmonic r index (src/accel_utils.c:1114-1123)
@@ -185,6 +195,53 @@ struct CorrOcc {
     static constexpr int value = T >= 512 ? 1 : (T >= 256 ? 2 : (T >= 128 ? 4 : 8));
 };
 
+// Shared memory of corr_kernel<N>, in float2: the FFT buffer, the twiddle
+// tables and (when that still leaves CorrOcc CTAs per SM) a staging row for
+// the next rstep's prepared data.
+template <int N>
+struct CorrSmem {
+    static constexpr int kBase = (fft_buf_len<N>() + FftPlan<N>::twsize() + 1) & ~1;
+    static constexpr bool kStage = (size_t)(kBase + N) * 8 * CorrOcc<N>::value <= 220 * 1024;
+    static constexpr int value = kBase + (kStage ? N : 0);
+};
+
+// Bulk (TMA engine) copy of one data row into shared memory, completed on an
+// mbarrier, and the bounded wait for it.
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void bulk_row_load(void *dst, const void *src, unsigned bytes,
+                                              uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// Waits for phase `parity` of the mbarrier; gives up after a bounded number
+// of polls (each try_wait itself suspends for a bounded time) and returns
+// false.
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, unsigned parity)
+{
+    for (int it = 0; it < (1 << 16); it++) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
+// Status bits written by the kernels (read back after each pass).
+constexpr unsigned kStatusRind = 1u;     // harmsum: a subharmonic r index left its row
+constexpr unsigned kStatusCopy = 2u;     // corr: a data-row copy did not complete
+
 template <int N>
 __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     corr_kernel(const SearchDev P, const RowGroup G)
@@ -192,9 +249,12 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     constexpr int R0 = FftPlan<N>::R0;
     constexpr int T = FftPlan<N>::T;
     constexpr int TWN = FftPlan<N>::twsize();
-    extern __shared__ float2 sm2[];
+    constexpr bool kStage = CorrSmem<N>::kStage;
+    extern __shared__ __align__(16) float2 sm2[];
+    __shared__ uint64_t s_bar;
     float2 *buf = sm2;
     float2 *tw = sm2 + fft_buf_len<N>();
+    float2 *dsm = sm2 + CorrSmem<N>::kBase;  // staged data row (kStage)
     const int tid = threadIdx.x;
     const int row = blockIdx.x;
     int gi = 0;
@@ -203,6 +263,17 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     const int s = G.sub[gi];
     const int lrow = row - G.rowstart[gi];
     const SubDev sd = P.subs[s];
+    const float2 *D0 = P.prepped + sd.data_off;
+
+    if constexpr (kStage) {
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (tid == 0)
+            bulk_row_load(dsm, D0, N * sizeof(float2), &s_bar);
+    }
 
     for (int i = tid; i < TWN; i += T)
         tw[i] = P.twiddles[sd.twoff + i];
@@ -218,17 +289,35 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     const int offset = sd.halfwidth * 2;  // binoffset * ACCEL_NUMBETWEEN
     const float norm = sd.pownorm;
     for (int b = 0; b < P.nb; b++) {
-        const float2 *D = P.prepped + sd.data_off + (long long)b * N;
         const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
         float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
                       (long long)lrow * sd.stride;
-        auto in = [&](int r) -> float2 { return cmulconj(D[tid + r * (N / R0)], kreg[r]); };
         auto out = [&](int m, float2 y) {
             const int kk = m - offset;
-            if (kk >= 0 && kk < numrs)
-                outp[kk] = __fmul_rn(__fadd_rn(__fmul_rn(y.x, y.x), __fmul_rn(y.y, y.y)), norm);
+            if (kk >= 0 && kk < numrs) {
+                const float pw = __fadd_rn(__fmul_rn(y.x, y.x), __fmul_rn(y.y, y.y));
+                // power-of-two fftlen: 1/fftlen^2 is already in the chunk
+                outp[kk] = IsPow2<N>::value ? pw : __fmul_rn(pw, norm);
+            }
         };
-        fft_block<N, +1>(buf, tw, tid, in, out);
+        if constexpr (kStage) {
+            // rstep b's row is (or will shortly be) in dsm; once every thread
+            // has read it, thread 0 starts the copy of rstep b + 1's row
+            if (!bar_wait(&s_bar, b & 1) && P.status)
+                atomicOr(P.status, kStatusCopy);
+            auto in = [&](int r) -> float2 { return cmulconj(dsm[tid + r * (N / R0)], kreg[r]); };
+            auto mid = [&] {
+                if (tid == 0 && b + 1 < P.nb) {
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    bulk_row_load(dsm, D0 + (long long)(b + 1) * N, N * sizeof(float2), &s_bar);
+                }
+            };
+            fft_block<N, +1>(buf, tw, tid, in, out, mid);
+        } else {
+            const float2 *D = D0 + (long long)b * N;
+            auto in = [&](int r) -> float2 { return cmulconj(D[tid + r * (N / R0)], kreg[r]); };
+            fft_block<N, +1>(buf, tw, tid, in, out);
+        }
         __syncthreads();
     }
 }
@@ -236,27 +325,18 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
 // ---------------------------------------------------------------------------
 // 3. Harmonic summing + threshold + compaction.
 
-constexpr int kHarmThreads = 256;
+constexpr int kHarmThreads = 128;
 constexpr int kHarmZ = 4;  // fundamental z rows in flight per thread
 
-// Warp-aggregated append of one hit per lane with hit == true.
-__device__ __forceinline__ void record_hits(const SearchDev &P, bool hit, int lane,
-                                            unsigned long long key, float v)
+// Append one hit.  Hits are rare (a few per rstep at the usual sigma
+// cutoffs), so a plain per-thread atomic costs less than a warp vote on every
+// comparison; the host sorts the keys, so their order here does not matter.
+__device__ __forceinline__ void record_hit(const SearchDev &P, unsigned long long key, float v)
 {
-    const unsigned mask = __ballot_sync(0xffffffffu, hit);
-    if (!mask)
-        return;
-    const int leader = __ffs(mask) - 1;
-    unsigned int base = 0;
-    if (lane == leader)
-        base = atomicAdd(P.hit_count, (unsigned int)__popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (hit) {
-        const unsigned long long idx = base + __popc(mask & ((1u << lane) - 1u));
-        if ((long long)idx < P.max_hits) {
-            P.hit_keys[idx] = key;
-            P.hit_pows[idx] = v;
-        }
+    const unsigned int idx = atomicAdd(P.hit_count, 1u);
+    if ((long long)idx < P.max_hits) {
+        P.hit_keys[idx] = key;
+        P.hit_pows[idx] = v;
     }
 }
 
@@ -277,7 +357,7 @@ size_t harmsum_smem_bytes(int nsubs, int numz0)
 // value is compared with that stage's cutoff.  Offsets are 32-bit (the
 // batch's volumes hold fewer than 2^32 floats; checked on the host).
 template <int S>
-__global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 3 : 2) harmsum_kernel(const SearchDev P)
+__global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 6 : 4) harmsum_kernel(const SearchDev P)
 {
     constexpr int NS = 1 << (S - 1);
     extern __shared__ int hsm[];
@@ -290,7 +370,6 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 3 : 2) harmsum_kernel(c
     const int tid = threadIdx.x;
     const int kk = blockIdx.x * kHarmThreads + tid;
     const bool valid = kk < P.corr_uselen;
-    const int lane = tid & 31;
     const long long rstep = P.first_rstep + b;
 
     if (tid < NS) {
@@ -319,7 +398,7 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 3 : 2) harmsum_kernel(c
         if (ri >= (unsigned int)s_numrs[s]) {
             // cannot happen for tables built as the reference builds them;
             // record it and read a cell that exists
-            atomicOr(P.status, 1u);
+            atomicOr(P.status, kStatusRind);
             ri = 0;
         }
         off[s] = s_base[s] + ri;
@@ -363,13 +442,11 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 3 : 2) harmsum_kernel(c
                 }
 #pragma unroll
                 for (int u = 0; u < kHarmZ; u++) {
-                    const bool hit = valid && (full || jj0 + u < numz0) && v[u] > cut[stage];
-                    if (__any_sync(0xffffffffu, hit)) {
-                        const unsigned long long key =
-                            ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) * numz0 +
-                             (jj0 + u)) * P.corr_uselen + kk;
-                        record_hits(P, hit, lane, key, v[u]);
-                    }
+                    if (valid && (full || jj0 + u < numz0) && v[u] > cut[stage])
+                        record_hit(P,
+                                   ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) *
+                                        numz0 + (jj0 + u)) * P.corr_uselen + kk,
+                                   v[u]);
                 }
             }
         }
@@ -393,13 +470,11 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 3 : 2) harmsum_kernel(c
             constexpr int stage = S - 1;
 #pragma unroll
             for (int u = 0; u < kHarmZ; u++) {
-                const bool hit = valid && (full || jj0 + u < numz0) && v[u] > cut[stage];
-                if (__any_sync(0xffffffffu, hit)) {
-                    const unsigned long long key =
-                        ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) * numz0 +
-                         (jj0 + u)) * P.corr_uselen + kk;
-                    record_hits(P, hit, lane, key, v[u]);
-                }
+                if (valid && (full || jj0 + u < numz0) && v[u] > cut[stage])
+                    record_hit(P,
+                               ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) *
+                                    numz0 + (jj0 + u)) * P.corr_uselen + kk,
+                               v[u]);
             }
         }
     }
@@ -478,9 +553,12 @@ cudaError_t launch_prep(const SearchDev &P, int maxfft, cudaStream_t st)
 template <int N>
 static cudaError_t launch_corr_n(const SearchDev &P, const RowGroup &G, int rows, cudaStream_t st)
 {
-    const size_t smem = sizeof(float2) * (fft_buf_len<N>() + FftPlan<N>::twsize());
+    const size_t smem = sizeof(float2) * CorrSmem<N>::value;
     cudaError_t e = cudaFuncSetAttribute(corr_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(corr_kernel<N>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess)
         return e;
     corr_kernel<N><<<rows, FftPlan<N>::T, smem, st>>>(P, G);

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "jerk.h"
@@ -686,9 +687,6 @@ struct PendingTiming {
 struct jerk_plan {
     int device = 0;
     cudaStream_t stream = nullptr;   // prep + correlation (and the caller's work)
-    cudaStream_t hstream = nullptr;  // harmonic sums, overlapping the next batch's correlation
-    cudaEvent_t ev_vol[2] = {nullptr, nullptr};   // volumes of buffer i written
-    cudaEvent_t ev_free[2] = {nullptr, nullptr};  // buffer i read by its harmonic sum
     bool own_stream = false;
     jerk_obs obs{};
     int nsubs = 0, maxfft = 0, batch = 8;
@@ -720,10 +718,9 @@ struct jerk_plan {
     // a search pass being enqueued batch by batch
     struct Pass {
         SearchDev a{};
-        cudaStream_t hs = nullptr;
         long long first = 0, count = 0, next = 0, nbatch = 0, ndone = 0;
-        bool used[2] = {false, false};
         bool all_enqueued = false;
+        int error = 0;  // first enqueue failure (the pass is then abandoned)
     } pass;
     static constexpr int kRing = 16;
     cudaEvent_t ev_batch[kRing] = {};  // harmonic sum of batch n done (n % kRing)
@@ -767,8 +764,7 @@ static cudaEvent_t take_event(jerk_plan *p)
 }
 
 // Bracket one launch: returns a token to pass to launch_end.
-static int launch_begin(jerk_plan *p, int cls, double bytes, double flops,
-                        cudaStream_t st = nullptr)
+static int launch_begin(jerk_plan *p, int cls, double bytes, double flops)
 {
     KernelClass &k = p->classes[cls];
     k.launches++;
@@ -777,15 +773,15 @@ static int launch_begin(jerk_plan *p, int cls, double bytes, double flops,
     if (!p->profiling)
         return -1;
     PendingTiming t{cls, take_event(p), take_event(p)};
-    cudaEventRecord(t.start, st ? st : p->stream);
+    cudaEventRecord(t.start, p->stream);
     p->pending.push_back(t);
     return (int)p->pending.size() - 1;
 }
 
-static void launch_end(jerk_plan *p, int token, cudaStream_t st = nullptr)
+static void launch_end(jerk_plan *p, int token)
 {
     if (token >= 0)
-        cudaEventRecord(p->pending[token].stop, st ? st : p->stream);
+        cudaEventRecord(p->pending[token].stop, p->stream);
 }
 
 // after a stream synchronisation: fold the recorded intervals into the classes
@@ -882,10 +878,6 @@ extern "C" void jerk_plan_destroy(jerk_plan *p)
     }
     for (auto e : p->event_pool)
         cudaEventDestroy(e);
-    if (p->hstream) {
-        cudaStreamSynchronize(p->hstream);
-        cudaStreamDestroy(p->hstream);
-    }
     if (p->ev_done)
         cudaEventDestroy(p->ev_done);
     for (int i = 0; i < jerk_plan::kRing; i++)
@@ -893,12 +885,6 @@ extern "C" void jerk_plan_destroy(jerk_plan *p)
             cudaEventDestroy(p->ev_batch[i]);
     if (p->h_counts)
         cudaFreeHost(p->h_counts);
-    for (int i = 0; i < 2; i++) {
-        if (p->ev_vol[i])
-            cudaEventDestroy(p->ev_vol[i]);
-        if (p->ev_free[i])
-            cudaEventDestroy(p->ev_free[i]);
-    }
     if (p->own_stream && p->stream)
         cudaStreamDestroy(p->stream);
     cudaSetDevice(cur);
@@ -1117,20 +1103,17 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     JERK_CUDA_B(cudaMemcpyAsync(p->d_wind, wind.data(), sizeof(int) * wind.size(),
                                 cudaMemcpyHostToDevice, p->stream));
     JERK_CUDA_B(cudaMalloc(&p->d_prepped, sizeof(float2) * p->prepped_f2));
-    // two volume / rinds buffers: batch k+1's correlation writes one while
-    // batch k's harmonic sum reads the other
-    JERK_CUDA_B(cudaMalloc(&p->d_planes, 2 * sizeof(float) * p->plane_floats));
-    JERK_CUDA_B(cudaMalloc(&p->d_rinds, 2 * sizeof(uint16_t) * (size_t)p->batch * nsubs *
+    // one volume / rinds buffer: every launch of a pass runs on the plan's
+    // stream, so batch k + 1's correlation starts after batch k's harmonic
+    // sum has read the volumes (running the two side by side on two streams
+    // measured slower than back to back: their CTAs then share SMs)
+    JERK_CUDA_B(cudaMalloc(&p->d_planes, sizeof(float) * p->plane_floats));
+    JERK_CUDA_B(cudaMalloc(&p->d_rinds, sizeof(uint16_t) * (size_t)p->batch * nsubs *
                                             obs->corr_uselen));
-    JERK_CUDA_B(cudaStreamCreateWithFlags(&p->hstream, cudaStreamNonBlocking));
     JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming));
     for (int i = 0; i < jerk_plan::kRing; i++)
         JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_batch[i], cudaEventDisableTiming));
     JERK_CUDA_B(cudaHostAlloc(&p->h_counts, 2 * sizeof(unsigned int), cudaHostAllocDefault));
-    for (int i = 0; i < 2; i++) {
-        JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_vol[i], cudaEventDisableTiming));
-        JERK_CUDA_B(cudaEventCreateWithFlags(&p->ev_free[i], cudaEventDisableTiming));
-    }
     JERK_CUDA_B(cudaMalloc(&p->d_hit_count, sizeof(unsigned int)));
     JERK_CUDA_B(cudaMalloc(&p->d_status, sizeof(unsigned int)));
     JERK_CUDA_B(cudaMemsetAsync(p->d_status, 0, sizeof(unsigned int), p->stream));
@@ -1260,9 +1243,6 @@ static int pass_begin(jerk_plan *p, const float2 *spec, long long first, long lo
     jerk_plan::Pass &ps = p->pass;
     ps = jerk_plan::Pass();
     ps.a = make_args(p, spec);
-    // profiling times every launch alone: the harmonic sums then run on the
-    // main stream instead of overlapping the next batch's correlation
-    ps.hs = p->profiling ? p->stream : p->hstream;
     ps.first = first;
     ps.count = count;
     ps.next = first;
@@ -1284,22 +1264,14 @@ static int pass_enqueue_one(jerk_plan *p)
 {
     jerk_plan::Pass &ps = p->pass;
     SearchDev &a = ps.a;
-    cudaStream_t hs = ps.hs;
-    const size_t rinds_per_buf = (size_t)p->batch * p->nsubs * p->obs.corr_uselen;
-    const int i = (int)(ps.nbatch & 1);
     const long long k = ps.next;
     a.first_rstep = k;
     a.nb = (int)std::min<long long>(p->batch, ps.first + ps.count - k);
-    a.planes = p->d_planes + (size_t)i * p->plane_floats;
-    a.rinds = p->d_rinds + (size_t)i * rinds_per_buf;
-    // buffer i is free once the harmonic sum two batches back has read it
-    if (ps.used[i])
-        JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
+    a.planes = p->d_planes;
+    a.rinds = p->d_rinds;
     int rc = run_volumes(p, a);
     if (rc != JERK_OK)
         return rc;
-    JERK_CUDA(cudaEventRecord(p->ev_vol[i], p->stream));
-    JERK_CUDA(cudaStreamWaitEvent(hs, p->ev_vol[i], 0));
     // algorithmic traffic: every volume of the batch read once
     double bytes = 0, flops = 0;
     const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
@@ -1310,14 +1282,12 @@ static int pass_enqueue_one(jerk_plan *p)
         bytes += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
     }
     flops = npts * p->nsubs;
-    const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops, hs);
-    cudaError_t e = launch_harmsum(a, hs);
-    launch_end(p, tok, hs);
+    const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops);
+    cudaError_t e = launch_harmsum(a, p->stream);
+    launch_end(p, tok);
     if (e != cudaSuccess)
         return cuda_fail(e, "harmsum_kernel");
-    JERK_CUDA(cudaEventRecord(p->ev_free[i], hs));
-    JERK_CUDA(cudaEventRecord(p->ev_batch[ps.nbatch % jerk_plan::kRing], hs));
-    ps.used[i] = true;
+    JERK_CUDA(cudaEventRecord(p->ev_batch[ps.nbatch % jerk_plan::kRing], p->stream));
     ps.next += a.nb;
     ps.nbatch++;
     return JERK_OK;
@@ -1326,10 +1296,6 @@ static int pass_enqueue_one(jerk_plan *p)
 static int pass_finish_enqueue(jerk_plan *p)
 {
     jerk_plan::Pass &ps = p->pass;
-    // join: the caller's stream sees every harmonic sum done
-    for (int i = 0; i < 2; i++)
-        if (ps.used[i])
-            JERK_CUDA(cudaStreamWaitEvent(p->stream, p->ev_free[i], 0));
     JERK_CUDA(cudaMemcpyAsync(p->h_counts, p->d_hit_count, sizeof(unsigned int),
                               cudaMemcpyDeviceToHost, p->stream));
     JERK_CUDA(cudaMemcpyAsync(p->h_counts + 1, p->d_status, sizeof(unsigned int),
@@ -1345,6 +1311,8 @@ static int pass_finish_enqueue(jerk_plan *p)
 static int pass_advance(jerk_plan *p, int ahead)
 {
     jerk_plan::Pass &ps = p->pass;
+    if (ps.error)
+        return ps.error;
     if (ps.all_enqueued)
         return 0;
     const int limit = ahead <= 0 ? 1 << 30 : std::min(ahead, jerk_plan::kRing - 2);
@@ -1353,9 +1321,11 @@ static int pass_advance(jerk_plan *p, int ahead)
             return 1;
         int rc = pass_enqueue_one(p);
         if (rc != JERK_OK)
-            return rc;
+            return ps.error = rc;
     }
     int rc = pass_finish_enqueue(p);
+    if (rc != JERK_OK)
+        ps.error = rc;
     return rc == JERK_OK ? 0 : rc;
 }
 
@@ -1376,6 +1346,8 @@ static int finish_search_pass(jerk_plan *p, unsigned int *nhits_out)
     JERK_CUDA(cudaEventSynchronize(p->ev_done));
     collect_timings(p);
     p->d2h_bytes += 2 * sizeof(unsigned int);
+    if (p->h_counts[1] & 2u)
+        return fail(JERK_ECUDA, "correlation: a data-row copy into shared memory timed out");
     if (p->h_counts[1])
         return fail(JERK_EINVAL, "harmonic sum: a subharmonic r index left its row");
     *nhits_out = p->h_counts[0];
@@ -1444,6 +1416,8 @@ extern "C" int jerk_search_ready(jerk_plan *p)
 {
     if (!p || !p->in_flight)
         return 1;
+    if (p->pass.error)
+        return p->pass.error;
     if (!p->pass.all_enqueued)
         return 0;
     const cudaError_t e = cudaEventQuery(p->ev_done);
@@ -1462,8 +1436,10 @@ extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *n
     p->in_flight = false;
     unsigned int nh = 0;
     int rc = pass_advance(p, 0);  // whatever is not enqueued yet
-    if (rc < 0)
+    if (rc < 0) {
+        cudaStreamSynchronize(p->stream);  // what was enqueued ends before the plan is reused
         return rc;
+    }
     rc = finish_search_pass(p, &nh);
     if (rc != JERK_OK)
         return rc;
@@ -1484,11 +1460,12 @@ extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *n
     std::vector<unsigned long long> keys(nh);
     std::vector<float> pows(nh);
     if (nh) {
-        JERK_CUDA(cudaMemcpyAsync(keys.data(), p->d_hit_keys, sizeof(unsigned long long) * nh,
-                                  cudaMemcpyDeviceToHost, p->stream));
-        JERK_CUDA(cudaMemcpyAsync(pows.data(), p->d_hit_pows, sizeof(float) * nh,
-                                  cudaMemcpyDeviceToHost, p->stream));
-        JERK_CUDA(cudaStreamSynchronize(p->stream));
+        // the pass has ended (ev_done); a synchronous copy does not wait for
+        // other work queued behind it on a stream shared with other plans
+        JERK_CUDA(cudaMemcpy(keys.data(), p->d_hit_keys, sizeof(unsigned long long) * nh,
+                             cudaMemcpyDeviceToHost));
+        JERK_CUDA(cudaMemcpy(pows.data(), p->d_hit_pows, sizeof(float) * nh,
+                             cudaMemcpyDeviceToHost));
         p->d2h_bytes += (long long)nh * (sizeof(unsigned long long) + sizeof(float));
     }
     std::vector<uint32_t> order(nh);
@@ -1500,27 +1477,49 @@ extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *n
     const int S = p->obs.numharmstages;
     const long long numrs0 = p->obs.corr_uselen, numz0 = p->subs[0].numz,
                     numw0 = p->subs[0].numw;
-    CandList L;
-    for (uint32_t i = 0; i < nh; i++) {
-        unsigned long long key = keys[order[i]];
-        const int kk = (int)(key % numrs0);
-        key /= numrs0;
-        const int jj = (int)(key % numz0);
-        key /= numz0;
-        const int ii = (int)(key % numw0);
-        key /= numw0;
-        const int stage = (int)(key % S);
-        const long long rs = (long long)(key / S);
-        const int nhm = 1 << stage;
-        jerk_cand c;
-        c.power = pows[order[i]];
-        c.sigma = (float)jerk_candidate_sigma(c.power, nhm, (double)p->obs.numindep[stage]);
-        c.numharm = nhm;
-        c.r = ((double)p->hsteps[(size_t)rs * p->nsubs].rlo + kk * kDR) / (double)nhm;
-        c.z = (p->zlo0 + jj * (double)kDZ) / (double)nhm;
-        c.w = (p->wlo0 + ii * (double)kDW) / (double)nhm;
-        insert_cand(L, c);
+    // decode + sigma per hit (independent, so spread over host threads when
+    // there are many), then the insertions in key order (sequential: each
+    // depends on the list the earlier ones left)
+    std::vector<jerk_cand> cv(nh);
+    auto decode = [&](uint32_t lo, uint32_t hi) {
+        for (uint32_t i = lo; i < hi; i++) {
+            unsigned long long key = keys[order[i]];
+            const int kk = (int)(key % numrs0);
+            key /= numrs0;
+            const int jj = (int)(key % numz0);
+            key /= numz0;
+            const int ii = (int)(key % numw0);
+            key /= numw0;
+            const int stage = (int)(key % S);
+            const long long rs = (long long)(key / S);
+            const int nhm = 1 << stage;
+            jerk_cand &c = cv[i];
+            c.power = pows[order[i]];
+            c.sigma = (float)jerk_candidate_sigma(c.power, nhm, (double)p->obs.numindep[stage]);
+            c.numharm = nhm;
+            c.r = ((double)p->hsteps[(size_t)rs * p->nsubs].rlo + kk * kDR) / (double)nhm;
+            c.z = (p->zlo0 + jj * (double)kDZ) / (double)nhm;
+            c.w = (p->wlo0 + ii * (double)kDW) / (double)nhm;
+        }
+    };
+    const uint32_t nthr =
+        nh < 8192 ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (nthr == 1) {
+        decode(0, nh);
+    } else {
+        std::vector<std::thread> pool;
+        const uint32_t per = (nh + nthr - 1) / nthr;
+        for (uint32_t t = 0; t < nthr; t++) {
+            const uint32_t lo = t * per, hi = std::min(nh, lo + per);
+            if (lo < hi)
+                pool.emplace_back(decode, lo, hi);
+        }
+        for (auto &th : pool)
+            th.join();
     }
+    CandList L;
+    for (uint32_t i = 0; i < nh; i++)
+        insert_cand(L, cv[i]);
     if (hits) {
         hits->count = nh;
         hits->keys = (unsigned long long *)malloc(sizeof(unsigned long long) * (nh ? nh : 1));
@@ -1552,8 +1551,8 @@ extern "C" long long jerk_plan_device_bytes(const jerk_plan *p)
 {
     if (!p)
         return 0;
-    return (long long)(2 * sizeof(float) * p->plane_floats +
-                       2 * sizeof(uint16_t) * (size_t)p->batch * p->nsubs * p->obs.corr_uselen +
+    return (long long)(sizeof(float) * p->plane_floats +
+                       sizeof(uint16_t) * (size_t)p->batch * p->nsubs * p->obs.corr_uselen +
                        sizeof(float2) * p->prepped_f2 +
                        (sizeof(unsigned long long) + sizeof(float)) * p->max_hits +
                        sizeof(StepDev) * p->hsteps.size() + sizeof(float2) * p->spec_cap +

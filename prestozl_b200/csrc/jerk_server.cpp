@@ -3,13 +3,17 @@
 // Spectra arrive at any time (jerk_server_submit); a worker thread that owns
 // the device admits them while slots and HBM allow (footprint = ffdot volumes
 // + tables + hit buffer + the spectrum, plus the kernel bank if it is not
-// already resident), keeps several searches in flight at once on their own
-// streams (continuous batching: a new request starts as soon as another one
-// finishes and frees its slot, and its kernels interleave with the others'
-// on the device), and hands finished candidate lists back through
+// already resident), keeps several searches in flight at once (continuous
+// batching: a new request starts as soon as another one finishes and frees
+// its slot), and hands finished candidate lists back through
 // jerk_server_poll.  Kernel banks are generated on the GPU once per
 // (zmax, wmax, numharm, geometry) and shared by every request that matches;
 // idle plans with identical geometry are reused instead of reallocated.
+//
+// The active searches share one stream: the worker enqueues their batches
+// round-robin, a few ahead of the device each, so the GPU runs one kernel at
+// a time, back to back (kernels of different searches sharing SMs measured
+// slower than the same kernels in sequence), while every request advances.
 //
 // It is built only on the public C ABI of jerk.h, so its results are exactly
 // jerk_search's for the same spectrum and parameters, alone or in a mix.
@@ -84,6 +88,7 @@ bool same_obs(const jerk_obs &a, const jerk_obs &b) { return memcmp(&a, &b, size
 
 struct jerk_server {
     jerk_server_config cfg{};
+    cudaStream_t stream = nullptr;  // shared by every plan of this server
     std::thread worker;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -123,8 +128,8 @@ static BankKey key_of(const Geometry &g)
                    g.fftlen);
 }
 
-// Device bytes a plan for g will hold (volumes double-buffered, rinds, chunks,
-// hit buffer, steps, spectrum staging).
+// Device bytes a plan for g will hold (volumes, rinds, chunks, hit buffer,
+// steps, spectrum staging).
 static long long plan_footprint(const Geometry &g, int batch)
 {
     long long vol = 0, chunks = 0;
@@ -135,8 +140,8 @@ static long long plan_footprint(const Geometry &g, int batch)
         chunks += (long long)s.fftlen * 8;
     }
     const long long rsteps = (long long)((g.obs.highestbin - g.obs.rlo) / (g.obs.corr_uselen / 2)) + 1;
-    return 2 * vol * batch + chunks * batch +
-           2LL * 2 * batch * (long long)g.subs.size() * g.obs.corr_uselen +
+    return vol * batch + chunks * batch +
+           2LL * batch * (long long)g.subs.size() * g.obs.corr_uselen +
            (long long)(1 << 22) * 12 + rsteps * (long long)g.subs.size() * 24 +
            g.obs.numbins * 8 + (64LL << 20);
 }
@@ -262,6 +267,7 @@ static bool admit(jerk_server *s, const Pending &pd)
         jerk_config c{};
         c.batch_rsteps = s->cfg.batch_rsteps;
         c.device_bank = bank.ptr;
+        c.stream = s->stream;
         rc = jerk_plan_create(&sl.plan, &sl.geo.obs, sl.geo.subs.data(), (int)sl.geo.subs.size(), &c);
         if (rc != JERK_OK) {
             release_bank(s, sl.key);
@@ -328,10 +334,9 @@ static void worker_main(jerk_server *s)
         // robin, so their kernels interleave instead of queueing one behind
         // another
         bool progressed = false;
-        for (auto &sl : s->active) {
-            const int adv = jerk_search_advance(sl.plan, s->cfg.batches_ahead);
-            (void)adv;  // errors surface through jerk_search_ready below
-        }
+        for (auto &sl : s->active)
+            jerk_search_advance(sl.plan, s->cfg.batches_ahead);  // errors: jerk_search_ready
+
         // completions
         for (size_t i = 0; i < s->active.size();) {
             Slot &sl = s->active[i];
@@ -344,7 +349,13 @@ static void worker_main(jerk_server *s)
             long long n = 0;
             const int rc = ready < 0 ? ready : jerk_search_collect(sl.plan, &c, &n, nullptr);
             release_bank(s, sl.key);
-            s->idle.push_back(IdlePlan{sl.plan, sl.geo.obs, sl.key, sl.bytes});
+            if (rc < 0) {
+                // a plan whose search failed is not reused
+                jerk_plan_destroy(sl.plan);
+                s->bytes_in_use -= sl.bytes;
+            } else {
+                s->idle.push_back(IdlePlan{sl.plan, sl.geo.obs, sl.key, sl.bytes});
+            }
             finish(s, sl.req, sl.t_submit, sl.t_start, rc, c, n);
             s->active.erase(s->active.begin() + i);
             progressed = true;
@@ -386,6 +397,15 @@ extern "C" int jerk_server_create(jerk_server **out, const jerk_server_config *c
             return JERK_ECUDA;
         }
         s->cfg.hbm_budget_bytes = (long long)(0.85 * (double)fr);
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(s->cfg.device);
+    const cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    cudaSetDevice(cur);
+    if (e != cudaSuccess) {
+        delete s;
+        return JERK_ECUDA;
     }
     s->worker = std::thread(worker_main, s);
     *out = s;
@@ -444,5 +464,7 @@ extern "C" void jerk_server_destroy(jerk_server *s)
         s->worker.join();
     for (auto &r : s->done)
         jerk_free(r.cands);
+    if (s->stream)
+        cudaStreamDestroy(s->stream);
     delete s;
 }
