@@ -3,15 +3,16 @@
 Workload (the paper-scale configuration): 2^25-sample spectra (2^24 complex
 bins, dt = 54.6 us, T ~ 1832 s) of seeded Gaussian noise plus four injected
 pulsars, searched with -zmax 200 -wmax 300 -numharm 16 -sigma 3.0
-(23,366 rsteps of 718 bins per spectrum).  Data are synthetic (no dataset is
+(23,364 rsteps of 718 bins per spectrum).  Data are synthetic (no dataset is
 available offline); the reference's published runs used real GBT data.
 
 A step is one full search of one spectrum.  value: spectra/hour over K timed
 steps with the spectra already resident in HBM.  e2e: the same through the
 public C ABI with the spectrum in pinned host memory (host-to-device copy and
 the hit/candidate read-back inside the timed region).  Each spectrum (128 MiB)
-and the per-batch ffdot volumes (~1.3 GB) exceed the 126 MB L2, so no flush is
-needed between steps.
+and the per-batch ffdot volumes (163 MB per rstep, GBs per batch) exceed the
+126 MB L2, so no flush is needed between steps.  The rsteps per batch are
+autotuned (cached per geometry) unless --batch is given.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -42,6 +43,23 @@ N_SAMPLES = 1 << 25
 DT = 54.6e-6
 ZMAX, WMAX, NUMHARM, SIGMA = 200, 300, 16, 3.0
 WORKLOAD = "jerk search, 2^25-sample spectra, -zmax 200 -wmax 300 -numharm 16 -sigma 3.0"
+
+
+# FP32 CUDA-core peak of one B200 at its maximum SM clock (148 SMs x 128 FP32
+# lanes x 2 flops per FMA x 1965 MHz); the correlation kernels are bound by it.
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+# DRAM traffic of one corr_kernel<2048> launch at 8 rsteps per batch, from an
+# ncu capture (dram__bytes_read.sum / dram__bytes_write.sum) of
+#   python bench.py --rsteps 256 --steps 1 --warmup 1 --no-cpu-baseline --e2e-steps 1 --batch 8
+# The read side (kernel rows + data rows) is paid once per launch; the write
+# side (the volumes) grows with the rsteps per batch.
+CORR2048_TRAFFIC_B8 = {"read": 486.52288e6, "write": 1092.299e6, "batch": 8}
+
+
+def corr2048_traffic(batch: int) -> float:
+    t = CORR2048_TRAFFIC_B8
+    return t["read"] + t["write"] * batch / t["batch"]
 
 
 def peaks():
@@ -154,6 +172,32 @@ def reference_sample(spec_np, threads: int, target_s: float = 15.0, max_steps: i
     return dt / n, n, threads
 
 
+def reference_gpu(spec_np):
+    """The reference's own GPU search stage (accelsearch_cu: accel_kernels.cu +
+    cuFFT, compiled for sm_100a from its sources into oracle/_ref) on one
+    spectrum on this GPU, -batchsize 8: the plain reference on B200."""
+    from oracle import bindings as ob
+    from prestozl_b200 import synth
+
+    if not os.path.exists(getattr(ob, "REFGPU_CLI", "")):
+        return None
+    with tempfile.TemporaryDirectory() as tmp:
+        synth.write_fft(os.path.join(tmp, "paper"), spec_np, N_SAMPLES, DT)
+        ob.quiet_wisdom()
+        try:
+            out = subprocess.run([ob.REFGPU_CLI, "-zmax", str(ZMAX), "-wmax", str(WMAX),
+                                  "-numharm", str(NUMHARM), "-sigma", str(SIGMA),
+                                  "-batchsize", "8", "paper.fft"],
+                                 cwd=tmp, capture_output=True, text=True, timeout=900)
+            rec = json.loads([x for x in out.stderr.splitlines() if "refgpu_search_s" in x][-1])
+        except Exception as exc:  # reported, never required
+            return {"value": None, "error": str(exc)[:200]}
+    return {"value": 3600.0 / rec["refgpu_search_s"], "unit": UNIT,
+            "search_s": rec["refgpu_search_s"], "candidates": rec["ncands"], "batchsize": 8,
+            "what": "the reference's accelsearch_cu GPU stage (cuFFT), built for sm_100a, "
+                    "wall time of accelsearch_GPU on the same spectrum and GPU"}
+
+
 def run_reference(args):
     """--impl reference: the reference CPU search on this host's cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -239,11 +283,14 @@ def main():
                     help="spectra per timed job (plain: sequential searches; served: one burst)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=32, help="rsteps per batch")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="rsteps per batch (0: autotuned per geometry, cached)")
     ap.add_argument("--max-active", type=int, default=3, help="served: searches in flight")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip timing the reference's own GPU search on this GPU")
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--rsteps", type=int, default=0,
                     help="search only the first R rsteps of each spectrum (profiling runs; "
@@ -273,15 +320,21 @@ def main():
 
     obs, fftlen, subs = paper_setup()
     bank = jerk.DeviceBank(subs)
-    plan = jerk.JerkPlan(obs, subs, batch=args.batch, device_bank=bank.ptr.value)
-    nrsteps = plan.num_rsteps
-    nsearch = args.rsteps if args.rsteps > 0 else 0
-    served = not args.no_served and not nsearch
 
     # this rank's spectra, resident in HBM (each larger than L2)
     nspec = max(2, args.steps)
     specs = [make_spectrum(1000 * rank + i, "cuda") for i in range(nspec)]
     torch.cuda.synchronize()
+
+    tuned = None
+    if args.batch <= 0:
+        from prestozl_b200 import autotune
+        tuned = autotune.tune(obs, subs, bank.ptr.value, specs[0])
+        args.batch = tuned["batch_rsteps"]
+    plan = jerk.JerkPlan(obs, subs, batch=args.batch, device_bank=bank.ptr.value)
+    nrsteps = plan.num_rsteps
+    nsearch = args.rsteps if args.rsteps > 0 else 0
+    served = not args.no_served and not nsearch
 
     def barrier():
         if dist is not None:
@@ -394,7 +447,17 @@ def main():
     launches = max(d["launches"], 1)
     per_launch_s = d["ms"] / 1000.0 / launches
     achieved = d["bytes"] / launches / per_launch_s / 1e9
+    fp32_achieved = d["flops"] / launches / per_launch_s / 1e12
+    traffic = corr2048_traffic(args.batch) if dname == "corr_2048" else None
     peak, peak_kind = peaks()
+    hs = kstats.get("harmsum")
+    harmsum_roofline = None
+    if hs and hs["ms"] > 0:
+        hs_gbs = hs["bytes"] / (hs["ms"] / 1000.0) / 1e9
+        harmsum_roofline = {"bound": "hbm", "kernel": "harmsum", "achieved": hs_gbs,
+                            "peak": peak, "unit": "GB/s", "frac": hs_gbs / peak,
+                            "peak_source": peak_kind,
+                            "algorithmic": "every volume of the batch read once"}
     launches_per_spectrum = sum(v["launches"] for v in kstats.values())
     timed_spectra = args.steps * (2 if served else 1)
 
@@ -411,6 +474,7 @@ def main():
                        f"{WORKLOAD} (PARTIAL: first {nsearch} rsteps per spectrum)",
                        "numbins": N_SAMPLES // 2, "rsteps_per_spectrum": nrsteps,
                        "batch_rsteps": args.batch,
+                       "batch_autotune": tuned,
                        "form": ("served: one request loop per GPU, all step spectra submitted "
                                 f"at once, {args.max_active} in flight, shared resident bank")
                        if served else "plain: one spectrum per search call",
@@ -435,9 +499,15 @@ def main():
                     "d2h_bytes_per_step": int(d2h // e2e_steps)},
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind, "traffic": None,
-                         "fp32_tflops": d["flops"] / launches / per_launch_s / 1e12,
-                         "note": "corr kernels are FP32/shared-memory bound (see DESIGN.md)"},
+                         "peak_source": peak_kind, "traffic": traffic,
+                         "traffic_source": "ncu capture at 8 rsteps per batch, write side "
+                                           "scaled by rsteps per batch" if traffic else None,
+                         "fp32": {"achieved": fp32_achieved, "peak": FP32_PEAK_TFLOPS,
+                                  "unit": "TFLOP/s", "frac": fp32_achieved / FP32_PEAK_TFLOPS,
+                                  "peak_source": "nominal (148 SMs x 128 lanes x 2 x 1965 MHz)"},
+                         "note": "the correlation kernels are FP32-issue bound: the HBM "
+                                 "fraction is what they leave of the memory roofline"},
+            "roofline_harmsum": harmsum_roofline,
             "kernels": {k: {"launches": v["launches"], "ms": v["ms"],
                             "share": v["ms"] / max(sum(x["ms"] for x in kstats.values()), 1e-9),
                             "gbs": v["bytes"] / max(v["ms"], 1e-9) / 1e6,
@@ -466,6 +536,12 @@ def main():
                                   f"by {nrsteps} rsteps; OpenMP, FFT = project FFTW stand-in"}
             except Exception as exc:  # the baseline is reported, never required
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)}
+        if world == 1 and not args.no_ref_gpu and not nsearch:
+            ref_gpu = reference_gpu(specs[0].cpu().numpy())
+            if ref_gpu:
+                line["reference_gpu"] = ref_gpu
+                if ref_gpu.get("value"):
+                    line["speedup_vs_reference_gpu"] = value / ref_gpu["value"]
         print(json.dumps(line))
 
     plan.close()

@@ -24,6 +24,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 REF_LIB = os.path.join(REF_DIR, "libprestoref.so")
 REF_CLI = os.path.join(REF_DIR, "accelsearch")
 DROPIN_CLI = os.path.join(REF_DIR, "accelsearch_b200")
+REFGPU_CLI = os.path.join(REF_DIR, "accelsearch_refgpu")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REFERENCE_SOURCES = "/root/reference"
 
@@ -33,7 +34,7 @@ def build(reference: Optional[bool] = None) -> None:
     reference sources are present)."""
     if reference is None:
         reference = os.path.isdir(os.path.join(REFERENCE_SOURCES, "src"))
-    targets = ["oracle"] + (["ref", "dropin"] if reference else [])
+    targets = ["oracle"] + (["ref", "dropin", "refgpu"] if reference else [])
     subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
 
 
@@ -66,7 +67,7 @@ CAND_DTYPE = np.dtype([("power", np.float32), ("sigma", np.float32), ("numharm",
 _reflib = None
 
 
-def _quiet_wisdom() -> None:
+def quiet_wisdom() -> None:
     """The reference's FFT wrapper (src/fftcalls.c:13-35) reads a wisdom file
     from $PRESTO/lib and prints a warning to stdout when it is missing; point
     PRESTO at an empty one so the reference prints nothing."""
@@ -81,7 +82,7 @@ def _quiet_wisdom() -> None:
 def _ref():
     global _reflib
     if _reflib is None:
-        _quiet_wisdom()
+        quiet_wisdom()
         lib = C.CDLL(REF_LIB)
         lib.ref_open.restype = C.c_void_p
         lib.ref_open.argtypes = [C.c_int, C.POINTER(C.c_char_p)]

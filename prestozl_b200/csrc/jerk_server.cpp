@@ -296,7 +296,24 @@ static void worker_main(jerk_server *s)
 {
     cudaSetDevice(s->cfg.device);
     for (;;) {
-        // requests that waited in the queue longer than allowed fail
+        // admission
+        for (;;) {
+            Pending pd;
+            {
+                std::unique_lock<std::mutex> lk(s->mu);
+                if (s->stop && s->pending.empty() && s->active.empty())
+                    goto out;
+                if (s->pending.empty() || (int)s->active.size() >= s->cfg.max_active)
+                    break;
+                pd = s->pending.front();
+            }
+            if (!admit(s, pd))
+                break;
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->pending.pop_front();
+        }
+        // requests still waiting after admission had its chance, longer than
+        // allowed, fail
         if (s->cfg.queue_timeout_s > 0) {
             std::vector<Pending> expired;
             {
@@ -314,25 +331,8 @@ static void worker_main(jerk_server *s)
             for (auto &pd : expired)
                 finish(s, pd.req, pd.t_submit, now_s(), JERK_TIMEOUT, nullptr, 0);
         }
-        // admission
-        for (;;) {
-            Pending pd;
-            {
-                std::unique_lock<std::mutex> lk(s->mu);
-                if (s->stop && s->pending.empty() && s->active.empty())
-                    goto out;
-                if (s->pending.empty() || (int)s->active.size() >= s->cfg.max_active)
-                    break;
-                pd = s->pending.front();
-            }
-            if (!admit(s, pd))
-                break;
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->pending.pop_front();
-        }
         // keep every active search a few batches ahead of the device, round
-        // robin, so their kernels interleave instead of queueing one behind
-        // another
+        // robin, so every admitted request advances
         bool progressed = false;
         for (auto &sl : s->active)
             jerk_search_advance(sl.plan, s->cfg.batches_ahead);  // errors: jerk_search_ready

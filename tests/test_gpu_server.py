@@ -95,9 +95,10 @@ def test_requests_that_cannot_fit_or_wait_too_long_fail_alone():
         srv.poll(60000)
     assert ei.value.code == jerk.JERK_ENOMEM
     srv.close()
-    # one slot and a short deadline: the request queued behind a long one
-    # times out, the long one still finishes
-    srv = jerk.JerkServer(max_active=1, batch=4, queue_timeout_s=0.05)
+    # one slot and a deadline of ~zero: the loop admits what fits before it
+    # expires what still waits, so the first request takes the slot and the
+    # one queued behind it times out; the first still finishes
+    srv = jerk.JerkServer(max_active=1, batch=4, queue_timeout_s=1e-9)
     srv.submit(specs[0], *MIX[0][:6], tag=0)
     srv.submit(specs[2], *MIX[2][:6], tag=1)
     outcomes = {}
