@@ -327,11 +327,14 @@ def main():
     torch.cuda.synchronize()
 
     tuned = None
+    harm_mode = 0
     if args.batch <= 0:
         from prestozl_b200 import autotune
         tuned = autotune.tune(obs, subs, bank.ptr.value, specs[0])
         args.batch = tuned["batch_rsteps"]
-    plan = jerk.JerkPlan(obs, subs, batch=args.batch, device_bank=bank.ptr.value)
+        harm_mode = tuned.get("harm_mode", 0)
+    plan = jerk.JerkPlan(obs, subs, batch=args.batch, device_bank=bank.ptr.value,
+                         harm_mode=harm_mode)
     nrsteps = plan.num_rsteps
     nsearch = args.rsteps if args.rsteps > 0 else 0
     served = not args.no_served and not nsearch
@@ -394,7 +397,8 @@ def main():
     # ---- served: the request loop, every spectrum of the job submitted at once
     served_info = None
     if served:
-        srv = jerk.JerkServer(max_active=args.max_active, batch=args.batch, device=local)
+        srv = jerk.JerkServer(max_active=args.max_active, batch=args.batch, device=local,
+                              harm_mode=harm_mode)
         run_served(srv, specs[:1], True)  # warm: bank + plans
         barrier()
         job_s, service, total, ncand_s = run_served(srv, specs[: args.steps], True)
@@ -412,7 +416,8 @@ def main():
     hnp = [h.numpy() for h in host]
     barrier()
     if served:
-        srv = jerk.JerkServer(max_active=args.max_active, batch=args.batch, device=local)
+        srv = jerk.JerkServer(max_active=args.max_active, batch=args.batch, device=local,
+                              harm_mode=harm_mode)
         run_served(srv, hnp[:1], False)
         e2e_s, _, _, _ = run_served(srv, hnp, False)
         srv.close()

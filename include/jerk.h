@@ -96,6 +96,17 @@ typedef struct jerk_config {
     long long max_hits;       /* initial hit-buffer capacity; 0 = auto */
     void *stream;             /* cudaStream_t to run on; NULL = a private stream */
     const void *device_bank;  /* optional resident bank (jerk_bank_generate) */
+    int harm_mode;            /* harmonic-sum kernel (a tuning knob; results do
+                                 not depend on it): 1 = gather (global loads),
+                                 2 = gather + TMA prefetch of the next tile into
+                                 L2, 3 / 4 = TMA copies of 8 / 16-row tiles into
+                                 shared memory (modes 2-4 fall back to 1 where
+                                 tensor maps cannot be built); 0 = 1 */
+    int use_graph;            /* nonzero: each jerk_search / jerk_search_async
+                                 pass is captured once per (first_rstep,
+                                 num_rsteps) into a CUDA graph and replayed for
+                                 later spectra (the spectrum is staged into a
+                                 plan buffer first); 0 = launch batch by batch */
 } jerk_config;
 
 typedef struct jerk_plan jerk_plan;
@@ -220,6 +231,7 @@ typedef struct jerk_server_config {
     int batches_ahead;           /* batches each search keeps queued; 0 = 3 */
     double queue_timeout_s;      /* a request not admitted within this fails
                                     with JERK_TIMEOUT; 0 = never */
+    int harm_mode;               /* jerk_config.harm_mode of every plan */
 } jerk_server_config;
 
 typedef struct jerk_request {

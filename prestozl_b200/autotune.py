@@ -10,7 +10,9 @@ and cached in a JSON file (``$JERK_TUNE_CACHE``, default
 ``~/.cache/prestozl_b200/autotune.json``).
 
 The FFT radix plans are fixed per fftlen (``csrc/jerk_fft.cuh``) and the
-kernels' tile shapes are compile-time; B is the run-time knob.
+kernels' tile shapes are compile-time; the run-time knobs are B and the
+harmonic-sum kernel (jerk_config.harm_mode: plain gathers, gathers with TMA
+prefetch into L2, or TMA tiles in shared memory).
 """
 
 from __future__ import annotations
@@ -21,7 +23,8 @@ from typing import Dict, Optional, Sequence
 
 from . import jerk
 
-DEFAULT_CANDIDATES = (8, 16, 32, 64)
+DEFAULT_CANDIDATES = (16, 32, 64)
+DEFAULT_HARM_MODES = (1, 2, 4)
 
 
 def cache_path() -> str:
@@ -53,16 +56,18 @@ def _store(db: Dict[str, dict]) -> None:
     os.replace(tmp, path)
 
 
-def cached_batch(obs: jerk.Obs, subs: Sequence[dict]) -> Optional[int]:
-    e = _load().get(geometry_key(obs, subs))
-    return int(e["batch_rsteps"]) if e else None
+def cached(obs: jerk.Obs, subs: Sequence[dict]) -> Optional[dict]:
+    """The cached choice for this geometry ({"batch_rsteps", "harm_mode", ...})."""
+    return _load().get(geometry_key(obs, subs))
 
 
 def tune(obs: jerk.Obs, subs: Sequence[dict], bank_ptr: int, spectrum,
-         candidates: Sequence[int] = DEFAULT_CANDIDATES, rsteps: int = 1024,
+         candidates: Sequence[int] = DEFAULT_CANDIDATES,
+         harm_modes: Sequence[int] = DEFAULT_HARM_MODES, rsteps: int = 1024,
          use_cache: bool = True) -> dict:
-    """Time a partial search of ``rsteps`` rsteps for each candidate B (the
-    spectrum may be a CUDA tensor or a host array) and cache the fastest."""
+    """Time a partial search of ``rsteps`` rsteps for each (B, harm_mode) pair
+    (the spectrum may be a CUDA tensor or a host array) and cache the fastest.
+    Both knobs change only speed: the candidates are the same for all."""
     import torch
 
     key = geometry_key(obs, subs)
@@ -71,24 +76,27 @@ def tune(obs: jerk.Obs, subs: Sequence[dict], bank_ptr: int, spectrum,
         return db[key]
     times = {}
     for B in candidates:
-        try:
-            plan = jerk.JerkPlan(obs, subs, batch=B, device_bank=bank_ptr)
-        except jerk.JerkError:
-            continue  # e.g. volumes beyond 32-bit offsets, or out of memory
-        n = min(rsteps, plan.num_rsteps)
-        plan.search(spectrum, 0, max(B, n // 4))  # warm
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        plan.search(spectrum, 0, n)
-        e1.record()
-        torch.cuda.synchronize()
-        times[B] = e0.elapsed_time(e1) / n
-        plan.close()
+        for hr in harm_modes:
+            try:
+                plan = jerk.JerkPlan(obs, subs, batch=B, device_bank=bank_ptr, harm_mode=hr)
+            except jerk.JerkError:
+                continue  # e.g. volumes beyond 32-bit offsets, or out of memory
+            n = min(rsteps, plan.num_rsteps)
+            plan.search(spectrum, 0, max(B, n // 4))  # warm
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plan.search(spectrum, 0, n)
+            e1.record()
+            torch.cuda.synchronize()
+            times[(B, hr)] = e0.elapsed_time(e1) / n
+            plan.close()
     if not times:
         raise RuntimeError("no batch size could be planned")
     best = min(times, key=times.get)
-    entry = {"batch_rsteps": best, "ms_per_rstep": {str(k): v for k, v in times.items()},
+    entry = {"batch_rsteps": best[0], "harm_mode": best[1],
+             "ms_per_rstep": {f"B{k[0]}/mode{k[1]}": v for k, v in times.items()},
              "rsteps_timed": rsteps}
     if use_cache:
         db[key] = entry

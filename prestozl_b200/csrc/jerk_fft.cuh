@@ -235,6 +235,8 @@ __device__ __forceinline__ int pad_add(int pbase, int c)
 
 // One middle stage, in place in buf.  Every thread of the block must call it
 // (it holds two barriers); only threads with act == true (tid < T) work.
+// The twiddles and the butterfly run before the first barrier: only the
+// writes must wait until every thread has read its inputs.
 template <int N, int SIGN, int T, int Ns, int R>
 __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw, int tid, bool act)
 {
@@ -256,6 +258,13 @@ __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw,
                     for (int r = 0; r < R; r++)
                         v[p][r] = buf[pad(j + r * NB)];
                 }
+                const int k = j % Ns;
+                if (Ns > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; r++)
+                        v[p][r] = cmul(v[p][r], twiddle<SIGN>(tw, r * Ns + k));
+                }
+                Dft<R, SIGN>::run(v[p]);
             }
         }
     }
@@ -266,12 +275,6 @@ __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw,
             const int j = tid + p * T;
             if (NB % T == 0 || j < NB) {
                 const int k = j % Ns;
-                if (Ns > 1) {
-#pragma unroll
-                    for (int r = 1; r < R; r++)
-                        v[p][r] = cmul(v[p][r], twiddle<SIGN>(tw, r * Ns + k));
-                }
-                Dft<R, SIGN>::run(v[p]);
                 const int idxD = (j / Ns) * Ns * R + k;
                 if constexpr (IsPow2<Ns>::value && IsPow2<R>::value) {
                     const int pd = pad(idxD);

@@ -326,7 +326,6 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
 // 3. Harmonic summing + threshold + compaction.
 
 constexpr int kHarmThreads = 128;
-constexpr int kHarmZ = 4;  // fundamental z rows in flight per thread
 
 // Append one hit.  Hits are rare (a few per rstep at the usual sigma
 // cutoffs), so a plain per-thread atomic costs less than a warp vote on every
@@ -342,8 +341,9 @@ __device__ __forceinline__ void record_hit(const SearchDev &P, unsigned long lon
 
 // Shared memory (dynamic): zrow[s][jj] = zinds_s[jj] * stride_s, the row
 // offset inside subharmonic s's volume for fundamental z row jj; rows are
-// padded to a multiple of 4 entries so four rows load as one int4.
-__host__ __device__ __forceinline__ int zrow_pitch(int numz0) { return (numz0 + 3) & ~3; }
+// padded to a multiple of 8 entries (zero offsets past numz0) so a thread's
+// 4 or 8 rows load as int4s.
+__host__ __device__ __forceinline__ int zrow_pitch(int numz0) { return (numz0 + 7) & ~7; }
 
 size_t harmsum_smem_bytes(int nsubs, int numz0)
 {
@@ -351,14 +351,43 @@ size_t harmsum_smem_bytes(int nsubs, int numz0)
 }
 
 // Thread = one fundamental r (kk) of one w row (ii) of one rstep (b); it
-// walks all z rows four at a time.  Per point the float adds run in the
+// walks all z rows ZU at a time.  Used where the TMA path's boxes (below)
+// do not fit in shared memory.  Per point the float adds run in the
 // reference's order: stage 1 adds 1/2, stage 2 adds 1/4 then 3/4, ...
 // (src/accel_utils.c:1356-1377 applied stage by stage); after each stage the
 // value is compared with that stage's cutoff.  Offsets are 32-bit (the
 // batch's volumes hold fewer than 2^32 floats; checked on the host).
-template <int S>
-__global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 6 : 4) harmsum_kernel(const SearchDev P)
+template <int S, int ZU>
+struct HarmOcc {
+    static constexpr int value = ZU <= 4 ? (S <= 5 ? 6 : 4) : (S <= 5 ? 4 : 2);
+};
+
+// L2 prefetch, by the copy engine, of the boxes (HarmTma) that fundamental
+// rows [j0, j0 + kPrefetchRows) of this CTA will gather: one tensor prefetch
+// per subharmonic, no shared memory, nothing to wait for.
+constexpr int kPrefetchRows = 16;
+
+template <int NS>
+__device__ __forceinline__ void prefetch_tile(const SearchDev &P, const HarmTma &T, int j0,
+                                              const int *rstart, const int *wind, int b)
 {
+    if (j0 >= P.numz0)
+        return;
+    for (int s = 0; s < NS; s++) {
+        const int zs = s == 0 ? j0 : P.zinds[P.subs[s].zinds_off + j0];
+        asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];"
+                     :: "l"(reinterpret_cast<uint64_t>(&T.map[s])), "r"(rstart[s]), "r"(zs),
+                        "r"(wind[s]), "r"(b)
+                     : "memory");
+    }
+}
+
+template <int S, int ZU, bool PF>
+__global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
+    harmsum_kernel(const SearchDev P, const __grid_constant__ HarmTma T)
+{
+    constexpr int kHarmZ = ZU;
+    static_assert(ZU == 4 || ZU == 8, "whole int4s of z offsets");
     constexpr int NS = 1 << (S - 1);
     extern __shared__ int hsm[];
     __shared__ unsigned int s_base[NS];
@@ -372,12 +401,20 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 6 : 4) harmsum_kernel(c
     const bool valid = kk < P.corr_uselen;
     const long long rstep = P.first_rstep + b;
 
+    __shared__ int s_pwind[NS], s_prstart[NS];  // prefetch box corners (PF)
     if (tid < NS) {
         const SubDev sd = P.subs[tid];
         const int wind = tid == 0 ? ii : P.wind[sd.wind_off + ii];
         s_base[tid] = (unsigned int)(sd.plane_off + (long long)b * sd.plane_size +
                                      (long long)wind * sd.numz * sd.stride);
         s_numrs[tid] = P.steps[rstep * NS + tid].numrs;
+        if constexpr (PF) {
+            const int k0 = blockIdx.x * kHarmThreads;
+            s_pwind[tid] = wind;
+            s_prstart[tid] = tid == 0 ? k0
+                                      : (int)(P.rinds[((long long)b * NS + tid) * P.corr_uselen + k0] &
+                                              ~3u);
+        }
     }
     for (int i = tid; i < NS * pitch; i += kHarmThreads) {
         const int s = i / pitch, jj = i - s * pitch;
@@ -411,8 +448,19 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 6 : 4) harmsum_kernel(c
     const float *planes = P.planes;
     // subharmonics [0, NA) belong to stages 0 .. S-2, [NA, NS) to the last
     constexpr int NA = NS > 1 ? NS / 2 : 1;
+    if constexpr (PF) {
+        if (tid == 0) {
+            prefetch_tile<NS>(P, T, 0, s_prstart, s_pwind, b);
+            prefetch_tile<NS>(P, T, kPrefetchRows, s_prstart, s_pwind, b);
+        }
+    }
     for (int jj0 = 0; jj0 < numz0; jj0 += kHarmZ) {
         const bool full = jj0 + kHarmZ <= numz0;
+        if constexpr (PF) {
+            // one tile ahead of the rows being gathered
+            if (tid == 0 && jj0 > 0 && jj0 % kPrefetchRows == 0)
+                prefetch_tile<NS>(P, T, jj0 + kPrefetchRows, s_prstart, s_pwind, b);
+        }
         float v[kHarmZ];
         // phase 1: every gather of stages 0 .. S-2 for the four rows in flight
         // at once, then the adds in the reference's order
@@ -420,11 +468,14 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 6 : 4) harmsum_kernel(c
             float x[NA][kHarmZ];
 #pragma unroll
             for (int s = 0; s < NA; s++) {
-                const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
-                x[s][0] = planes[off[s] + z.x];
-                x[s][1] = planes[off[s] + z.y];
-                x[s][2] = planes[off[s] + z.z];
-                x[s][3] = planes[off[s] + z.w];
+#pragma unroll
+                for (int q = 0; q < kHarmZ / 4; q++) {
+                    const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0 + 4 * q);
+                    x[s][4 * q + 0] = planes[off[s] + z.x];
+                    x[s][4 * q + 1] = planes[off[s] + z.y];
+                    x[s][4 * q + 2] = planes[off[s] + z.z];
+                    x[s][4 * q + 3] = planes[off[s] + z.w];
+                }
             }
 #pragma unroll
             for (int u = 0; u < kHarmZ; u++)
@@ -455,11 +506,14 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 6 : 4) harmsum_kernel(c
             float x[NS - NA][kHarmZ];
 #pragma unroll
             for (int s = NA; s < NS; s++) {
-                const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0);
-                x[s - NA][0] = planes[off[s] + z.x];
-                x[s - NA][1] = planes[off[s] + z.y];
-                x[s - NA][2] = planes[off[s] + z.z];
-                x[s - NA][3] = planes[off[s] + z.w];
+#pragma unroll
+                for (int q = 0; q < kHarmZ / 4; q++) {
+                    const int4 z = *reinterpret_cast<const int4 *>(hsm + s * pitch + jj0 + 4 * q);
+                    x[s - NA][4 * q + 0] = planes[off[s] + z.x];
+                    x[s - NA][4 * q + 1] = planes[off[s] + z.y];
+                    x[s - NA][4 * q + 2] = planes[off[s] + z.z];
+                    x[s - NA][4 * q + 3] = planes[off[s] + z.w];
+                }
             }
 #pragma unroll
             for (int s = NA; s < NS; s++) {
@@ -477,6 +531,205 @@ __global__ void __launch_bounds__(kHarmThreads, S <= 5 ? 6 : 4) harmsum_kernel(c
                                v[u]);
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3b. Harmonic summing fed by TMA (the default where its boxes fit).
+//
+// Same thread mapping, same float adds in the same order and the same hit
+// keys as harmsum_kernel, so the results are bitwise the same; the
+// difference is where the operands come from.  The CTA walks the fundamental
+// z rows in tiles of ZT.  For each tile, one thread issues one tensor copy per
+// subharmonic (cp.async.bulk.tensor.4d): the box of that subharmonic's
+// volume that the tile's 128 fundamental r x ZT fundamental z can touch --
+// rows zinds_s[z0] .. + Z[s], cells from the tile's first r index (rounded
+// down to 4, the 16-byte rule of the x coordinate) .. + W[s] -- into shared
+// memory, completing on an mbarrier.  The threads then gather from shared
+// memory, so the global-memory latency that bounds harmsum_kernel is paid by
+// the copy engine, many tiles in flight per SM.
+
+template <int S, int ZT>
+struct HarmTmaOcc {
+    static constexpr int value = S <= 5 ? (ZT <= 8 ? 5 : 3) : (ZT <= 8 ? 3 : 2);
+};
+
+template <int S, int ZT>
+__global__ void __launch_bounds__(kHarmThreads, HarmTmaOcc<S, ZT>::value)
+    harmsum_tma_kernel(const SearchDev P, const __grid_constant__ HarmTma T)
+{
+    constexpr int NS = 1 << (S - 1);
+    constexpr int NA = NS > 1 ? NS / 2 : 1;
+    constexpr int ZU = 4;  // z rows per compute step
+    static_assert(ZT % ZU == 0, "tile of whole steps");
+    extern __shared__ __align__(128) float tsm[];
+    // tensor-copy destinations 128-byte aligned whatever the static shared
+    // variables before the dynamic block (128 bytes of slack are allocated)
+    float *box = tsm + ((128u - (smem_u32(tsm) & 127u)) & 127u) / 4u;
+    int *zoff = reinterpret_cast<int *>(box + T.box_floats);  // [NS][pitch]
+    __shared__ uint64_t s_bar;
+    __shared__ int s_wind[NS], s_rstart[NS], s_numrs[NS];
+    const int numz0 = P.numz0;
+    const int pitch = zrow_pitch(numz0);
+    const int b = blockIdx.z;
+    const int ii = blockIdx.y;
+    const int tid = threadIdx.x;
+    const int k0 = blockIdx.x * kHarmThreads;
+    const int kk = k0 + tid;
+    const bool valid = kk < P.corr_uselen;
+    const long long rstep = P.first_rstep + b;
+
+    if (tid < NS) {
+        const SubDev sd = P.subs[tid];
+        s_wind[tid] = tid == 0 ? ii : P.wind[sd.wind_off + ii];
+        s_rstart[tid] = tid == 0 ? k0
+                                 : (int)(P.rinds[((long long)b * NS + tid) * P.corr_uselen + k0] & ~3u);
+        s_numrs[tid] = P.steps[rstep * NS + tid].numrs;
+    }
+    // zoff[s][jj]: offset in the shared buffer of subharmonic s's row for
+    // fundamental row jj, within the box of jj's tile
+    for (int i = tid; i < NS * pitch; i += kHarmThreads) {
+        const int s = i / pitch, jj = i - s * pitch;
+        int o = T.boxoff[s];
+        if (jj < numz0) {
+            const int j0 = jj - jj % ZT;
+            const int zi = s == 0 ? jj : P.zinds[P.subs[s].zinds_off + jj];
+            const int z0 = s == 0 ? j0 : P.zinds[P.subs[s].zinds_off + j0];
+            int dz = zi - z0;
+            if (dz < 0 || dz >= T.Z[s]) {  // cannot happen for tables built as the reference builds them
+                atomicOr(P.status, kStatusRind);
+                dz = 0;
+            }
+            o += dz * T.W[s];
+        }
+        zoff[i] = o;
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (smem_u32(box) & 127u) {  // unreachable by construction; never issue a misaligned copy
+        if (tid == 0)
+            atomicOr(P.status, kStatusCopy);
+        return;
+    }
+
+    // this thread's cell in every box
+    int col[NS];
+    col[0] = tid;
+#pragma unroll
+    for (int s = 1; s < NS; s++) {
+        int c = 0;
+        if (valid) {
+            const unsigned int ri = P.rinds[((long long)b * NS + s) * P.corr_uselen + kk];
+            c = (int)ri - s_rstart[s];
+            if (ri >= (unsigned int)s_numrs[s] || c < 0 || c >= T.W[s]) {
+                atomicOr(P.status, kStatusRind);
+                c = 0;
+            }
+        }
+        col[s] = c;
+    }
+    float cut[S];
+#pragma unroll
+    for (int st = 0; st < S; st++)
+        cut[st] = P.powcut[st];
+
+    const int ntiles = (numz0 + ZT - 1) / ZT;
+    for (int t = 0; t < ntiles; t++) {
+        const int z0 = t * ZT;
+        if (tid == 0) {
+            // the previous tile's reads (generic proxy) are ordered before
+            // this tile's writes by the copy engine (async proxy)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                         :: "r"(smem_u32(&s_bar)), "r"(T.box_bytes) : "memory");
+            for (int s = 0; s < NS; s++) {
+                const int zs = s == 0 ? z0 : P.zinds[P.subs[s].zinds_off + z0];
+                asm volatile(
+                    "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                    " [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                    :: "r"(smem_u32(box + T.boxoff[s])), "l"(reinterpret_cast<uint64_t>(&T.map[s])),
+                       "r"(s_rstart[s]), "r"(zs), "r"(s_wind[s]), "r"(b), "r"(smem_u32(&s_bar))
+                    : "memory");
+            }
+        }
+        const bool ok = bar_wait(&s_bar, t & 1);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(P.status, kStatusCopy);
+                bar_wait(&s_bar, t & 1);  // once more, bounded, for the copies in flight
+            }
+            return;
+        }
+        const int nrows = min(ZT, numz0 - z0);
+        for (int u0 = 0; u0 < nrows; u0 += ZU) {
+            const int jj0 = z0 + u0;
+            const bool full = u0 + ZU <= nrows;
+            float v[ZU];
+            {
+                float x[NA][ZU];
+#pragma unroll
+                for (int s = 0; s < NA; s++) {
+                    const int4 z = *reinterpret_cast<const int4 *>(zoff + s * pitch + jj0);
+                    x[s][0] = box[z.x + col[s]];
+                    x[s][1] = box[z.y + col[s]];
+                    x[s][2] = box[z.z + col[s]];
+                    x[s][3] = box[z.w + col[s]];
+                }
+#pragma unroll
+                for (int u = 0; u < ZU; u++)
+                    v[u] = x[0][u];
+                int s = 1;
+#pragma unroll
+                for (int stage = 0; stage < (S > 1 ? S - 1 : 1); stage++) {
+                    if (stage > 0) {
+#pragma unroll
+                        for (int h = 0; h < (1 << (stage - 1)); h++, s++) {
+#pragma unroll
+                            for (int u = 0; u < ZU; u++)
+                                v[u] = __fadd_rn(v[u], x[s][u]);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < ZU; u++) {
+                        if (valid && (full || u0 + u < nrows) && v[u] > cut[stage])
+                            record_hit(P,
+                                       ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) *
+                                            numz0 + (jj0 + u)) * P.corr_uselen + kk,
+                                       v[u]);
+                    }
+                }
+            }
+            if constexpr (S > 1) {
+                float x[NS - NA][ZU];
+#pragma unroll
+                for (int s = NA; s < NS; s++) {
+                    const int4 z = *reinterpret_cast<const int4 *>(zoff + s * pitch + jj0);
+                    x[s - NA][0] = box[z.x + col[s]];
+                    x[s - NA][1] = box[z.y + col[s]];
+                    x[s - NA][2] = box[z.z + col[s]];
+                    x[s - NA][3] = box[z.w + col[s]];
+                }
+#pragma unroll
+                for (int s = NA; s < NS; s++) {
+#pragma unroll
+                    for (int u = 0; u < ZU; u++)
+                        v[u] = __fadd_rn(v[u], x[s - NA][u]);
+                }
+                constexpr int stage = S - 1;
+#pragma unroll
+                for (int u = 0; u < ZU; u++) {
+                    if (valid && (full || u0 + u < nrows) && v[u] > cut[stage])
+                        record_hit(P,
+                                   ((((unsigned long long)rstep * S + stage) * P.numw0 + ii) *
+                                        numz0 + (jj0 + u)) * P.corr_uselen + kk,
+                                   v[u]);
+                }
+            }
+        }
+        __syncthreads();  // every read of this tile's boxes is done
     }
 }
 
@@ -596,30 +849,80 @@ cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int r
     }
 }
 
-template <int S>
-static cudaError_t launch_harmsum_s(const SearchDev &P, cudaStream_t st)
+template <int S, bool PF>
+static cudaError_t launch_harmsum_s(const SearchDev &P, const HarmTma &T, cudaStream_t st)
 {
     const size_t smem = harmsum_smem_bytes(P.nsubs, P.numz0);
-    cudaError_t e = cudaFuncSetAttribute(harmsum_kernel<S>,
+    cudaError_t e = cudaFuncSetAttribute(harmsum_kernel<S, 4, PF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
     const dim3 grid((P.corr_uselen + kHarmThreads - 1) / kHarmThreads, P.numw0, P.nb);
-    harmsum_kernel<S><<<grid, kHarmThreads, smem, st>>>(P);
+    harmsum_kernel<S, 4, PF><<<grid, kHarmThreads, smem, st>>>(P, T);
     return cudaGetLastError();
 }
 
-cudaError_t launch_harmsum(const SearchDev &P, cudaStream_t st)
+template <bool PF>
+static cudaError_t launch_harmsum_p(const SearchDev &P, const HarmTma &T, cudaStream_t st)
 {
     switch (P.nstages) {
-    case 1: return launch_harmsum_s<1>(P, st);
-    case 2: return launch_harmsum_s<2>(P, st);
-    case 3: return launch_harmsum_s<3>(P, st);
-    case 4: return launch_harmsum_s<4>(P, st);
-    case 5: return launch_harmsum_s<5>(P, st);
-    case 6: return launch_harmsum_s<6>(P, st);
+    case 1: return launch_harmsum_s<1, PF>(P, T, st);
+    case 2: return launch_harmsum_s<2, PF>(P, T, st);
+    case 3: return launch_harmsum_s<3, PF>(P, T, st);
+    case 4: return launch_harmsum_s<4, PF>(P, T, st);
+    case 5: return launch_harmsum_s<5, PF>(P, T, st);
+    case 6: return launch_harmsum_s<6, PF>(P, T, st);
     default: return cudaErrorInvalidValue;
     }
+}
+
+// The gather kernel; with prefetch, T holds tensor maps whose boxes were
+// sized for tiles of kPrefetchRows rows.
+cudaError_t launch_harmsum(const SearchDev &P, const HarmTma &T, bool prefetch, cudaStream_t st)
+{
+    return prefetch ? launch_harmsum_p<true>(P, T, st) : launch_harmsum_p<false>(P, T, st);
+}
+
+size_t harmsum_tma_smem_bytes(const HarmTma &T, int nsubs, int numz0)
+{
+    return 128 + sizeof(float) * (size_t)T.box_floats + harmsum_smem_bytes(nsubs, numz0);
+}
+
+template <int S, int ZT>
+static cudaError_t launch_harmsum_tma_s(const SearchDev &P, const HarmTma &T, cudaStream_t st)
+{
+    const size_t smem = harmsum_tma_smem_bytes(T, P.nsubs, P.numz0);
+    cudaError_t e = cudaFuncSetAttribute(harmsum_tma_kernel<S, ZT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(harmsum_tma_kernel<S, ZT>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess)
+        return e;
+    const dim3 grid((P.corr_uselen + kHarmThreads - 1) / kHarmThreads, P.numw0, P.nb);
+    harmsum_tma_kernel<S, ZT><<<grid, kHarmThreads, smem, st>>>(P, T);
+    return cudaGetLastError();
+}
+
+template <int ZT>
+static cudaError_t launch_harmsum_tma_z(const SearchDev &P, const HarmTma &T, cudaStream_t st)
+{
+    switch (P.nstages) {
+    case 1: return launch_harmsum_tma_s<1, ZT>(P, T, st);
+    case 2: return launch_harmsum_tma_s<2, ZT>(P, T, st);
+    case 3: return launch_harmsum_tma_s<3, ZT>(P, T, st);
+    case 4: return launch_harmsum_tma_s<4, ZT>(P, T, st);
+    case 5: return launch_harmsum_tma_s<5, ZT>(P, T, st);
+    case 6: return launch_harmsum_tma_s<6, ZT>(P, T, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// zt: fundamental z rows per tile (8 or 16), as the boxes in T were sized
+cudaError_t launch_harmsum_tma(const SearchDev &P, const HarmTma &T, int zt, cudaStream_t st)
+{
+    return zt == 8 ? launch_harmsum_tma_z<8>(P, T, st) : launch_harmsum_tma_z<16>(P, T, st);
 }
 
 }  // namespace jerk

@@ -2,6 +2,8 @@
 // plan (jerk_plan.cpp).  Plain structs, no torch types.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include <cstdint>
 
 namespace jerk {
@@ -68,6 +70,21 @@ struct SearchDev {
     unsigned int *hit_count;
     long long max_hits;
     unsigned int *status;     // bit 0: a subharmonic r index fell outside its row
+                              // (or its TMA box); bit 1: a bounded wait on a bulk
+                              // or tensor copy gave up
+};
+
+// Tensor maps of the harmonic sum's TMA path: subharmonic s's batch volumes
+// as a 4-D tensor (r, z, w, b) and the box one CTA loads per z tile:
+// W[s] r cells (a multiple of 4, starting at the tile's first r index rounded
+// down to 4) by Z[s] z rows, at boxoff[s] floats into the shared buffer.
+struct HarmTma {
+    CUtensorMap map[kMaxSubs];
+    int W[kMaxSubs];
+    int Z[kMaxSubs];
+    int boxoff[kMaxSubs];
+    int box_floats;           // shared floats of all boxes (offsets 128-byte aligned)
+    int box_bytes;            // bytes the tensor copies of one tile deliver
 };
 
 // One response kernel of the bank (jerk_bank.cu).

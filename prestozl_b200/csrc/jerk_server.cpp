@@ -266,6 +266,7 @@ static bool admit(jerk_server *s, const Pending &pd)
     if (!sl.plan) {
         jerk_config c{};
         c.batch_rsteps = s->cfg.batch_rsteps;
+        c.harm_mode = s->cfg.harm_mode;
         c.device_bank = bank.ptr;
         c.stream = s->stream;
         rc = jerk_plan_create(&sl.plan, &sl.geo.obs, sl.geo.subs.data(), (int)sl.geo.subs.size(), &c);
@@ -296,7 +297,8 @@ static void worker_main(jerk_server *s)
 {
     cudaSetDevice(s->cfg.device);
     for (;;) {
-        // admission
+        // admission (requests queued before t_round all get a chance now)
+        const double t_round = now_s();
         for (;;) {
             Pending pd;
             {
@@ -312,15 +314,15 @@ static void worker_main(jerk_server *s)
             std::lock_guard<std::mutex> lk(s->mu);
             s->pending.pop_front();
         }
-        // requests still waiting after admission had its chance, longer than
-        // allowed, fail
+        // requests that had their admission chance this round and are still
+        // waiting, longer than allowed, fail (later arrivals get theirs first)
         if (s->cfg.queue_timeout_s > 0) {
             std::vector<Pending> expired;
             {
                 std::lock_guard<std::mutex> lk(s->mu);
                 const double t = now_s();
                 for (auto it = s->pending.begin(); it != s->pending.end();) {
-                    if (t - it->t_submit > s->cfg.queue_timeout_s) {
+                    if (it->t_submit < t_round && t - it->t_submit > s->cfg.queue_timeout_s) {
                         expired.push_back(*it);
                         it = s->pending.erase(it);
                     } else {

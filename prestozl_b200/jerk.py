@@ -60,7 +60,8 @@ class Cand(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [("batch_rsteps", C.c_int), ("max_hits", C.c_longlong),
-                ("stream", C.c_void_p), ("device_bank", C.c_void_p)]
+                ("stream", C.c_void_p), ("device_bank", C.c_void_p), ("harm_mode", C.c_int),
+                ("use_graph", C.c_int)]
 
 
 class KernelStat(C.Structure):
@@ -71,7 +72,7 @@ class KernelStat(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_longlong), ("max_active", C.c_int),
                 ("batch_rsteps", C.c_int), ("device", C.c_int), ("batches_ahead", C.c_int),
-                ("queue_timeout_s", C.c_double)]
+                ("queue_timeout_s", C.c_double), ("harm_mode", C.c_int)]
 
 
 class Request(C.Structure):
@@ -299,7 +300,8 @@ class JerkPlan:
     """A search plan on the current CUDA device (jerk_plan_create)."""
 
     def __init__(self, obs: Obs, subs: Sequence[dict], batch: int = 8, max_hits: int = 0,
-                 stream: int = 0, device_bank: int = 0):
+                 stream: int = 0, device_bank: int = 0, harm_mode: int = 0,
+                 use_graph: bool = False):
         self.obs = obs
         self._kerns = []
         arr = (Subharm * len(subs))()
@@ -313,7 +315,8 @@ class JerkPlan:
             arr[i] = Subharm(s["numharm"], s["harmnum"], s.get("zmax", 0), s.get("wmax", 0),
                              s["numz"], s["numw"], s["fftlen"], s["halfwidth"], kp)
         self.subs = arr
-        cfg = Config(batch, max_hits, stream or None, device_bank or None)
+        cfg = Config(batch, max_hits, stream or None, device_bank or None, harm_mode,
+                     int(bool(use_graph)))
         self._p = C.c_void_p()
         _check(lib().jerk_plan_create(C.byref(self._p), C.byref(obs), arr, len(subs),
                                       C.byref(cfg)))
@@ -412,9 +415,10 @@ class JerkServer:
     tensors) are kept alive here until their result has been polled."""
 
     def __init__(self, hbm_budget_bytes: int = 0, max_active: int = 0, batch: int = 0,
-                 device: int = 0, batches_ahead: int = 0, queue_timeout_s: float = 0.0):
+                 device: int = 0, batches_ahead: int = 0, queue_timeout_s: float = 0.0,
+                 harm_mode: int = 0):
         cfg = ServerConfig(hbm_budget_bytes, max_active, batch, device, batches_ahead,
-                           queue_timeout_s)
+                           queue_timeout_s, harm_mode)
         self._s = C.c_void_p()
         _check(lib().jerk_server_create(C.byref(self._s), C.byref(cfg)))
         self._keep = {}

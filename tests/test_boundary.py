@@ -113,3 +113,12 @@ def test_errors_are_returned_not_fatal():
     assert ei.value.code == jerk.JERK_EINVAL
     with pytest.raises(jerk.JerkError):
         jerk.obs_from_params(1 << 10, 1 << 11, 1e-3, 20, 60, 3, 2.0)  # numharm not 2^k
+
+
+def test_bad_tuning_knob_is_rejected_before_any_device_work():
+    obs, fftlen, _ = jerk.obs_from_params(1 << 19, 1 << 20, 64e-6, 20, 60, 8, 2.0)
+    subs = jerk.subharm_sizes(obs, fftlen)
+    with pytest.raises(jerk.JerkError) as ei:
+        jerk.JerkPlan(obs, subs, batch=8, harm_mode=7)
+    assert ei.value.code == jerk.JERK_EINVAL
+    assert "harm_mode" in str(ei.value)

@@ -51,3 +51,35 @@ def test_reference_gpu_matches_reference_cpu(tmp_path):
             assert abs(float(a) - float(b)) <= 0.05 * max(1.0, abs(float(b))), (g, w)
         if len(g) > 12 and g[1].isdigit():
             fund = False
+
+
+def test_paper_scale_dropin_matches_reference_gpu(tmp_path):
+    """At the paper configuration (2^25 samples, -zmax 200 -wmax 300
+    -numharm 16 -sigma 3.0 -batchsize 8; seeded noise + 4 injected pulsars)
+    this project's drop-in and the reference's own GPU accelsearch_cu write
+    the same ACCEL file: same candidates, same optimised r/z/w, powers and
+    sigmas as printed."""
+    torch = pytest.importorskip("torch")
+    build.build()
+    if not (os.path.exists(ob.REFGPU_CLI) and os.path.exists(ob.DROPIN_CLI)):
+        pytest.skip("reference GPU / drop-in binaries not built")
+    import numpy as np
+
+    N, dt = 1 << 25, 54.6e-6
+    pulsars = synth.random_pulsars(np.random.default_rng(0), 4)
+    spec = synth.presto_fft_torch(synth.timeseries_torch(N, dt, pulsars, 0, device="cuda"))
+    spec = spec.cpu().numpy()
+    torch.cuda.synchronize()
+    flags = ["-zmax", "200", "-wmax", "300", "-numharm", "16", "-sigma", "3.0", "-batchsize", "8"]
+    files = {}
+    for name, cli in (("refgpu", ob.REFGPU_CLI), ("dropin", ob.DROPIN_CLI)):
+        d = tmp_path / name
+        d.mkdir()
+        synth.write_fft(str(d / "paper"), spec, N, dt)
+        env = dict(os.environ, PRESTO=str(d))
+        out = subprocess.run([cli, *flags, "paper.fft"], cwd=d, env=env, capture_output=True,
+                             text=True, timeout=900)
+        assert out.returncode == 0, out.stderr[-2000:]
+        files[name] = (d / "paper_ACCEL_200_JERK_300").read_text()
+    assert len(accel_rows(files["refgpu"])) > 10
+    assert files["dropin"] == files["refgpu"]
