@@ -292,13 +292,16 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
         const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
         float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
                       (long long)lrow * sd.stride;
+        // the power is formed for every output and the store predicated on
+        // the good-bin range (one unsigned compare): measured faster than a
+        // branch around both.  Power-of-two fftlen: 1/fftlen^2 is already in
+        // the chunk.
         auto out = [&](int m, float2 y) {
             const int kk = m - offset;
-            if (kk >= 0 && kk < numrs) {
-                const float pw = __fadd_rn(__fmul_rn(y.x, y.x), __fmul_rn(y.y, y.y));
-                // power-of-two fftlen: 1/fftlen^2 is already in the chunk
-                outp[kk] = IsPow2<N>::value ? pw : __fmul_rn(pw, norm);
-            }
+            const float pw = __fadd_rn(__fmul_rn(y.x, y.x), __fmul_rn(y.y, y.y));
+            const float o = IsPow2<N>::value ? pw : __fmul_rn(pw, norm);
+            if ((unsigned)kk < (unsigned)numrs)
+                outp[kk] = o;
         };
         if constexpr (kStage) {
             // rstep b's row is (or will shortly be) in dsm; once every thread
