@@ -113,3 +113,47 @@ def test_requests_that_cannot_fit_or_wait_too_long_fail_alone():
     assert outcomes.get(0) == "ok"
     assert outcomes.get("err") == jerk.JERK_TIMEOUT
     assert st["failed"] == 1
+
+
+def test_poisson_stream_of_dedispersion_trials_peaks_at_the_pulsar_trial():
+    """The served stream in miniature: trial spectra arrive at Poisson times
+    (40 per second) while earlier ones are on the GPU; one pulsar's SNR peaks
+    at trial 5 and falls off as a Gaussian in trial index (sigma 1.5 trials).
+    Every trial is answered, latencies are reported, and the pulsar's best
+    candidate sigma is highest at the peak trial."""
+    import time
+
+    torch = pytest.importorskip("torch")
+    build.build()
+    N, dt, ntrials, peak = 1 << 22, 64e-6, 10, 5
+    psr = synth.Pulsar(f=87.3, z=30.0, w=60.0, snr=30.0, nharm=4)
+    specs = []
+    for t in range(ntrials):
+        snr = psr.snr * float(np.exp(-0.5 * ((t - peak) / 1.5) ** 2))
+        p = synth.Pulsar(psr.f, psr.z, psr.w, snr, psr.nharm)
+        ts = synth.timeseries_torch(N, dt, [p] if snr > 1.0 else [], 700 + t, device="cuda")
+        specs.append(synth.presto_fft_torch(ts).contiguous())
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(7)
+    gaps = rng.exponential(1.0 / 40.0, ntrials)
+    srv = jerk.JerkServer(max_active=3, batch=32)
+    t0 = time.perf_counter()
+    for t in range(ntrials):
+        time.sleep(float(gaps[t]))
+        srv.submit(specs[t], N, dt, 100, 200, 8, 3.0, tag=t)
+    best, lat = {}, []
+    for _ in range(ntrials):
+        tag, cands, tm = srv.poll(120000)
+        lat.append(tm["done"] - tm["submit"])
+        # the pulsar's candidates: within its drift (z/2 + w/12 bins) of f * T
+        r0 = psr.f * N * dt
+        near = cands[np.abs(cands["r"] - r0) < 30.0] if len(cands) else cands
+        best[tag] = float(near["sigma"].max()) if len(near) else 0.0
+    srv.close()
+    wall = time.perf_counter() - t0
+    print(f"{ntrials} trials in {wall:.2f} s; latency p50 {np.percentile(lat, 50):.2f} s "
+          f"p99 {np.percentile(lat, 99):.2f} s; best sigma by trial "
+          f"{[round(best[t], 1) for t in range(ntrials)]}")
+    assert sorted(best) == list(range(ntrials))
+    assert max(best, key=best.get) == peak
+    assert best[peak] > best[0] and best[peak] > best[ntrials - 1]
