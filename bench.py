@@ -368,6 +368,28 @@ def main():
     plain_s = replicas.max_over_ranks(sum(step_ms) / 1000.0, dist, "cuda")
     plain_value = world * args.steps / plain_s * 3600.0
 
+    # ---- batched under a captured CUDA graph: the same searches, each pass
+    # replayed from one graph (captured on the warm-up call)
+    graph_info = None
+    if not nsearch:
+        gplan = jerk.JerkPlan(obs, subs, batch=args.batch, device_bank=bank.ptr.value,
+                              harm_mode=harm_mode, use_graph=True)
+        gplan.search(specs[0], 0, nsearch)
+        torch.cuda.synchronize()
+        barrier()
+        g_ms = []
+        for i in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            gplan.search(specs[i % nspec], 0, nsearch)
+            e1.record()
+            torch.cuda.synchronize()
+            g_ms.append(e0.elapsed_time(e1))
+        gplan.close()
+        g_s = replicas.max_over_ranks(sum(g_ms) / 1000.0, dist, "cuda")
+        graph_info = {"value": world * args.steps / g_s * 3600.0,
+                      "ms_per_spectrum": statistics.mean(g_ms)}
+
     # ---- plain drop-in: what accelsearch_GPU does per spectrum -- upload the
     # host kernel bank, allocate a plan (-batchsize 8), copy the host spectrum,
     # search, build the list, free everything
@@ -487,6 +509,7 @@ def main():
                                  "(served) or each search (plain); max over ranks",
                        "l2": "inputs larger than L2 (128 MiB spectra, GB-sized volumes), no flush",
                        "parallelism": f"replicas x{world}"},
+            "batched_graph": graph_info,
             "plain": {"value": plain_value, "ms_per_spectrum": statistics.mean(step_ms),
                       "p50_ms": float(np.percentile(step_ms, 50)),
                       "p99_ms": float(np.percentile(step_ms, 99))},
