@@ -25,6 +25,7 @@
 //                      src/accel_kernels.cu:781-862)
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -264,6 +265,10 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     const int lrow = row - G.rowstart[gi];
     const SubDev sd = P.subs[s];
     const float2 *D0 = P.prepped + sd.data_off;
+    // this CTA's rsteps: all of the batch, or a share of them when a small
+    // group's rows alone would leave SMs idle (gridDim.y > 1)
+    const int bchunk = (P.nb + (int)gridDim.y - 1) / (int)gridDim.y;
+    const int b0 = min(P.nb, (int)blockIdx.y * bchunk), b1 = min(P.nb, b0 + bchunk);
 
     if constexpr (kStage) {
         if (tid == 0) {
@@ -271,8 +276,8 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         __syncthreads();
-        if (tid == 0)
-            bulk_row_load(dsm, D0, N * sizeof(float2), &s_bar);
+        if (tid == 0 && b0 < b1)
+            bulk_row_load(dsm, D0 + (long long)b0 * N, N * sizeof(float2), &s_bar);
     }
 
     for (int i = tid; i < TWN; i += T)
@@ -288,7 +293,7 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
 
     const int offset = sd.halfwidth * 2;  // binoffset * ACCEL_NUMBETWEEN
     const float norm = sd.pownorm;
-    for (int b = 0; b < P.nb; b++) {
+    for (int b = b0; b < b1; b++) {
         const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
         float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
                       (long long)lrow * sd.stride;
@@ -306,11 +311,11 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
         if constexpr (kStage) {
             // rstep b's row is (or will shortly be) in dsm; once every thread
             // has read it, thread 0 starts the copy of rstep b + 1's row
-            if (!bar_wait(&s_bar, b & 1) && P.status)
+            if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
                 atomicOr(P.status, kStatusCopy);
             auto in = [&](int r) -> float2 { return cmulconj(dsm[tid + r * (N / R0)], kreg[r]); };
             auto mid = [&] {
-                if (tid == 0 && b + 1 < P.nb) {
+                if (tid == 0 && b + 1 < b1) {
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     bulk_row_load(dsm, D0 + (long long)(b + 1) * N, N * sizeof(float2), &s_bar);
                 }
@@ -362,7 +367,9 @@ size_t harmsum_smem_bytes(int nsubs, int numz0)
 // batch's volumes hold fewer than 2^32 floats; checked on the host).
 template <int S, int ZU>
 struct HarmOcc {
-    static constexpr int value = ZU <= 4 ? (S <= 5 ? 6 : 4) : (S <= 5 ? 4 : 2);
+    // S <= 5, 4 rows per step: 7 CTAs of 128 threads (72 registers) measured
+    // 6 % faster than 6 CTAs (80 registers); 8 CTAs spill
+    static constexpr int value = ZU <= 4 ? (S <= 5 ? 7 : 4) : (S <= 5 ? 4 : 2);
 };
 
 // L2 prefetch, by the copy engine, of the boxes (HarmTma) that fundamental
@@ -850,6 +857,21 @@ cudaError_t launch_prep(const SearchDev &P, int maxfft, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// SMs of the current device (queried once; every B200 has 148)
+static int sm_count()
+{
+    static int n = 0;
+    if (n <= 0) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+            n = v;
+        else
+            return 148;
+    }
+    return n;
+}
+
 template <int N>
 static cudaError_t launch_corr_n(const SearchDev &P, const RowGroup &G, int rows, cudaStream_t st)
 {
@@ -861,7 +883,10 @@ static cudaError_t launch_corr_n(const SearchDev &P, const RowGroup &G, int rows
                                  (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess)
         return e;
-    corr_kernel<N><<<rows, FftPlan<N>::T, smem, st>>>(P, G);
+    // a group with fewer rows than two waves of CTAs also splits its rsteps
+    const int wave = sm_count() * CorrOcc<N>::value;
+    const int split = rows >= 2 * wave ? 1 : std::max(1, std::min(P.nb, (2 * wave + rows - 1) / rows));
+    corr_kernel<N><<<dim3(rows, split), FftPlan<N>::T, smem, st>>>(P, G);
     return cudaGetLastError();
 }
 
