@@ -50,7 +50,9 @@ def _load() -> Dict[str, dict]:
 def _store(db: Dict[str, dict]) -> None:
     path = cache_path()
     os.makedirs(os.path.dirname(path), exist_ok=True)
-    tmp = path + ".tmp"
+    # one temporary file per process: ranks of one node may store at once;
+    # os.replace is atomic, so readers see one whole file or another
+    tmp = f"{path}.{os.getpid()}.tmp"
     with open(tmp, "w") as fh:
         json.dump(db, fh, indent=1, sort_keys=True)
     os.replace(tmp, path)
