@@ -64,7 +64,8 @@ typedef struct jerk_obs {
     int numz;                 /* fundamental f-dot count */
     int numw;                 /* accelobs.numw (0 when -wmax 0) */
     int numharmstages;        /* log2(numharm) + 1 */
-    int norm_type;            /* 0: block median (the only one supported) */
+    int norm_type;            /* 0: block median; 1: local power (-locpow);
+                                 ignored when nph > 0 (-photon) */
     float nph;                /* > 0: photon normalisation */
     float powcut[JERK_MAX_STAGES];
     long long numindep[JERK_MAX_STAGES];

@@ -296,6 +296,33 @@ def geom_from_refobs(o: RefObs) -> OrcGeom:
     return g
 
 
+def local_powers(powers: np.ndarray) -> np.ndarray:
+    """The oracle's -locpow local power levels (direct restatement)."""
+    p = np.ascontiguousarray(powers, dtype=np.float32)
+    out = np.zeros_like(p)
+    f = _orc().orc_local_powers
+    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    f(p.ctypes.data, len(p), out.ctypes.data)
+    return out
+
+
+def ref_local_powers(powers: np.ndarray) -> np.ndarray:
+    """The reference's own corr_loc_pow (FFT correlation)."""
+    p = np.array(powers, dtype=np.float32)  # the reference may work in place
+    out = np.zeros_like(p)
+    f = _ref().ref_corr_loc_pow
+    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    f(p.ctypes.data, len(p), out.ctypes.data)
+    return out
+
+
+def invsqrtf(x: float, reference: bool = False) -> float:
+    f = _ref().ref_invsqrtf if reference else _orc().orc_invsqrtf
+    f.restype = C.c_float
+    f.argtypes = [C.c_float]
+    return float(f(x))
+
+
 class Oracle:
     """The oracle restatement on explicit arrays.
 

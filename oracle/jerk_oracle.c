@@ -69,7 +69,7 @@ typedef struct orc_geom {
     int corr_uselen;
     int numz;              /* fundamental numz (obs->numz) */
     int numharmstages;
-    int norm_type;         /* 0 = block median */
+    int norm_type;         /* 0 = block median, 1 = local power (-locpow) */
     double nph;            /* > 0: photon normalisation */
     float powcut[6];
     long long numindep[6];
@@ -366,6 +366,50 @@ static int cmp_float(const void *a, const void *b)
     return (fa > fb) - (fa < fb);
 }
 
+/* The reference's fast inverse square root (src/misc_utils.c:293-304): the
+ * published bit-level first guess and one Newton step, in float.  The
+ * reference is built with -ffast-math, and gcc then evaluates the Newton step
+ * as y * (1.5 - (0.5 x)(y y)) -- bit-identical to the reference build over
+ * 40,000 inputs, where the source order differs in about one case in six. */
+static float invsqrtf_ref(float x)
+{
+    union {
+        float f;
+        int32_t i;
+    } t;
+    t.f = x;
+    t.i = 0x5f3759df - (t.i >> 1);
+    const float y = t.f;
+    const float yy = y * y;
+    const float hx = 0.5f * x;
+    return y * (1.5f - hx * yy);
+}
+
+/* Local power levels of the -locpow normalisation (src/corr_routines.c:309-366,
+ * used at src/accel_utils.c:1186-1203).  The reference correlates the powers,
+ * through realfft / real_corr_conv (whose round trip scales by 2/n), with a
+ * double top-hat of weight (n/2)/NUMLOCPOWAVG -- integer division -- at offsets
+ * DELTAAVGBINS+1 .. NUMLOCPOWAVG/2+DELTAAVGBINS on both sides; restated as the
+ * direct sum (checked against the reference's own routine to 2e-7).  The first
+ * and last kern_half_width bins take the nearest interior value. */
+#define LOC_NUMAVG 20 /* NUMLOCPOWAVG, include/presto.h:100 */
+#define LOC_DELTA 5   /* DELTAAVGBINS, include/presto.h:104 */
+static void local_powers(const float *p, int n, float *out)
+{
+    const int khw = LOC_NUMAVG / 2 + LOC_DELTA;
+    const double w = (double)((n / 2) / LOC_NUMAVG) * 2.0 / (double)n;
+    for (int i = khw; i < n - khw; i++) {
+        double s = 0.0;
+        for (int d = LOC_DELTA + 1; d <= khw; d++)
+            s += (double)p[i + d] + (double)p[i - d];
+        out[i] = (float)(w * s);
+    }
+    for (int i = 0; i < khw; i++) {
+        out[i] = out[khw];
+        out[n - 1 - i] = out[n - 1 - khw];
+    }
+}
+
 static float median_of(float *arr, int n)
 {
     qsort(arr, n, sizeof(float), cmp_float);
@@ -445,7 +489,7 @@ static int fderivs(const orc_geom *g, const orc_sub *s, const float *fft, double
         double norm = 1.0 / sqrt(g->nph);
         for (int ii = 0; ii < 2 * numdata; ii++)
             data[ii] *= norm;
-    } else {
+    } else if (g->norm_type == 0) {
         double norm;
         powers = (float *)malloc(sizeof(float) * numdata);
         for (int ii = 0; ii < numdata; ii++) {
@@ -457,6 +501,23 @@ static int fderivs(const orc_geom *g, const orc_sub *s, const float *fft, double
         free(powers);
         for (int ii = 0; ii < 2 * numdata; ii++)
             data[ii] *= norm;
+    } else {
+        /* -locpow: float norm per bin, invsqrtf of the local power */
+        float *loc = (float *)malloc(sizeof(float) * numdata);
+        powers = (float *)calloc((size_t)numdata, sizeof(float));
+        for (int ii = 0; ii < numdata; ii++) {
+            float r = data[2 * ii], i = data[2 * ii + 1];
+            float rr = r * r, ii2 = i * i;
+            powers[ii] = rr + ii2;
+        }
+        local_powers(powers, numdata, loc);
+        for (int ii = 0; ii < numdata; ii++) {
+            const float norm = invsqrtf_ref(loc[ii]);
+            data[2 * ii] *= norm;
+            data[2 * ii + 1] *= norm;
+        }
+        free(powers);
+        free(loc);
     }
 
     /* spread_no_pad + forward FFT (double) */
@@ -779,3 +840,7 @@ long orc_insert_hits(const orc_cand *hits, long nhits, const long long *numindep
     free(L.c);
     return n;
 }
+
+/* exported for pinning against the reference build */
+void orc_local_powers(const float *p, int n, float *out) { local_powers(p, n, out); }
+float orc_invsqrtf(float x) { return invsqrtf_ref(x); }

@@ -279,6 +279,18 @@ int ref_fftlen_from_kernwidth(int kernwidth) { return fftlen_from_kernwidth(kern
 
 float ref_median(float *arr, int n) { return median(arr, n); }
 
+/* The reference's local power levels (src/corr_routines.c:309-366) and its
+ * fast inverse square root (src/misc_utils.c:293-304), for pinning the
+ * -locpow normalisation. */
+void ref_corr_loc_pow(float *powers, int n, float *out)
+{
+    float *lp = corr_loc_pow(powers, n);
+    memcpy(out, lp, sizeof(float) * n);
+    vect_free(lp);
+}
+
+float ref_invsqrtf(float x) { return invsqrtf(x); }
+
 /* The reference's kernel response for one (z, w), before placement and FFT:
  * numkern complex64 values from gen_w_response (src/responses.c:333-418). */
 int ref_gen_w_response(double roffset, int numbetween, double z, double w, int numkern,

@@ -62,6 +62,40 @@ struct NextPow2<1> {
     static constexpr int value = 1;
 };
 
+// The reference's fast inverse square root (src/misc_utils.c:293-304): the
+// published bit-level first guess and one Newton step in float, in the
+// operation order the reference build evaluates it (y * (1.5 - (0.5 x)(y y)),
+// its compiler's reassociation under -ffast-math), each step rounded on its
+// own (no FMA).
+__device__ __forceinline__ float invsqrtf_ref(float x)
+{
+    const float y = __int_as_float(0x5f3759df - (__float_as_int(x) >> 1));
+    const float yy = __fmul_rn(y, y);
+    const float hx = __fmul_rn(0.5f, x);
+    return __fmul_rn(y, __fsub_rn(1.5f, __fmul_rn(hx, yy)));
+}
+
+// -locpow local power levels (src/corr_routines.c:309-366): the double
+// top-hat of weight ((M/2)/NUMLOCPOWAVG, integer division) * 2/M at offsets
+// DELTAAVGBINS+1 .. NUMLOCPOWAVG/2+DELTAAVGBINS either side -- the reference
+// applies it by FFT correlation, restated as the direct sum -- with the first
+// and last kern_half_width bins taking the nearest interior value.
+constexpr int kLocAvg = 20;   // NUMLOCPOWAVG (include/presto.h:100)
+constexpr int kLocDelta = 5;  // DELTAAVGBINS (include/presto.h:104)
+
+template <int M>
+__device__ __forceinline__ float local_power(const float *pw, int i)
+{
+    constexpr int khw = kLocAvg / 2 + kLocDelta;
+    const double w = (double)((M / 2) / kLocAvg) * 2.0 / (double)M;
+    const int c = i < khw ? khw : (i >= M - khw ? M - 1 - khw : i);
+    double s = 0.0;
+#pragma unroll
+    for (int d = kLocDelta + 1; d <= khw; d++)
+        s = __dadd_rn(s, __dadd_rn((double)pw[c + d], (double)pw[c - d]));
+    return __double2float_rn(__dmul_rn(w, s));
+}
+
 template <int N>
 __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
 {
@@ -94,9 +128,19 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
         keys[i] = INFINITY;
     __syncthreads();
 
-    double norm;
+    double norm = 1.0;
     if (P.nph > 0.0f) {
         norm = __ddiv_rn(1.0, __dsqrt_rn((double)P.nph));
+    } else if (P.norm_type == 1) {
+        // -locpow: a float norm per bin (src/accel_utils.c:1186-1203)
+        static_assert(M >= 2 * (kLocAvg / 2 + kLocDelta), "chunk too short for -locpow");
+        for (int i = tid; i < M; i += nt) {
+            const float nrm = invsqrtf_ref(local_power<M>(keys, i));
+            float2 v = data[i];
+            v.x = __fmul_rn(v.x, nrm);
+            v.y = __fmul_rn(v.y, nrm);
+            data[i] = v;
+        }
     } else {
         // median(): the order statistic of rank (M-1)/2 (src/median.c);
         // bitonic sort of the powers, padded with +inf
@@ -119,11 +163,13 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
         const double med = (double)keys[(M - 1) / 2];
         norm = __ddiv_rn(1.0, __dsqrt_rn(__ddiv_rn(med, kLn2)));
     }
-    for (int i = tid; i < M; i += nt) {
-        float2 v = data[i];
-        v.x = __double2float_rn(__dmul_rn((double)v.x, norm));
-        v.y = __double2float_rn(__dmul_rn((double)v.y, norm));
-        data[i] = v;
+    if (!(P.nph <= 0.0f && P.norm_type == 1)) {
+        for (int i = tid; i < M; i += nt) {
+            float2 v = data[i];
+            v.x = __double2float_rn(__dmul_rn((double)v.x, norm));
+            v.y = __double2float_rn(__dmul_rn((double)v.y, norm));
+            data[i] = v;
+        }
     }
     __syncthreads();
 

@@ -1028,8 +1028,8 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     if (obs->numharmstages < 1 || obs->numharmstages > kMaxStages ||
         nsubs != jerk_subharm_count(obs->numharmstages))
         return fail(JERK_EINVAL, "jerk_plan_create: nsubs does not match numharmstages");
-    if (obs->norm_type != 0 && !(obs->nph > 0.0f))
-        return fail(JERK_EUNSUPPORTED, "only block-median or photon normalisation is supported");
+    if (obs->norm_type != 0 && obs->norm_type != 1 && !(obs->nph > 0.0f))
+        return fail(JERK_EINVAL, "norm_type must be 0 (block median) or 1 (local power)");
     if (obs->corr_uselen <= 0 || obs->corr_uselen % 2 || obs->corr_uselen > 65535)
         return fail(JERK_EINVAL, "bad corr_uselen");
 

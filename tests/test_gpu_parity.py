@@ -166,3 +166,39 @@ def test_graph_mode_replays_match_batch_by_batch(small):
     assert not np.array_equal(keys[0], keys[1])  # the replays did see new data
     plain.close()
     graph.close()
+
+
+def test_local_power_normalisation_matches_reference(tmp_path):
+    """-locpow (src/accel_utils.c:1186-1203): volumes against the FP64 oracle
+    (same normalisation restated) and the whole small search against the
+    reference CPU search run with -locpow."""
+    build.build()
+    H.ensure_oracle()
+    if not H.have_ref():
+        pytest.skip("the reference build (oracle/_ref) provides the kernel bank")
+    from prestozl_b200 import synth
+
+    spec, N, dt = synth.small_spectrum()
+    args = list(H.golden("small_cands.json")["args"]) + ["-locpow"]
+    prob = H.Problem(str(tmp_path), spec, N, dt, args)
+    assert prob.obs.norm_type == 1
+    obs = jerk.obs_from_refobs(prob.obs)
+    assert obs.norm_type == 1
+    p = jerk.JerkPlan(obs, prob.subs, batch=8)
+    worst = 0.0
+    for k in (0, prob.rstep_of(8281.0), p.num_rsteps - 1):
+        startr = prob.startr(k)
+        for i in range(len(prob.subs)):
+            got, rlo = p.volume(prob.spec, k, i)
+            h, want, _, _ = prob.oracle.fderivs(i, startr, startr + prob.rstep - 0.5)
+            err = float((np.abs(got.astype(np.float64) - want) / np.maximum(want, 1.0)).max())
+            worst = max(worst, err)
+            assert err <= POW_TOL, (k, i, err)
+    got = p.search(prob.spec)
+    p.close()
+    prob.ref.make_bank()
+    want, done = prob.ref.search()
+    probs = H.compare_cands(got, want, list(prob.obs.powcut))
+    assert not probs, probs[:10]
+    assert len(want) > 0
+    print(f"-locpow: max FP32 power error vs FP64 oracle {worst:.3e}, {len(want)} candidates")

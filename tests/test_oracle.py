@@ -155,3 +155,21 @@ def test_insertion_walk_matches_reference_on_crafted_sequences(small):
         assert np.array_equal(got["sigma"], want["sigma"])
         unsorted += int(np.any(np.diff(want["r"]) < 0))
     assert unsorted > 0
+
+
+def test_local_power_normalisation_matches_reference():
+    """-locpow: the oracle's direct double-top-hat local power equals the
+    reference's FFT correlation (src/corr_routines.c:309-366) to 1e-6, for
+    every chunk length the FFT lengths give, and its fast inverse square root
+    (src/misc_utils.c:293-304) is bit-exact."""
+    if not ob.have_reference():
+        pytest.skip("reference build absent")
+    ob.quiet_wisdom()
+    rng = np.random.default_rng(11)
+    for n in (64, 96, 192, 256, 384, 512, 640, 1024, 2048, 2560, 3840):
+        p = rng.exponential(1.0, n).astype(np.float32)
+        want = ob.ref_local_powers(p)
+        got = ob.local_powers(p)
+        assert np.max(np.abs(got / want - 1.0)) < 1e-6, n
+    for x in rng.exponential(2.0, 1000).astype(np.float32):
+        assert ob.invsqrtf(float(x)) == ob.invsqrtf(float(x), reference=True)
