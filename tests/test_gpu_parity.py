@@ -202,3 +202,28 @@ def test_local_power_normalisation_matches_reference(tmp_path):
     assert not probs, probs[:10]
     assert len(want) > 0
     print(f"-locpow: max FP32 power error vs FP64 oracle {worst:.3e}, {len(want)} candidates")
+
+
+@pytest.mark.parametrize("numharm", [1, 2])
+def test_few_harmonics_match_reference(numharm, tmp_path):
+    """-numharm 1 and 2 on the small spectrum: the whole search equals the
+    reference CPU search (the reference's own GPU path returns no candidates
+    at -numharm 1: its search sits inside numharmstages > 1)."""
+    build.build()
+    H.ensure_oracle()
+    if not H.have_ref():
+        pytest.skip("the reference build (oracle/_ref) provides the kernel bank")
+    from prestozl_b200 import synth
+
+    spec, N, dt = synth.small_spectrum()
+    args = list(H.golden("small_cands.json")["args"])
+    args[args.index("-numharm") + 1] = str(numharm)
+    prob = H.Problem(str(tmp_path), spec, N, dt, args)
+    p = jerk.JerkPlan(jerk.obs_from_refobs(prob.obs), prob.subs, batch=16)
+    got = p.search(prob.spec)
+    p.close()
+    prob.ref.make_bank()
+    want, _ = prob.ref.search()
+    assert len(want) > 0
+    probs = H.compare_cands(got, want, list(prob.obs.powcut))
+    assert not probs, probs[:10]
