@@ -1032,6 +1032,10 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
         return fail(JERK_EINVAL, "norm_type must be 0 (block median) or 1 (local power)");
     if (obs->corr_uselen <= 0 || obs->corr_uselen % 2 || obs->corr_uselen > 65535)
         return fail(JERK_EINVAL, "bad corr_uselen");
+    for (int s = 0; s < nsubs; s++)  // before any device work
+        if (!fftlen_supported(subs[s].fftlen))
+            return fail(JERK_EUNSUPPORTED, "unsupported fftlen " + std::to_string(subs[s].fftlen) +
+                                               " (at most 7680 here)");
 
     jerk_plan *p = new jerk_plan();
     cudaGetDevice(&p->device);
