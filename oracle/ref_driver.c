@@ -28,7 +28,8 @@
 typedef struct refctx {
     accelobs obs;
     infodata idata;
-    Cmdline *cmd;
+    Cmdline *cmd;      /* -> own_cmd */
+    Cmdline own_cmd;   /* this context's parsed options */
     subharminfo **shis;
 } refctx;
 
@@ -48,10 +49,26 @@ typedef struct ref_cand {
 
 extern Cmdline *parseCmdline(int argc, char **argv);
 
+/* The reference's parser (src/accelsearch_cmd.c:24, :1259) fills one
+ * file-static Cmdline and never resets it, so an option given to one parse
+ * (-locpow, -photon, ...) would stay set for every later one in this process.
+ * Each open therefore restores the parser's defaults before parsing and keeps
+ * its own copy of the result. */
+static Cmdline *g_cmd_static;
+static Cmdline g_cmd_defaults;
+
 refctx *ref_open(int argc, char **argv)
 {
     refctx *c = (refctx *)calloc(1, sizeof(refctx));
-    c->cmd = parseCmdline(argc, argv);
+    if (!g_cmd_static) {
+        char prog[] = "accelsearch", file[] = "defaults.fft";
+        char *a[] = {prog, file};
+        g_cmd_static = parseCmdline(2, a);
+        g_cmd_defaults = *g_cmd_static;
+    }
+    *g_cmd_static = g_cmd_defaults;
+    c->own_cmd = *parseCmdline(argc, argv);
+    c->cmd = &c->own_cmd;
     create_accelobs(&c->obs, &c->idata, c->cmd, 1);
     return c;
 }

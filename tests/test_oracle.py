@@ -173,3 +173,21 @@ def test_local_power_normalisation_matches_reference():
         assert np.max(np.abs(got / want - 1.0)) < 1e-6, n
     for x in rng.exponential(2.0, 1000).astype(np.float32):
         assert ob.invsqrtf(float(x)) == ob.invsqrtf(float(x), reference=True)
+
+
+def test_reference_options_do_not_leak_between_opens(tmp_path):
+    """The reference's option parser keeps its options in one static struct;
+    the driver restores the defaults before each parse, so a -locpow search
+    opened earlier in the process does not turn the next search's
+    normalisation into local power."""
+    if not ob.have_reference():
+        pytest.skip("reference build absent")
+    spec, N, dt = synth.small_spectrum()
+    root = str(tmp_path / "s")
+    synth.write_fft(root, spec, N, dt)
+    args = ["-zmax", "20", "-wmax", "60", "-numharm", "8", "-sigma", "2.0"]
+    a = ob.RefSearch(root + ".fft", args + ["-locpow"])
+    b = ob.RefSearch(root + ".fft", args)
+    assert a.obs.norm_type == 1 and b.obs.norm_type == 0
+    a.close()
+    b.close()
