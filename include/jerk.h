@@ -93,7 +93,8 @@ typedef struct jerk_cand {
 } jerk_cand;
 
 typedef struct jerk_config {
-    int batch_rsteps;         /* rsteps per batch (the reference's -batchsize); 0 = auto */
+    int batch_rsteps;         /* rsteps per batch (the reference's -batchsize); 0 = 8;
+                                 capped to what 32-bit volume offsets allow */
     long long max_hits;       /* initial hit-buffer capacity; 0 = auto */
     void *stream;             /* cudaStream_t to run on; NULL = a private stream */
     const void *device_bank;  /* optional resident bank (jerk_bank_generate) */

@@ -273,6 +273,7 @@ cudaError_t launch_bank_fft_any(int N, const BankRow *rows, int first, int count
     case 4096: return launch_bank_fft<4096>(rows, first, count, tw, twoff, bank, st);
     case 5120: return launch_bank_fft<5120>(rows, first, count, tw, twoff, bank, st);
     case 7680: return launch_bank_fft<7680>(rows, first, count, tw, twoff, bank, st);
+    case 10240: return launch_bank_fft<10240>(rows, first, count, tw, twoff, bank, st);
     default: return cudaErrorInvalidValue;
     }
 }

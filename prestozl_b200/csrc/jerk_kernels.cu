@@ -96,6 +96,17 @@ __device__ __forceinline__ float local_power(const float *pw, int i)
     return __double2float_rn(__dmul_rn(w, s));
 }
 
+// Whether prep_impl<N> keeps the FFT twiddles in shared memory beside its
+// buffer, data chunk and sort keys (every length up to 7680), or reads them
+// from global memory (10240, whose tables alone take 100 KB).
+template <int N>
+struct PrepTwInSmem {
+    static constexpr int M = N / 2;
+    static constexpr bool value =
+        (size_t)(fft_buf_len<N>() + FftPlan<N>::twsize() + M) * 8 +
+            (size_t)NextPow2<M>::value * 4 <= 200 * 1024;
+};
+
 template <int N>
 __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
 {
@@ -106,13 +117,19 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
     const StepDev st = P.steps[(P.first_rstep + b) * P.nsubs + s];
     constexpr int TWN = FftPlan<N>::twsize();
     float2 *buf = reinterpret_cast<float2 *>(smem);
-    float2 *tw = buf + fft_buf_len<N>();
-    float2 *data = tw + TWN;
+    // buffer, twiddles, data chunk, sort keys; at the longest fftlen the
+    // twiddles stay in global memory (read through L1) to leave room
+    constexpr bool kTwS = PrepTwInSmem<N>::value;
+    float2 *tws = buf + fft_buf_len<N>();
+    float2 *data = tws + (kTwS ? TWN : 0);
     float *keys = reinterpret_cast<float *>(data + M);
+    const float2 *tw = kTwS ? tws : P.twiddles + sd.twoff;
     const int tid = threadIdx.x, nt = blockDim.x;
 
-    for (int i = tid; i < TWN; i += nt)
-        tw[i] = P.twiddles[sd.twoff + i];
+    if constexpr (kTwS) {
+        for (int i = tid; i < TWN; i += nt)
+            tws[i] = P.twiddles[sd.twoff + i];
+    }
 
     // get_fourier_amplitudes: M bins from lobin, zero outside the file
     const long long lobin = st.rlo - sd.halfwidth;
@@ -225,6 +242,7 @@ __global__ void prep_kernel(const SearchDev P)
         JERK_PREP_CASE(4096)
         JERK_PREP_CASE(5120)
         JERK_PREP_CASE(7680)
+        JERK_PREP_CASE(10240)
 #undef JERK_PREP_CASE
     default:
         break;
@@ -840,7 +858,8 @@ template <int N>
 static size_t prep_bytes_n()
 {
     constexpr int M = N / 2;
-    return sizeof(float2) * (size_t)(fft_buf_len<N>() + FftPlan<N>::twsize() + M) +
+    constexpr int TW = PrepTwInSmem<N>::value ? FftPlan<N>::twsize() : 0;
+    return sizeof(float2) * (size_t)(fft_buf_len<N>() + TW + M) +
            sizeof(float) * (size_t)NextPow2<M>::value;
 }
 
@@ -851,7 +870,7 @@ size_t prep_smem_bytes(int maxfft)
     if (NN <= maxfft && prep_bytes_n<NN>() > b)      \
         b = prep_bytes_n<NN>();
     JERK_PB(128) JERK_PB(192) JERK_PB(256) JERK_PB(384) JERK_PB(512) JERK_PB(768)
-    JERK_PB(1024) JERK_PB(1280) JERK_PB(2048) JERK_PB(4096) JERK_PB(5120) JERK_PB(7680)
+    JERK_PB(1024) JERK_PB(1280) JERK_PB(2048) JERK_PB(4096) JERK_PB(5120) JERK_PB(7680) JERK_PB(10240)
 #undef JERK_PB
     return b;
 }
@@ -862,7 +881,7 @@ int fft_twiddle_size(int N)
     switch (N) {
 #define JERK_TS(NN) case NN: return FftPlan<NN>::twsize();
     JERK_TS(128) JERK_TS(192) JERK_TS(256) JERK_TS(384) JERK_TS(512) JERK_TS(768)
-    JERK_TS(1024) JERK_TS(1280) JERK_TS(2048) JERK_TS(4096) JERK_TS(5120) JERK_TS(7680)
+    JERK_TS(1024) JERK_TS(1280) JERK_TS(2048) JERK_TS(4096) JERK_TS(5120) JERK_TS(7680) JERK_TS(10240)
 #undef JERK_TS
     default: return -1;
     }
@@ -873,7 +892,7 @@ void fft_twiddle_table(int N, float2 *out)
     switch (N) {
 #define JERK_TT(NN) case NN: fft_stage_twiddles<NN>(out); break;
     JERK_TT(128) JERK_TT(192) JERK_TT(256) JERK_TT(384) JERK_TT(512) JERK_TT(768)
-    JERK_TT(1024) JERK_TT(1280) JERK_TT(2048) JERK_TT(4096) JERK_TT(5120) JERK_TT(7680)
+    JERK_TT(1024) JERK_TT(1280) JERK_TT(2048) JERK_TT(4096) JERK_TT(5120) JERK_TT(7680) JERK_TT(10240)
 #undef JERK_TT
     default: break;
     }
@@ -887,7 +906,7 @@ int prep_threads(int maxfft)
     if (NN <= maxfft && FftPlan<NN>::T > t)          \
         t = FftPlan<NN>::T;
     JERK_PT(128) JERK_PT(192) JERK_PT(256) JERK_PT(384) JERK_PT(512) JERK_PT(768)
-    JERK_PT(1024) JERK_PT(1280) JERK_PT(2048) JERK_PT(4096) JERK_PT(5120) JERK_PT(7680)
+    JERK_PT(1024) JERK_PT(1280) JERK_PT(2048) JERK_PT(4096) JERK_PT(5120) JERK_PT(7680) JERK_PT(10240)
 #undef JERK_PT
     return (t + 31) / 32 * 32;
 }
@@ -940,7 +959,7 @@ bool fftlen_supported(int n)
 {
     switch (n) {
     case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 1280:
-    case 2048: case 4096: case 5120: case 7680:
+    case 2048: case 4096: case 5120: case 7680: case 10240:
         return true;
     default:
         return false;
@@ -963,6 +982,7 @@ cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int r
     case 4096: return launch_corr_n<4096>(P, G, rows, st);
     case 5120: return launch_corr_n<5120>(P, G, rows, st);
     case 7680: return launch_corr_n<7680>(P, G, rows, st);
+    case 10240: return launch_corr_n<10240>(P, G, rows, st);
     default: return cudaErrorInvalidValue;
     }
 }

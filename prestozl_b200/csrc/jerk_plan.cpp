@@ -1035,7 +1035,7 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     for (int s = 0; s < nsubs; s++)  // before any device work
         if (!fftlen_supported(subs[s].fftlen))
             return fail(JERK_EUNSUPPORTED, "unsupported fftlen " + std::to_string(subs[s].fftlen) +
-                                               " (at most 7680 here)");
+                                               " (at most 10240 here)");
 
     jerk_plan *p = new jerk_plan();
     cudaGetDevice(&p->device);
@@ -1099,6 +1099,19 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
             st.pad = 0;
             maxnumrs[s] = std::max(maxnumrs[s], numrs);
         }
+    }
+
+    // The harmonic sum addresses one batch's volumes with 32-bit offsets, so
+    // the rsteps per batch (a speed knob only) are capped to what fits: at
+    // zmax 600, wmax 1200 one rstep's volumes already hold 1.6 G floats.
+    {
+        long long per_rstep = 0;
+        for (int s = 0; s < nsubs; s++)
+            per_rstep += (long long)subs[s].numw * subs[s].numz * ((maxnumrs[s] + 3) & ~3);
+        const long long cap = per_rstep > 0 ? ((1LL << 32) - 1) / per_rstep : p->batch;
+        if (cap < 1)
+            return bail(fail(JERK_EUNSUPPORTED, "ffdot volumes of one rstep exceed 2^32 floats"));
+        p->batch = (int)std::min<long long>(p->batch, cap);
     }
 
     // subharmonic layout

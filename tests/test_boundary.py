@@ -125,10 +125,10 @@ def test_bad_tuning_knob_is_rejected_before_any_device_work():
 
 
 def test_unsupported_fft_length_is_rejected_before_any_device_work():
-    # zmax 800, wmax 1200 needs fftlen 10240
-    obs, fftlen, _ = jerk.obs_from_params(1 << 24, 1 << 25, 54.6e-6, 800, 1200, 16, 3.0)
-    assert fftlen == 10240
+    # zmax 1200, wmax 1500 needs fftlen 15360 (the longest supported is 10240)
+    obs, fftlen, _ = jerk.obs_from_params(1 << 24, 1 << 25, 54.6e-6, 1200, 1500, 16, 3.0)
+    assert fftlen == 15360
     subs = jerk.subharm_sizes(obs, fftlen)
     with pytest.raises(jerk.JerkError) as ei:
         jerk.JerkPlan(obs, subs, batch=4)
-    assert ei.value.code == jerk.JERK_EUNSUPPORTED and "10240" in str(ei.value)
+    assert ei.value.code == jerk.JERK_EUNSUPPORTED and "15360" in str(ei.value)
