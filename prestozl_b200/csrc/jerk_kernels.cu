@@ -253,11 +253,12 @@ __global__ void prep_kernel(const SearchDev P)
 // 2. Correlation: one CTA per kernel row, all rsteps of the batch.
 
 // Occupancy target for corr_kernel: enough CTAs per SM that 128-thread CTAs
-// give 16 resident warps (registers are capped to fit).
+// give 16 resident warps (registers are capped to fit); CTAs of 384 threads
+// or more run one per SM (two would cap them at 64 registers and spill).
 template <int N>
 struct CorrOcc {
     static constexpr int T = FftPlan<N>::T;
-    static constexpr int value = T >= 512 ? 1 : (T >= 256 ? 2 : (T >= 128 ? 4 : 8));
+    static constexpr int value = T >= 384 ? 1 : (T >= 256 ? 2 : (T >= 128 ? 4 : 8));
 };
 
 // Shared memory of corr_kernel<N>, in float2: the FFT buffer, the twiddle
