@@ -214,6 +214,38 @@ int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
                        int corr_uselen, float nph, float *volume, int *numrs, long long *rlo,
                        void *stream);
 
+/* The search's input from a time series, on the GPU: the steps the reference
+ * takes for a ".dat" input (src/accel_utils.c:1696-1753) before it searches.
+ *
+ * jerk_realfft replaces realfft(idata, n, -1) (src/fastffts.c:163-235): the
+ * forward real FFT of n float samples, unnormalised, packed as the reference
+ * packs it -- n/2 complex64 values, value 0 = (DC, Nyquist), value k = bin k.
+ * n must be a power of two from 2^15 to 2^27 (JERK_EUNSUPPORTED otherwise).
+ * FP32 like the reference's, so results agree to FP32 rounding.
+ *
+ * jerk_deredden replaces deredden(fft, numamps) (src/accel_utils.c:1557-1633)
+ * in place on numamps complex64 values (8 <= numamps < 2^31), bit-exact with
+ * the reference.
+ *
+ * jerk_spectrum_from_timeseries runs both and then sets bin 0 to (1, 1), as
+ * create_accelobs prepares a .dat input searched without -photon
+ * (src/accel_utils.c:1747-1753, 1829-1834).
+ *
+ * All pointers are device pointers owned by the caller: the series and the
+ * spectrum 8-byte aligned (they may be the same buffer: n floats = n/2
+ * complex64), scratch 256-byte aligned and at least the matching
+ * *_scratch_bytes (0 = size not supported).  Asynchronous on stream
+ * (NULL = default stream); nothing is allocated. */
+long long jerk_realfft_scratch_bytes(long long n);
+int jerk_realfft(const float *timeseries, long long n, void *spectrum, void *scratch,
+                 long long scratch_bytes, void *stream);
+long long jerk_deredden_scratch_bytes(long long numamps);
+int jerk_deredden(void *spectrum, long long numamps, void *scratch, long long scratch_bytes,
+                  void *stream);
+long long jerk_spectrum_scratch_bytes(long long n);
+int jerk_spectrum_from_timeseries(const float *timeseries, long long n, void *spectrum,
+                                  void *scratch, long long scratch_bytes, void *stream);
+
 /* The served form: a request loop on one GPU (continuous batching).
  * Submitted spectra wait in a queue; a worker thread that owns the device
  * admits them while fewer than max_active searches run and their device

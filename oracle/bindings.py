@@ -138,6 +138,17 @@ class RefSearch:
         _ref().ref_get_obs(self.ctx, C.byref(o))
         self.obs = o
 
+    def spectrum(self) -> np.ndarray:
+        """The spectrum the reference searches (after its .dat preparation)."""
+        out = np.zeros(int(self.obs.numbins), dtype=np.complex64)
+        f = _ref().ref_copy_spectrum
+        f.restype = C.c_long
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
+        n = f(self.ctx, out.ctypes.data, len(out))
+        if n < 0:
+            raise RuntimeError("the reference holds no spectrum in memory")
+        return out[:n]
+
     def close(self):
         if self.ctx:
             _ref().ref_close(self.ctx)
@@ -314,6 +325,47 @@ def ref_local_powers(powers: np.ndarray) -> np.ndarray:
     f.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     f(p.ctypes.data, len(p), out.ctypes.data)
     return out
+
+
+def deredden(spectrum: np.ndarray, reference: bool = False) -> np.ndarray:
+    """Red-noise removal (src/accel_utils.c:1557-1633) on a copy of a
+    complex64 spectrum: the oracle's restatement, or the reference's own."""
+    f = _ref().deredden if reference else _orc().orc_deredden
+    f.restype = None
+    f.argtypes = [C.c_void_p, C.c_int]
+    a = np.array(spectrum, dtype=np.complex64)
+    f(a.ctypes.data, len(a))
+    return a
+
+
+def ref_realfft(series: np.ndarray) -> np.ndarray:
+    """The reference's forward realfft (src/fastffts.c:163-235, isign -1) on a
+    copy of a float32 series, as built here (its complex FFT is the FFTW
+    stand-in under shim/)."""
+    f = _ref().realfft
+    f.restype = None
+    f.argtypes = [C.c_void_p, C.c_long, C.c_int]
+    a = np.array(series, dtype=np.float32)
+    f(a.ctypes.data, len(a), -1)
+    return a.view(np.complex64)
+
+
+def packed_rfft(series: np.ndarray) -> np.ndarray:
+    """The FP64 forward real FFT in the reference's packing: n/2 complex
+    values, value 0 = (DC, Nyquist)."""
+    X = np.fft.rfft(np.asarray(series, dtype=np.float64))
+    n = len(series)
+    out = X[: n // 2].copy()
+    out[0] = complex(X[0].real, X[n // 2].real)
+    return out
+
+
+def pair_magnitude(packed: np.ndarray) -> np.ndarray:
+    """|X[k]| + |X[M-k]| for a packed spectrum of M values (bin 0 pairs with
+    itself): the scale of the rounding a real FFT built on an M-point complex
+    FFT leaves in bin k."""
+    a = np.abs(np.asarray(packed))
+    return a + np.concatenate([a[:1], a[:0:-1]])
 
 
 def invsqrtf(x: float, reference: bool = False) -> float:

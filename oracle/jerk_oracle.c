@@ -844,3 +844,65 @@ long orc_insert_hits(const orc_cand *hits, long nhits, const long long *numindep
 /* exported for pinning against the reference build */
 void orc_local_powers(const float *p, int n, float *out) { local_powers(p, n, out); }
 float orc_invsqrtf(float x) { return invsqrtf_ref(x); }
+
+/* ------------------------------------------------------------------ */
+/* Red-noise removal of a spectrum read from a time series              */
+
+/* deredden (src/accel_utils.c:1557-1633): the powers are split into blocks
+ * that start at bin 1 with 6 bins and grow as 6 ln(start bin) (at most 200),
+ * while a whole block still fits below numamps.  Each block's level is its
+ * median power (rank (n-1)/2, src/median.c) over ln 2.  Bins are scaled by
+ * invsqrtf of a level that runs linearly from one block's level to the
+ * next's, across the second half of one block and the first half of the
+ * next; the first half block takes the first level and the tail past the
+ * last block extends the last slope.  The DC bin becomes (1, 0).  All
+ * arithmetic in the reference's types: powers and levels in float, the
+ * division by ln 2 and by the half block sum in double. */
+void orc_deredden(float *fft, int numamps)
+{
+    const int initlen = 6, maxlen = 200;
+    float *pw = malloc(sizeof(float) * (size_t)numamps), *tmp = malloc(sizeof(float) * maxlen);
+    fft[0] = 1.0f;
+    fft[1] = 0.0f;
+    for (int i = 0; i < numamps; i++)
+        pw[i] = fft[2 * i] * fft[2 * i] + fft[2 * i + 1] * fft[2 * i + 1];
+    int binnum = 1, numwrote = 1, buflen = initlen, lastlen;
+    memcpy(tmp, pw + binnum, sizeof(float) * buflen);
+    float mean_old = (float)(median_of(tmp, buflen) / log(2.0)), dslope = 1.0f;
+    const float norm0 = invsqrtf_ref(mean_old);
+    for (int k = numwrote; k < binnum + buflen / 2; k++) {
+        fft[2 * k] *= norm0;
+        fft[2 * k + 1] *= norm0;
+    }
+    numwrote += buflen / 2;
+    binnum += buflen;
+    lastlen = buflen;
+    buflen = (int)(initlen * log((double)binnum));
+    if (buflen > maxlen)
+        buflen = maxlen;
+    while (binnum + buflen < numamps) {
+        memcpy(tmp, pw + binnum, sizeof(float) * buflen);
+        const float mean_new = (float)(median_of(tmp, buflen) / log(2.0));
+        dslope = (float)((double)(mean_new - mean_old) / (0.5 * (double)(lastlen + buflen)));
+        int ii = 0;
+        for (int k = numwrote; k < binnum + buflen / 2; k++, ii++) {
+            const float norm = invsqrtf_ref(mean_old + dslope * (float)ii);
+            fft[2 * k] *= norm;
+            fft[2 * k + 1] *= norm;
+        }
+        numwrote += ii;
+        binnum += buflen;
+        lastlen = buflen;
+        mean_old = mean_new;
+        buflen = (int)(initlen * log((double)binnum));
+        if (buflen > maxlen)
+            buflen = maxlen;
+    }
+    for (int k = numwrote, ii = 0; k < numamps; k++, ii++) {
+        const float norm = invsqrtf_ref(mean_old + dslope * (float)ii);
+        fft[2 * k] *= norm;
+        fft[2 * k + 1] *= norm;
+    }
+    free(pw);
+    free(tmp);
+}

@@ -324,6 +324,18 @@ int ref_gen_w_response(double roffset, int numbetween, double z, double w, int n
  * only the single-thread order of insertions is deterministic. */
 void ref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
 
+/* The spectrum the reference searches, when it holds one in memory: a .dat
+ * input after its realfft and deredden (src/accel_utils.c:1696-1753), or a
+ * memory-mapped .fft.  Copies up to max complex values; -1 if none. */
+long ref_copy_spectrum(const refctx *c, float *out, long max)
+{
+    if (!c->obs.fft)
+        return -1;
+    long n = c->obs.numbins < max ? c->obs.numbins : max;
+    memcpy(out, c->obs.fft, sizeof(fcomplex) * (size_t)n);
+    return n;
+}
+
 void ref_close(refctx *c)
 {
     if (!c)

@@ -62,19 +62,6 @@ struct NextPow2<1> {
     static constexpr int value = 1;
 };
 
-// The reference's fast inverse square root (src/misc_utils.c:293-304): the
-// published bit-level first guess and one Newton step in float, in the
-// operation order the reference build evaluates it (y * (1.5 - (0.5 x)(y y)),
-// its compiler's reassociation under -ffast-math), each step rounded on its
-// own (no FMA).
-__device__ __forceinline__ float invsqrtf_ref(float x)
-{
-    const float y = __int_as_float(0x5f3759df - (__float_as_int(x) >> 1));
-    const float yy = __fmul_rn(y, y);
-    const float hx = __fmul_rn(0.5f, x);
-    return __fmul_rn(y, __fsub_rn(1.5f, __fmul_rn(hx, yy)));
-}
-
 // -locpow local power levels (src/corr_routines.c:309-366): the double
 // top-hat of weight ((M/2)/NUMLOCPOWAVG, integer division) * 2/M at offsets
 // DELTAAVGBINS+1 .. NUMLOCPOWAVG/2+DELTAAVGBINS either side -- the reference

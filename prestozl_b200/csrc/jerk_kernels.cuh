@@ -104,4 +104,20 @@ struct RowGroup {
     int rowstart[kMaxSubs + 1];  // prefix sums of numw * numz
 };
 
+// Records msg as the text jerk_last_error returns and passes code back.
+int set_error(int code, const char *msg);
+
+// The reference's fast inverse square root (src/misc_utils.c:293-304): the
+// published bit-level first guess and one Newton step in float, in the
+// operation order the reference build evaluates it (y * (1.5 - (0.5 x)(y y)),
+// its compiler's reassociation under -ffast-math), each step rounded on its
+// own (no FMA).
+__device__ __forceinline__ float invsqrtf_ref(float x)
+{
+    const float y = __int_as_float(0x5f3759df - (__float_as_int(x) >> 1));
+    const float yy = __fmul_rn(y, y);
+    const float hx = __fmul_rn(0.5f, x);
+    return __fmul_rn(y, __fsub_rn(1.5f, __fmul_rn(hx, yy)));
+}
+
 }  // namespace jerk

@@ -68,6 +68,9 @@ static int cuda_fail(cudaError_t e, const char *what)
     } while (0)
 
 extern "C" const char *jerk_last_error(void) { return g_err.c_str(); }
+
+// Error reporting for the entry points compiled in other files.
+int jerk::set_error(int code, const char *msg) { return fail(code, msg); }
 extern "C" void jerk_free(void *p) { free(p); }
 
 // ---------------------------------------------------------------------------

@@ -108,7 +108,9 @@ EXPORTS = [
     "jerk_plan_kernel_stats", "jerk_plan_transfer_stats", "jerk_volume_static",
     "jerk_search_async", "jerk_search_advance", "jerk_search_ready", "jerk_search_collect", "jerk_plan_device_bytes",
     "jerk_server_create", "jerk_server_submit", "jerk_server_poll", "jerk_server_stats",
-    "jerk_server_destroy",
+    "jerk_server_destroy", "jerk_realfft_scratch_bytes", "jerk_realfft",
+    "jerk_deredden_scratch_bytes", "jerk_deredden", "jerk_spectrum_scratch_bytes",
+    "jerk_spectrum_from_timeseries",
 ]
 
 
@@ -176,6 +178,14 @@ def lib() -> C.CDLL:
     L.jerk_volume_static.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.POINTER(Subharm),
                                      C.c_void_p, C.c_double, C.c_int, C.c_float, C.c_void_p,
                                      C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.c_void_p]
+    for f in ("jerk_realfft_scratch_bytes", "jerk_deredden_scratch_bytes",
+              "jerk_spectrum_scratch_bytes"):
+        getattr(L, f).restype = C.c_longlong
+        getattr(L, f).argtypes = [C.c_longlong]
+    for f in ("jerk_realfft", "jerk_spectrum_from_timeseries"):
+        getattr(L, f).argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
+                                  C.c_void_p]
+    L.jerk_deredden.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
     _lib = L
     return L
 
@@ -282,6 +292,58 @@ def volume_static(spectrum_dev: int, numbins: int, lobin: int, sub: dict, kernel
     if rc != JERK_OK:
         raise JerkError(rc, "jerk_volume_static failed (see stderr)")
     return numrs.value, rlo.value
+
+
+def _input_call(fn: str, size_fn: str, x, n: int, out):
+    import torch
+
+    if not (getattr(x, "is_cuda", False) and x.is_contiguous()):
+        raise JerkError(JERK_EINVAL, f"{fn}: expects a contiguous CUDA tensor")
+    nbytes = getattr(lib(), size_fn)(n)
+    if nbytes <= 0:
+        raise JerkError(JERK_EUNSUPPORTED, f"{fn}: size {n} not supported")
+    scratch = torch.empty(nbytes, dtype=torch.uint8, device=x.device)
+    stream = torch.cuda.current_stream(x.device).cuda_stream
+    if fn == "jerk_deredden":
+        _check(lib().jerk_deredden(x.data_ptr(), n, scratch.data_ptr(), nbytes, stream or None))
+    else:
+        _check(getattr(lib(), fn)(x.data_ptr(), n, out.data_ptr(), scratch.data_ptr(), nbytes,
+                                  stream or None))
+    return out if out is not None else x
+
+
+def _series_out(ts, out):
+    import torch
+
+    if ts.dtype != torch.float32 or ts.dim() != 1:
+        raise JerkError(JERK_EINVAL, "the time series must be a 1-D float32 tensor")
+    if out is None:
+        out = torch.empty(ts.numel() // 2, dtype=torch.complex64, device=ts.device)
+    return out
+
+
+def realfft(ts, out=None):
+    """Forward real FFT of a float32 CUDA time series in PRESTO's packing
+    (realfft(data, n, -1), src/fastffts.c:163-235): n/2 complex64 values,
+    value 0 = (DC, Nyquist).  ``out`` may be ``ts`` viewed as complex64
+    (in place).  Asynchronous on torch's current stream."""
+    out = _series_out(ts, out)
+    return _input_call("jerk_realfft", "jerk_realfft_scratch_bytes", ts, ts.numel(), out)
+
+
+def deredden(spec):
+    """The reference's red-noise removal (src/accel_utils.c:1557-1633), in
+    place on a complex64 CUDA spectrum; bit-exact with the reference."""
+    return _input_call("jerk_deredden", "jerk_deredden_scratch_bytes", spec, spec.numel(), None)
+
+
+def spectrum_from_timeseries(ts, out=None):
+    """realfft, deredden and bin 0 set to (1, 1): the spectrum the reference
+    searches for a .dat input without -photon (src/accel_utils.c:1747-1753,
+    1829-1834)."""
+    out = _series_out(ts, out)
+    return _input_call("jerk_spectrum_from_timeseries", "jerk_spectrum_scratch_bytes", ts,
+                       ts.numel(), out)
 
 
 def _spectrum_arg(spectrum):

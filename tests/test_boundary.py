@@ -132,3 +132,29 @@ def test_unsupported_fft_length_is_rejected_before_any_device_work():
     with pytest.raises(jerk.JerkError) as ei:
         jerk.JerkPlan(obs, subs, batch=4)
     assert ei.value.code == jerk.JERK_EUNSUPPORTED and "15360" in str(ei.value)
+
+
+def test_input_entry_points_size_and_reject_before_any_device_work():
+    """jerk_realfft / jerk_deredden: scratch sizes from the host alone, and
+    unsupported lengths, null or misaligned pointers and short scratch come
+    back as error codes before anything reaches the device."""
+    L = jerk.lib()
+    M = 1 << 24
+    # the four-step scratch: M complex values plus two twiddle tables
+    assert L.jerk_realfft_scratch_bytes(1 << 25) >= 8 * M
+    for bad in (0, 3, 1 << 14, (1 << 25) + 2, 1 << 28, 3 << 20):
+        assert L.jerk_realfft_scratch_bytes(bad) == 0, bad
+    assert L.jerk_deredden_scratch_bytes(7) == 0
+    assert L.jerk_deredden_scratch_bytes(8) > 0
+    assert L.jerk_deredden_scratch_bytes(1 << 24) >= 4 * ((1 << 24) // 100)
+    assert L.jerk_spectrum_scratch_bytes(1 << 25) == max(
+        L.jerk_realfft_scratch_bytes(1 << 25), L.jerk_deredden_scratch_bytes(1 << 24))
+    big = L.jerk_realfft_scratch_bytes(1 << 20)
+    assert L.jerk_realfft(4096, 3 << 20, 4096, 4096, big, None) == jerk.JERK_EUNSUPPORTED
+    assert L.jerk_realfft(None, 1 << 20, 4096, 4096, big, None) == jerk.JERK_EINVAL
+    assert L.jerk_realfft(4100, 1 << 20, 4096, 4096, big, None) == jerk.JERK_EINVAL  # misaligned
+    assert L.jerk_realfft(4096, 1 << 20, 4096, 4096, big - 1, None) == jerk.JERK_EINVAL
+    assert "scratch" in jerk.lib().jerk_last_error().decode()
+    assert L.jerk_deredden(4096, 7, 4096, 1 << 20, None) == jerk.JERK_EINVAL
+    assert L.jerk_deredden(4096, 1 << 20, 4096, 16, None) == jerk.JERK_EINVAL
+    assert L.jerk_spectrum_from_timeseries(4096, 100, 4096, 4096, big, None) == jerk.JERK_EUNSUPPORTED

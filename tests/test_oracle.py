@@ -191,3 +191,67 @@ def test_reference_options_do_not_leak_between_opens(tmp_path):
     assert a.obs.norm_type == 1 and b.obs.norm_type == 0
     a.close()
     b.close()
+
+
+def _reddish_spectrum(n: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    amp = 10.0 / np.sqrt(np.arange(n) + 1.0) + 1.0
+    return (rng.standard_normal(n) * amp + 1j * rng.standard_normal(n) * amp).astype(np.complex64)
+
+
+def test_deredden_restatement_matches_reference():
+    """The oracle's red-noise removal is bit-exact with the reference's
+    deredden (src/accel_utils.c:1557-1633) from the smallest spectrum it
+    accepts to 2^20 bins."""
+    if not ob.have_reference():
+        pytest.skip("reference build absent")
+    for n in (8, 9, 13, 14, 100, 1000, 4097, 12345, 1 << 16, 1 << 20):
+        s = _reddish_spectrum(n, n)
+        a, b = ob.deredden(s), ob.deredden(s, reference=True)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), n
+        assert a[0] == 1.0
+
+
+def test_reference_realfft_packing_and_precision():
+    """The reference's realfft (as built here) equals the FP64 packed
+    transform to FP32 rounding: every bin k within 2e-6 of |X[k]| + |X[M-k]|
+    (both come from one pair of complex FFT outputs) plus 1e-5 of the
+    spectrum's rms magnitude, and the rms error below 2e-7 of it.  (A packing, sign or scale
+    slip would be of order 1.)"""
+    if not ob.have_reference():
+        pytest.skip("reference build absent")
+    ob.quiet_wisdom()
+    for logn in (15, 18):
+        n = 1 << logn
+        rng = np.random.default_rng(logn)
+        x = (rng.standard_normal(n) + 0.02 * np.cumsum(rng.standard_normal(n))).astype(np.float32)
+        want = ob.packed_rfft(x)
+        got = ob.ref_realfft(x).astype(np.complex128)
+        rms = np.sqrt(np.mean(np.abs(want) ** 2))
+        err = np.abs(got - want)
+        assert np.all(err <= 2e-6 * ob.pair_magnitude(want) + 1e-5 * rms), logn
+        assert np.sqrt(np.mean(err ** 2)) <= 2e-7 * rms, logn
+
+
+def test_dat_input_is_realfft_then_deredden_then_bin0(tmp_path):
+    """For a .dat input the reference searches realfft -> deredden with bin 0
+    then set to (1, 1) (src/accel_utils.c:1696-1753, 1829-1834), nothing
+    more: its in-memory spectrum equals those steps applied to the series,
+    bitwise, and the oracle's deredden gives the same bits."""
+    if not ob.have_reference():
+        pytest.skip("reference build absent")
+    ob.quiet_wisdom()
+    N, dt = 1 << 16, 64e-6
+    rng = np.random.default_rng(16)
+    ts = (rng.standard_normal(N) + 0.02 * np.cumsum(rng.standard_normal(N))).astype(np.float32)
+    root = str(tmp_path / "series")
+    ts.tofile(root + ".dat")
+    synth.write_inf(root, N, dt)
+    ref = ob.RefSearch(root + ".dat", ["-zmax", "20", "-wmax", "60", "-numharm", "4"])
+    got = ref.spectrum()
+    ref.close()
+    raw = ob.ref_realfft(ts)
+    for reference in (True, False):
+        want = ob.deredden(raw, reference=reference)
+        want[0] = 1.0 + 1.0j
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), reference
