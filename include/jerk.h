@@ -214,6 +214,32 @@ int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
                        int corr_uselen, float nph, float *volume, int *numrs, long long *rlo,
                        void *stream);
 
+/* Candidate polishing on the GPU: the volume search of the reference's
+ * harmonic polishing, max_rzw_arr_harmonics (src/maximize_rzw.c:84-190),
+ * which optimize_accelcand (src/accel_utils.c:573-657) runs for every final
+ * candidate of a search with -wmax.  Per harmonic n = numharm .. 1 it
+ * correlates the spectrum with 17 x 17 (z, w) responses at 8 points per bin
+ * around (n r, n z, n w), sums |amplitude|^2 / locpow over the harmonics and
+ * takes the first strict maximum; *rout, *zout, *wout are the polished
+ * fundamental values as the reference computes them, *maxpow the summed
+ * power there.
+ *   spectrum  numdata complex64 values on the HOST (the searched spectrum;
+ *             value 0 is obs.lobin), read around each harmonic only
+ *   rin       the candidate's r minus obs.lobin; zin, win its z and w
+ *   locpow    numharm floats: get_localpower3d (src/characteristics.c:75-135)
+ *             of harmonic n = numharm - i at (n rin, n zin, n win), as float
+ * A jerk_polisher holds the device buffers (grown to the largest candidate)
+ * and runs on its stream (NULL: its own); one call at a time per polisher.
+ * Correlation or response FFTs longer than 8192 points (about zmax 300 with
+ * wmax 600 and above) return JERK_EUNSUPPORTED.  Not in the reference: the
+ * reference runs this on the CPU, one candidate after another. */
+typedef struct jerk_polisher jerk_polisher;
+int jerk_polisher_create(jerk_polisher **polisher, void *stream);
+void jerk_polisher_destroy(jerk_polisher *polisher);
+int jerk_polish_rzw(jerk_polisher *polisher, const void *spectrum, long long numdata, int numharm,
+                    double rin, double zin, double win, const float *locpow, double *rout,
+                    double *zout, double *wout, float *maxpow);
+
 /* The search's input from a time series, on the GPU: the steps the reference
  * takes for a ".dat" input (src/accel_utils.c:1696-1753) before it searches.
  *

@@ -149,6 +149,19 @@ class RefSearch:
             raise RuntimeError("the reference holds no spectrum in memory")
         return out[:n]
 
+    def polish(self, numharm: int, r: float, z: float, w: float):
+        """The reference's polishing volume search for a candidate (r
+        relative to obs.lobin): ((r, z, w) polished, locpow per harmonic,
+        highest harmonic first)."""
+        f = _ref().ref_polish
+        f.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_void_p,
+                      C.c_void_p]
+        rzw = np.zeros(3)
+        lp = np.zeros(numharm, dtype=np.float32)
+        if f(self.ctx, numharm, r, z, w, rzw.ctypes.data, lp.ctypes.data) != 0:
+            raise RuntimeError("the reference holds no spectrum in memory")
+        return tuple(float(v) for v in rzw), lp
+
     def close(self):
         if self.ctx:
             _ref().ref_close(self.ctx)

@@ -324,6 +324,73 @@ int ref_gen_w_response(double roffset, int numbetween, double z, double w, int n
  * only the single-thread order of insertions is deterministic. */
 void ref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
 
+/* The reference's candidate optimisation (optimize_accelcand,
+ * src/accel_utils.c:573-657) of one candidate; obs must hold the spectrum in
+ * memory (a .dat input or a memory-mapped .fft).  out receives, per
+ * harmonic h: pows, hirs, hizs, hiws and the 7 doubles of rderivs (pow,
+ * phs, dpow, dphs, d2pow, d2phs, locpow), 11 doubles each; *sigma the
+ * recomputed sigma.  Returns 0, or -1 without a spectrum in memory. */
+int ref_optimize_cand(refctx *c, float power, int numharm, double r, double z, double w,
+                      double *out, float *sigma)
+{
+    if (!c->obs.fft)
+        return -1;
+    accelcand cand;
+    memset(&cand, 0, sizeof(cand));
+    cand.power = power;
+    cand.numharm = numharm;
+    cand.r = r;
+    cand.z = z;
+    cand.w = w;
+    optimize_accelcand(&cand, &c->obs);
+    for (int h = 0; h < numharm; h++) {
+        double *o = out + 11 * h;
+        o[0] = cand.pows[h];
+        o[1] = cand.hirs[h];
+        o[2] = cand.hizs[h];
+        o[3] = cand.hiws[h];
+        o[4] = cand.derivs[h].pow;
+        o[5] = cand.derivs[h].phs;
+        o[6] = cand.derivs[h].dpow;
+        o[7] = cand.derivs[h].dphs;
+        o[8] = cand.derivs[h].d2pow;
+        o[9] = cand.derivs[h].d2phs;
+        o[10] = cand.derivs[h].locpow;
+    }
+    *sigma = cand.sigma;
+    free(cand.pows);
+    free(cand.hirs);
+    free(cand.hizs);
+    free(cand.hiws);
+    free(cand.derivs);
+    return 0;
+}
+
+/* The reference's harmonic polishing volume search (max_rzw_arr_harmonics,
+ * src/maximize_rzw.c:84-190) for a candidate at (rin, zin, win), rin
+ * relative to obs.lobin: rzw[0..2] = polished r, z, w; locpow[i] = the float
+ * local power of harmonic n = numharm - i that it divides by
+ * (get_localpower3d, src/characteristics.c:75-135).  -1 without a spectrum
+ * in memory. */
+int ref_polish(refctx *c, int numharm, double rin, double zin, double win, double *rzw,
+               float *locpow)
+{
+    if (!c->obs.fft)
+        return -1;
+    rderivs *d = (rderivs *)malloc(sizeof(rderivs) * numharm);
+    double *pows = (double *)malloc(sizeof(double) * numharm);
+    for (int i = 0; i < numharm; i++) {
+        const int n = numharm - i;
+        locpow[i] = (float)get_localpower3d(c->obs.fft, c->obs.numbins, rin * n, zin * n,
+                                            win * n);
+    }
+    max_rzw_arr_harmonics(c->obs.fft, c->obs.numbins, numharm, rin, zin, win, rzw, rzw + 1,
+                          rzw + 2, d, pows);
+    free(d);
+    free(pows);
+    return 0;
+}
+
 /* The spectrum the reference searches, when it holds one in memory: a .dat
  * input after its realfft and deredden (src/accel_utils.c:1696-1753), or a
  * memory-mapped .fft.  Copies up to max complex values; -1 if none. */

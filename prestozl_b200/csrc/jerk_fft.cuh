@@ -217,6 +217,7 @@ __device__ __forceinline__ float2 twiddle(const float2 *tw, int m)
 __host__ __device__ __forceinline__ constexpr int pad(int i) { return i + (i >> 4); }
 template <int N>
 __host__ __device__ constexpr int fft_buf_len() { return N + N / 16; }
+__host__ __device__ constexpr int fft_buf_len_rt(int n) { return n + n / 16; }
 
 template <int X>
 struct IsPow2 {

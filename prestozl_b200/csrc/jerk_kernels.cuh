@@ -106,6 +106,8 @@ struct RowGroup {
 
 // Records msg as the text jerk_last_error returns and passes code back.
 int set_error(int code, const char *msg);
+// w_resp_halfwidth(z, w, LOWACC) (src/responses.c:49-84).
+int w_resp_halfwidth_lowacc(double z, double w);
 
 // The reference's fast inverse square root (src/misc_utils.c:293-304): the
 // published bit-level first guess and one Newton step in float, in the

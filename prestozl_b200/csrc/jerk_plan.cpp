@@ -109,6 +109,8 @@ static int w_resp_halfwidth(double z, double w)
     return (int)(1.1 * maxdev) + 16;
 }
 
+int jerk::w_resp_halfwidth_lowacc(double z, double w) { return w_resp_halfwidth(z, w); }
+
 static long long next2_to_n(long long x)
 {
     long long n = 1;

@@ -110,7 +110,8 @@ EXPORTS = [
     "jerk_server_create", "jerk_server_submit", "jerk_server_poll", "jerk_server_stats",
     "jerk_server_destroy", "jerk_realfft_scratch_bytes", "jerk_realfft",
     "jerk_deredden_scratch_bytes", "jerk_deredden", "jerk_spectrum_scratch_bytes",
-    "jerk_spectrum_from_timeseries",
+    "jerk_spectrum_from_timeseries", "jerk_polisher_create", "jerk_polisher_destroy",
+    "jerk_polish_rzw",
 ]
 
 
@@ -186,6 +187,13 @@ def lib() -> C.CDLL:
         getattr(L, f).argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
                                   C.c_void_p]
     L.jerk_deredden.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
+    L.jerk_polisher_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p]
+    L.jerk_polisher_destroy.argtypes = [C.c_void_p]
+    L.jerk_polisher_destroy.restype = None
+    L.jerk_polish_rzw.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_double,
+                                  C.c_double, C.c_double, C.c_void_p, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_float)]
     _lib = L
     return L
 
@@ -344,6 +352,38 @@ def spectrum_from_timeseries(ts, out=None):
     out = _series_out(ts, out)
     return _input_call("jerk_spectrum_from_timeseries", "jerk_spectrum_scratch_bytes", ts,
                        ts.numel(), out)
+
+
+class Polisher:
+    """Candidate polishing on the GPU (jerk_polish_rzw): the volume search of
+    the reference's harmonic polishing (src/maximize_rzw.c:84-190)."""
+
+    def __init__(self):
+        self.ptr = C.c_void_p()
+        _check(lib().jerk_polisher_create(C.byref(self.ptr), None))
+
+    def polish(self, spectrum: np.ndarray, numharm: int, r: float, z: float, w: float,
+               locpow) -> Tuple[float, float, float, float]:
+        """(r, z, w, summed power) polished; r relative to the spectrum's bin
+        0; locpow[i] the local power of harmonic numharm - i."""
+        spec = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        lp = np.ascontiguousarray(locpow, dtype=np.float32)
+        ro, zo, wo, mp = C.c_double(), C.c_double(), C.c_double(), C.c_float()
+        _check(lib().jerk_polish_rzw(self.ptr, spec.ctypes.data, len(spec), numharm, r, z, w,
+                                     lp.ctypes.data, C.byref(ro), C.byref(zo), C.byref(wo),
+                                     C.byref(mp)))
+        return ro.value, zo.value, wo.value, mp.value
+
+    def close(self):
+        if self.ptr:
+            lib().jerk_polisher_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _spectrum_arg(spectrum):

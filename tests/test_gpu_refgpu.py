@@ -14,6 +14,7 @@ match.
 import json
 import os
 import subprocess
+import time
 
 import pytest
 
@@ -71,15 +72,19 @@ def test_paper_scale_dropin_matches_reference_gpu(tmp_path):
     spec = spec.cpu().numpy()
     torch.cuda.synchronize()
     flags = ["-zmax", "200", "-wmax", "300", "-numharm", "16", "-sigma", "3.0", "-batchsize", "8"]
-    files = {}
+    files, wall = {}, {}
     for name, cli in (("refgpu", ob.REFGPU_CLI), ("dropin", ob.DROPIN_CLI)):
         d = tmp_path / name
         d.mkdir()
         synth.write_fft(str(d / "paper"), spec, N, dt)
         env = dict(os.environ, PRESTO=str(d))
+        t0 = time.perf_counter()
         out = subprocess.run([cli, *flags, "paper.fft"], cwd=d, env=env, capture_output=True,
                              text=True, timeout=900)
+        wall[name] = time.perf_counter() - t0
         assert out.returncode == 0, out.stderr[-2000:]
         files[name] = (d / "paper_ACCEL_200_JERK_300").read_text()
+    print(f"paper scale, whole accelsearch_cu run: reference GPU {wall['refgpu']:.1f} s, "
+          f"drop-in {wall['dropin']:.1f} s; {len(accel_rows(files['refgpu']))} ACCEL rows")
     assert len(accel_rows(files["refgpu"])) > 10
     assert files["dropin"] == files["refgpu"]
