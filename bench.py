@@ -147,8 +147,11 @@ def make_spectrum(seed: int, device):
 # CPU reference: the reference's own accelsearch (compiled from its sources
 # into oracle/_ref), on a bounded sample of rsteps of one spectrum.
 
-def reference_sample(spec_np, threads: int, target_s: float = 15.0, max_steps: int = 0):
-    """(seconds per rstep, rsteps timed, threads) of the reference CPU search."""
+def reference_sample(spec_np, threads: int, target_s: float = 15.0, max_steps: int = 0,
+                     polish_cands=None, polish_s: float = 10.0):
+    """(seconds per rstep, rsteps timed, threads, polishing) of the reference CPU
+    search; polishing = the reference's candidate polishing (one core, as its
+    CPU2 runs it) timed on up to polish_s seconds of the given candidates."""
     from oracle import bindings as ob
     from prestozl_b200 import synth
 
@@ -169,8 +172,104 @@ def reference_sample(spec_np, threads: int, target_s: float = 15.0, max_steps: i
         t0 = time.perf_counter()
         ref.search(max_steps=n)
         dt = time.perf_counter() - t0
+        polish = None
+        if polish_cands is not None and len(polish_cands):
+            ob.set_threads(1)
+            done, t_pol = 0, 0.0
+            for c in polish_cands:
+                t0 = time.perf_counter()
+                ref.polish(int(c["numharm"]), float(c["r"]) - ref.obs.lobin, float(c["z"]),
+                           float(c["w"]))
+                t_pol += time.perf_counter() - t0
+                done += 1
+                if t_pol > polish_s:
+                    break
+            polish = {"candidates": done, "s_per_candidate": t_pol / done, "cores": 1}
         ref.close()
-    return dt / n, n, threads
+    return dt / n, n, threads, polish
+
+
+def input_prep_leg(device, reps: int = 5):
+    """The .dat preparation on the GPU (jerk_spectrum_from_timeseries: realfft,
+    deredden, bin 0) of one N_SAMPLES float32 series already in HBM."""
+    import torch
+
+    from prestozl_b200 import jerk
+
+    g = torch.Generator(device=device)
+    g.manual_seed(11)
+    ts = torch.randn(N_SAMPLES, device=device, generator=g)
+    out = torch.empty(N_SAMPLES // 2, dtype=torch.complex64, device=device)
+    for _ in range(2):
+        jerk.spectrum_from_timeseries(ts, out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        jerk.spectrum_from_timeseries(ts, out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    alg = 8.0 * N_SAMPLES  # the series read once, the spectrum written once
+    return {"samples": N_SAMPLES, "ms_per_series": ms, "algorithmic_bytes": alg,
+            "achieved_gbs": alg / ms / 1e6, "kernels": "rf_twiddle x2, rf_column, rf_row, "
+            "rf_post, dr_level, dr_scale", "launches": 7,
+            "note": "three FFT passes and two red-noise passes move about 5x the algorithmic "
+                    "bytes; one-off per series (about 0.02 % of its search)"}
+
+
+def polish_leg(spec_np, cands, max_cands: int = 64):
+    """GPU polishing (jerk_polish_rzw) of a search's final candidates.  The
+    local powers only scale the per-harmonic sums, so 1.0 is passed: the
+    device work is the same."""
+    from prestozl_b200 import jerk
+
+    sel = list(cands[:max_cands])
+    if not sel:
+        return None
+    pol = jerk.Polisher()
+    args = [(int(c["numharm"]), float(c["r"]), float(c["z"]), float(c["w"])) for c in sel]
+    nh, r, z, w = args[0]
+    pol.polish(spec_np, nh, r, z, w, np.ones(nh, np.float32))  # buffers, modules
+    t0 = time.perf_counter()
+    for nh, r, z, w in args:
+        pol.polish(spec_np, nh, r, z, w, np.ones(nh, np.float32))
+    dt = time.perf_counter() - t0
+    pol.close()
+    counts = {}
+    for nh, _, _, _ in args:
+        counts[str(nh)] = counts.get(str(nh), 0) + 1
+    return {"candidates": len(args), "ms_per_candidate": dt * 1000.0 / len(args),
+            "numharm_counts": counts,
+            "timing": "host wall clock around each synchronous call (upload, 6 kernel kinds, "
+                      "result copy)",
+            "launches_per_candidate": "2 + 3 per distinct kernel FFT length + 1 per w-response "
+                                      "FFT length + 1"}
+
+
+def run_extras(args):
+    """--extras-only: the input-preparation and polishing legs alone, on one
+    paper-scale spectrum with candidates on the search's grid (a few hundred
+    MB on the device; the form profiled with ncu).  Polishing runs first."""
+    import torch
+
+    from prestozl_b200 import build
+
+    build.build()
+    torch.cuda.set_device(0)
+    spec_np = make_spectrum(7, "cuda").cpu().numpy()
+    rng = np.random.default_rng(5)
+    cands = []
+    for nh in (16, 8, 4, 2):
+        for _ in range(args.extras_cands):
+            r = float(rng.integers(40000 * nh, (1 << 24) - 40000)) / (2 * nh) * 2
+            cands.append({"numharm": nh, "r": r,
+                          "z": float(rng.integers(-ZMAX // 2, ZMAX // 2 + 1)) * 2 / nh,
+                          "w": float(rng.integers(-WMAX // 20, WMAX // 20 + 1)) * 20 / nh})
+    pol = polish_leg(spec_np, cands, max_cands=len(cands))
+    prep = input_prep_leg("cuda", reps=args.extras_reps)
+    prep["frac_of_hbm"] = prep["achieved_gbs"] / peaks()[0]
+    print(json.dumps({"impl": "ours", "mode": "extras-only", "input_prep": prep, "polish": pol}))
 
 
 def reference_gpu(spec_np):
@@ -219,7 +318,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     per, times = [], []
     for i in range(args.warmup + args.steps):
-        sec, n, _ = reference_sample(spec, threads, target_s=args.ref_seconds)
+        sec, n, _, _ = reference_sample(spec, threads, target_s=args.ref_seconds)
         if i >= args.warmup:
             times.append(sec * plan_rsteps)
             per.append(n)
@@ -289,6 +388,14 @@ def main():
     ap.add_argument("--max-active", type=int, default=3, help="served: searches in flight")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the input-preparation and candidate-polishing legs")
+    ap.add_argument("--extras-only", action="store_true",
+                    help="only the input-preparation and polishing legs (small footprint)")
+    ap.add_argument("--extras-cands", type=int, default=4,
+                    help="--extras-only: candidates per harmonic count (16, 8, 4, 2)")
+    ap.add_argument("--extras-reps", type=int, default=5,
+                    help="--extras-only: timed input preparations")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference's own GPU search on this GPU")
@@ -300,6 +407,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.extras_only:
+        run_extras(args)
         return
 
     import torch
@@ -363,6 +473,8 @@ def main():
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         ncands.append(len(c))
+        if i == 0:
+            cands0 = c
     torch.cuda.synchronize()
     barrier()
     plain_wall = time.perf_counter() - t_all0
@@ -487,6 +599,14 @@ def main():
                             "peak_source": peak_kind,
                             "algorithmic": "every volume of the batch read once"}
     launches_per_spectrum = sum(v["launches"] for v in kstats.values())
+
+    # ---- next to the search: input preparation and candidate polishing
+    extras = {}
+    if not args.no_extras:
+        extras["input_prep"] = input_prep_leg("cuda")
+        extras["input_prep"]["frac_of_hbm"] = extras["input_prep"]["achieved_gbs"] / peaks()[0]
+        spec0_np = specs[0].cpu().numpy()
+        extras["polish"] = polish_leg(spec0_np, cands0)
     timed_spectra = args.steps * (2 if served else 1)
 
     value = served_info["value"] if served else plain_value
@@ -547,6 +667,7 @@ def main():
             "wall_s": plain_wall,
             "candidates_per_spectrum": ncands,
         }
+        line.update(extras)
         if served:
             line["plain_dropin"] = dropin
             line["speedup_vs_plain"] = value / plain_value
@@ -557,12 +678,18 @@ def main():
                 if ob.have_reference():
                     spec_np = specs[0].cpu().numpy()
                     threads = os.cpu_count() or 1
-                    sec, n, th = reference_sample(spec_np, threads, target_s=args.ref_seconds)
+                    sec, n, th, pol = reference_sample(
+                        spec_np, threads, target_s=args.ref_seconds,
+                        polish_cands=cands0 if line.get("polish") else None)
                     cpu_val = 3600.0 / (sec * nrsteps)
                     line["cpu_baseline"] = {
                         "value": cpu_val, "unit": UNIT, "cores": th, "kind": "reference",
                         "sample": f"first {n} rsteps of one spectrum ({sec * n:.1f} s), scaled "
                                   f"by {nrsteps} rsteps; OpenMP, FFT = project FFTW stand-in"}
+                    if pol:
+                        line["cpu_baseline"]["polish"] = pol
+                        line["polish"]["speedup_vs_reference_cpu"] = (
+                            pol["s_per_candidate"] * 1000.0 / line["polish"]["ms_per_candidate"])
             except Exception as exc:  # the baseline is reported, never required
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)}
         if world == 1 and not args.no_ref_gpu and not nsearch:

@@ -27,7 +27,8 @@
 // as runs of blocks of equal length (about 130 runs cover 2^31 bins), passed
 // to the kernels by value.  One warp per block takes the median power (the
 // value of rank (n-1)/2, which the reference's quickselect returns) over
-// ln 2; one warp per segment between block midpoints then scales its bins by
+// ln 2 (a bitonic sort in registers); one warp per segment between block
+// midpoints then scales its bins by
 // invsqrtf of the linearly interpolated level, in the reference's float and
 // double steps.
 
@@ -81,23 +82,39 @@ __global__ void rf_twiddle_kernel(float2 *tw)
 }
 
 // Step 1: CTA m2 transforms column m2 of z (stride R2) and stores row k1 of
-// the scratch at a[k1 * R2 + m2], times exp(-2 pi i m2 k1 / M).
+// the scratch at a[k1 * R2 + m2], times exp(-2 pi i m2 k1 / M).  The twiddle
+// is the double product of two per-CTA tables, exp(-2 pi i m2 lo / M) and
+// exp(-2 pi i m2 64 hi / M) for k1 = 64 hi + lo (exponents reduced mod M
+// exactly), rounded once to float.
+constexpr int kTwLo = 64;
 template <int R1>
 __global__ void __launch_bounds__(FftPlan<R1>::T)
     rf_column_kernel(const float2 *__restrict__ z, int R2, const float2 *__restrict__ tw,
                      float2 *__restrict__ a)
 {
     constexpr int T = FftPlan<R1>::T;
+    constexpr int NHI = (R1 + kTwLo - 1) / kTwLo;
     extern __shared__ float2 rf_buf[];
+    __shared__ double2 t_lo[kTwLo], t_hi[NHI];
     const int tid = threadIdx.x;
     const int m2 = blockIdx.x;
     const long long M = (long long)R1 * R2;
-    auto in = [&](int r) -> float2 { return z[m2 + (size_t)R2 * (size_t)(tid + r * T)]; };
-    auto out = [&](int k1, float2 y) {
-        const long long e = ((long long)m2 * k1) & (M - 1);
+    for (int i = tid; i < kTwLo + NHI; i += T) {
+        const long long e = i < kTwLo ? ((long long)m2 * i) & (M - 1)
+                                      : ((long long)m2 * kTwLo * (i - kTwLo)) & (M - 1);
         double s, c;
         sincospi(-2.0 * (double)e / (double)M, &s, &c);
-        a[(size_t)k1 * R2 + m2] = cmul(y, make_float2((float)c, (float)s));
+        if (i < kTwLo)
+            t_lo[i] = make_double2(c, s);
+        else
+            t_hi[i - kTwLo] = make_double2(c, s);
+    }
+    // fft_block's first barrier orders these writes before the reads in out()
+    auto in = [&](int r) -> float2 { return z[m2 + (size_t)R2 * (size_t)(tid + r * T)]; };
+    auto out = [&](int k1, float2 y) {
+        const double2 u = t_hi[k1 / kTwLo], v = t_lo[k1 % kTwLo];
+        const float2 w = make_float2((float)(u.x * v.x - u.y * v.y), (float)(u.x * v.y + u.y * v.x));
+        a[(size_t)k1 * R2 + m2] = cmul(y, w);
     };
     fft_block<R1, -1>(rf_buf, tw, tid, in, out);
 }
@@ -285,7 +302,43 @@ __device__ __forceinline__ float dr_power(float2 v)
 
 constexpr int kDrWarps = 8;
 
-// One warp per block: level[b] = median power / ln 2.
+// Ascending bitonic sort of 128 values held 4 per lane (value e = lane + 32 j
+// in v[j]) across one warp.
+__device__ __forceinline__ void warp_sort128(float (&v)[4], int lane)
+{
+#pragma unroll
+    for (int s = 2; s <= 128; s <<= 1) {
+#pragma unroll
+        for (int d = s >> 1; d > 0; d >>= 1) {
+            if (d >= 32) {
+                const int dj = d >> 5;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    if ((j & dj) == 0) {
+                        const bool asc = ((lane + 32 * j) & s) == 0;
+                        const float a = v[j], b = v[j | dj];
+                        v[j] = asc ? fminf(a, b) : fmaxf(a, b);
+                        v[j | dj] = asc ? fmaxf(a, b) : fminf(a, b);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int e = lane + 32 * j;
+                    const float o = __shfl_xor_sync(0xffffffffu, v[j], d);
+                    const bool keep_min = (((e & s) == 0) == ((e & d) == 0));
+                    v[j] = keep_min ? fminf(v[j], o) : fmaxf(v[j], o);
+                }
+            }
+        }
+    }
+}
+
+// One warp per block: level[b] = median power / ln 2.  Blocks are at most 128
+// bins long below 2^31 bins ((int)(6 ln 2^31) = 128): sorted in registers,
+// padded with +inf; the value at sorted position (n-1)/2 is the one the
+// reference's quickselect returns.  (Longer blocks, which the walk never
+// makes, would take the stable-rank count.)
 __global__ void __launch_bounds__(32 * kDrWarps)
     dr_level_kernel(const float2 *__restrict__ x, const __grid_constant__ DrRuns runs, int nb,
                     double ln2, float *__restrict__ level)
@@ -294,15 +347,28 @@ __global__ void __launch_bounds__(32 * kDrWarps)
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * kDrWarps + w;
     if (b >= nb)
-        return;  // whole warps leave; only __syncwarp below
+        return;  // whole warps leave; only warp-level syncs below
     const int2 blk = dr_block(runs, b);
     const int n = blk.y;
+    const int k = (n - 1) / 2;
+    if (n <= 128) {
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int i = lane + 32 * j;
+            v[j] = i < n ? dr_power(x[blk.x + i]) : INFINITY;
+        }
+        warp_sort128(v, lane);
+        const float m0 = __shfl_sync(0xffffffffu, v[0], k & 31);
+        const float m1 = __shfl_sync(0xffffffffu, v[1], k & 31);
+        if (lane == 0)
+            level[b] = (float)((double)(k < 32 ? m0 : m1) / ln2);
+        return;
+    }
     float *p = pw[w];
     for (int i = lane; i < n; i += 32)
         p[i] = dr_power(x[blk.x + i]);
     __syncwarp();
-    // the element whose position in a stable sort is (n-1)/2
-    const int k = (n - 1) / 2;
     for (int i = lane; i < n; i += 32) {
         const float v = p[i];
         int pos = 0;
