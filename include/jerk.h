@@ -304,6 +304,11 @@ typedef struct jerk_request {
     float sigma;
     double flo, fhi;             /* accelsearch's -flo / -fhi (defaults 1, 10000) */
     long long tag;               /* the caller's id, returned with the result */
+    int timeseries;              /* nonzero: `spectrum` holds N float32 samples of a time
+                                    series (a dedispersed trial), and the server makes the
+                                    spectrum on the GPU as the reference does for a .dat
+                                    input (jerk_spectrum_from_timeseries); numbins is taken
+                                    as N / 2.  N: a power of two from 2^15 to 2^27 */
 } jerk_request;
 
 typedef struct jerk_result {

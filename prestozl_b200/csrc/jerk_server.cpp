@@ -68,12 +68,19 @@ struct Slot {
     jerk_plan *plan = nullptr;
     long long bytes = 0;
     double t_submit = 0, t_start = 0;
+    void *series = nullptr;  // time-series requests: the series, then its spectrum, + scratch
+    long long series_bytes = 0;
 };
 
 struct IdlePlan {
     jerk_plan *plan;
     jerk_obs obs;
     BankKey key;
+    long long bytes;
+};
+
+struct SeriesBuf {
+    void *ptr;
     long long bytes;
 };
 
@@ -98,6 +105,7 @@ struct jerk_server {
     // worker-owned
     std::vector<Slot> active;
     std::vector<IdlePlan> idle;
+    std::vector<SeriesBuf> series_pool;  // time-series buffers between requests
     std::map<BankKey, Bank> banks;
     long long bytes_in_use = 0;
     // counters (under mu)
@@ -146,6 +154,65 @@ static long long plan_footprint(const Geometry &g, int batch)
            g.obs.numbins * 8 + (64LL << 20);
 }
 
+// Device bytes of a time-series request's buffer: the series (turned into its
+// spectrum in place), then the preparation's scratch.
+static long long series_footprint(const jerk_request &r)
+{
+    if (!r.timeseries)
+        return 0;
+    return ((4 * r.N + 255) & ~255LL) + jerk_spectrum_scratch_bytes(r.N);
+}
+
+// Back to the pool (freeing would synchronise the device under the other
+// searches); the stream orders its next use after everything that read it.
+static void release_series(jerk_server *s, Slot &sl)
+{
+    if (sl.series) {
+        s->series_pool.push_back(SeriesBuf{sl.series, sl.series_bytes});
+        sl.series = nullptr;
+        sl.series_bytes = 0;
+    }
+}
+
+static bool pool_fits(const jerk_server *s, long long bytes)
+{
+    for (const auto &b : s->series_pool)
+        if (b.bytes >= bytes)
+            return true;
+    return false;
+}
+
+// Upload (if on the host) and prepare a time-series request's spectrum on the
+// server's stream, ahead of its search there.
+static int prepare_series(jerk_server *s, Slot &sl)
+{
+    const long long bytes = series_footprint(sl.req);
+    for (size_t i = 0; i < s->series_pool.size(); i++) {
+        if (s->series_pool[i].bytes >= bytes) {
+            sl.series = s->series_pool[i].ptr;
+            sl.series_bytes = s->series_pool[i].bytes;
+            s->series_pool.erase(s->series_pool.begin() + i);
+            break;
+        }
+    }
+    if (!sl.series) {
+        const int rc = jerk_device_alloc(bytes, &sl.series);
+        if (rc != JERK_OK)
+            return rc;
+        sl.series_bytes = bytes;
+        s->bytes_in_use += bytes;
+    }
+    const long long sbytes = 4 * sl.req.N;
+    const long long off = (sbytes + 255) & ~255LL;
+    if (cudaMemcpyAsync(sl.series, sl.req.spectrum, (size_t)sbytes,
+                        sl.req.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                        s->stream) != cudaSuccess)
+        return JERK_ECUDA;
+    return jerk_spectrum_from_timeseries((const float *)sl.series, sl.req.N, sl.series,
+                                         (char *)sl.series + off, sl.series_bytes - off,
+                                         s->stream);
+}
+
 static void release_bank(jerk_server *s, const BankKey &k)
 {
     auto it = s->banks.find(k);
@@ -158,6 +225,11 @@ static void release_bank(jerk_server *s, const BankKey &k)
 // Free idle plans and unused banks until `need` more bytes fit the budget.
 static void make_room(jerk_server *s, long long need)
 {
+    while (s->bytes_in_use + need > s->cfg.hbm_budget_bytes && !s->series_pool.empty()) {
+        jerk_device_free(s->series_pool.back().ptr);
+        s->bytes_in_use -= s->series_pool.back().bytes;
+        s->series_pool.pop_back();
+    }
     while (s->bytes_in_use + need > s->cfg.hbm_budget_bytes && !s->idle.empty()) {
         IdlePlan ip = s->idle.front();
         s->idle.erase(s->idle.begin());
@@ -223,7 +295,10 @@ static bool admit(jerk_server *s, const Pending &pd)
         s->banks[sl.key].users++;  // pinned while this request is admitted
     const long long bank_bytes =
         have_bank ? 0 : 8 * jerk_bank_elements(sl.geo.subs.data(), (int)sl.geo.subs.size());
-    const long long need = (sl.plan ? 0 : plan_footprint(sl.geo, s->cfg.batch_rsteps)) + bank_bytes;
+    const long long series_bytes =
+        pool_fits(s, series_footprint(pd.req)) ? 0 : series_footprint(pd.req);
+    const long long need = (sl.plan ? 0 : plan_footprint(sl.geo, s->cfg.batch_rsteps)) + bank_bytes +
+                           series_bytes;
     if (need > s->cfg.hbm_budget_bytes) {
         // can never fit, even alone: fail this request, keep serving the rest
         if (sl.plan)
@@ -278,8 +353,17 @@ static bool admit(jerk_server *s, const Pending &pd)
         sl.bytes = jerk_plan_device_bytes(sl.plan);
         s->bytes_in_use += sl.bytes;
     }
-    rc = jerk_search_async(sl.plan, pd.req.spectrum, pd.req.on_device, 0, 0);
+    if (pd.req.timeseries) {
+        rc = prepare_series(s, sl);
+        if (rc == JERK_OK)
+            rc = jerk_search_async(sl.plan, sl.series, 1, 0, 0);
+    } else {
+        rc = jerk_search_async(sl.plan, pd.req.spectrum, pd.req.on_device, 0, 0);
+    }
     if (rc != JERK_OK) {
+        if (sl.series)
+            cudaStreamSynchronize(s->stream);  // nothing may still read the buffer
+        release_series(s, sl);
         release_bank(s, sl.key);
         s->idle.push_back(IdlePlan{sl.plan, sl.geo.obs, sl.key, sl.bytes});
         finish(s, pd.req, pd.t_submit, sl.t_start, rc, nullptr, 0);
@@ -351,6 +435,11 @@ static void worker_main(jerk_server *s)
             long long n = 0;
             const int rc = ready < 0 ? ready : jerk_search_collect(sl.plan, &c, &n, nullptr);
             release_bank(s, sl.key);
+            if (sl.series) {
+                if (rc < 0)
+                    cudaStreamSynchronize(s->stream);  // a failed search may have left work queued
+                release_series(s, sl);
+            }
             if (rc < 0) {
                 // a plan whose search failed is not reused
                 jerk_plan_destroy(sl.plan);
@@ -370,6 +459,9 @@ static void worker_main(jerk_server *s)
         }
     }
 out:
+    for (auto &b : s->series_pool)
+        jerk_device_free(b.ptr);
+    s->series_pool.clear();
     for (auto &ip : s->idle)
         jerk_plan_destroy(ip.plan);
     s->idle.clear();
@@ -418,10 +510,16 @@ extern "C" int jerk_server_submit(jerk_server *s, const jerk_request *req)
 {
     if (!s || !req || !req->spectrum)
         return JERK_EINVAL;
+    jerk_request r = *req;
+    if (r.timeseries) {
+        if (jerk_spectrum_scratch_bytes(r.N) <= 0)
+            return JERK_EUNSUPPORTED;
+        r.numbins = r.N / 2;
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop)
         return JERK_EINVAL;
-    s->pending.push_back(Pending{*req, now_s()});
+    s->pending.push_back(Pending{r, now_s()});
     s->submitted++;
     s->cv_work.notify_all();
     return JERK_OK;

@@ -79,7 +79,8 @@ class Request(C.Structure):
     _fields_ = [("spectrum", C.c_void_p), ("on_device", C.c_int), ("numbins", C.c_longlong),
                 ("N", C.c_longlong), ("dt", C.c_double), ("zmax", C.c_int), ("wmax", C.c_int),
                 ("wmax_given", C.c_int), ("numharm", C.c_int), ("sigma", C.c_float),
-                ("flo", C.c_double), ("fhi", C.c_double), ("tag", C.c_longlong)]
+                ("flo", C.c_double), ("fhi", C.c_double), ("tag", C.c_longlong),
+                ("timeseries", C.c_int)]
 
 
 class Result(C.Structure):
@@ -528,15 +529,30 @@ class JerkServer:
 
     def submit(self, spectrum, N: int, dt: float, zmax: int, wmax: int, numharm: int,
                sigma: float, wmax_given: bool = True, flo: float = 1.0, fhi: float = 10000.0,
-               tag: Optional[int] = None) -> int:
-        ptr, dev, keep = _spectrum_arg(spectrum)
-        numbins = int(spectrum.shape[0]) if dev else len(keep)
+               tag: Optional[int] = None, timeseries: bool = False) -> int:
+        """Queue one search.  ``spectrum``: the complex64 spectrum (numpy or a
+        CUDA tensor), or with ``timeseries=True`` the N float32 samples of a
+        time series, which the server turns into its spectrum on the GPU as
+        the reference does for a .dat input."""
+        if timeseries:
+            if getattr(spectrum, "is_cuda", False):
+                ptr, dev, keep = C.c_void_p(spectrum.data_ptr()), 1, spectrum
+                n = int(spectrum.numel())
+            else:
+                keep = np.ascontiguousarray(spectrum, dtype=np.float32)
+                ptr, dev, n = C.c_void_p(keep.ctypes.data), 0, len(keep)
+            if n != N:
+                raise JerkError(JERK_EINVAL, "a time series request needs N samples")
+            numbins = N // 2
+        else:
+            ptr, dev, keep = _spectrum_arg(spectrum)
+            numbins = int(spectrum.shape[0]) if dev else len(keep)
         if tag is None:
             tag = self._next
         self._next = max(self._next, tag) + 1
         self._keep[tag] = keep
         req = Request(ptr, dev, numbins, N, dt, zmax, wmax, int(wmax_given), numharm, sigma,
-                      flo, fhi, tag)
+                      flo, fhi, tag, int(timeseries))
         _check(lib().jerk_server_submit(self._s, C.byref(req)))
         return tag
 

@@ -157,3 +157,53 @@ def test_poisson_stream_of_dedispersion_trials_peaks_at_the_pulsar_trial():
     assert sorted(best) == list(range(ntrials))
     assert max(best, key=best.get) == peak
     assert best[peak] > best[0] and best[peak] > best[ntrials - 1]
+
+
+def test_time_series_requests_equal_their_spectra():
+    """Dedispersed trials go straight into the served loop: a request that
+    carries the N float32 samples (from host memory or a CUDA tensor) gives
+    exactly the candidates of the spectrum the same series makes on the GPU
+    (jerk_spectrum_from_timeseries: realfft, deredden, bin 0 -- the
+    reference's .dat preparation), in a mix with ordinary spectrum requests;
+    the series buffers are reused between requests."""
+    torch = pytest.importorskip("torch")
+    build.build()
+    N, dt = 1 << 20, 64e-6
+    series = []
+    for seed in (31, 32):
+        rng = np.random.default_rng(seed)
+        ps = synth.random_pulsars(rng, 2, zmax=16.0, wmax=48.0, fmax=200.0)
+        ts = synth.timeseries(N, dt, ps, seed)
+        ts = ts + (0.02 * np.cumsum(rng.standard_normal(N))).astype(np.float32)
+        series.append(np.ascontiguousarray(ts, dtype=np.float32))
+    prepared = []
+    for ts in series:
+        spec = jerk.spectrum_from_timeseries(torch.from_numpy(ts).cuda())
+        torch.cuda.synchronize()
+        prepared.append(spec)
+    params = (N, dt, 20, 60, 8, 2.0)
+    srv = jerk.JerkServer(max_active=3, batch=16)
+    dev_series = torch.from_numpy(series[1]).cuda()
+    srv.submit(series[0], *params, tag=0, timeseries=True)
+    srv.submit(prepared[0], *params, tag=1)
+    srv.submit(dev_series, *params, tag=2, timeseries=True)
+    srv.submit(prepared[1], *params, tag=3)
+    srv.submit(series[1], *params, tag=4, timeseries=True)  # reuses a pooled buffer
+    got = {}
+    while len(got) < 5:
+        r = srv.poll(60000)
+        assert r is not None, "server stalled"
+        got[r[0]] = r[1]
+    st = srv.stats()
+    srv.close()
+    assert st["failed"] == 0
+    assert len(got[1]) > 0 and len(got[3]) > 0
+    assert np.array_equal(got[0], got[1])
+    assert np.array_equal(got[2], got[3]) and np.array_equal(got[4], got[3])
+    with pytest.raises(jerk.JerkError):  # not a supported series length
+        s2 = jerk.JerkServer(max_active=1)
+        try:
+            s2.submit(np.zeros(3 << 16, np.float32), 3 << 16, dt, 20, 60, 8, 2.0,
+                      timeseries=True)
+        finally:
+            s2.close()
