@@ -268,6 +268,18 @@ int jerk_realfft(const float *timeseries, long long n, void *spectrum, void *scr
 long long jerk_deredden_scratch_bytes(long long numamps);
 int jerk_deredden(void *spectrum, long long numamps, void *scratch, long long scratch_bytes,
                   void *stream);
+/* Birdie zapping of the spectrum made from a time series, replacing the
+ * loop of src/accelsearch_lib.c:393-418 over zapbirds (src/zapping.c:29-81,
+ * from memory): for each birdie [lobins[i], hibins[i]] in Fourier bins, in
+ * list order (stopping at the first at or above N/2, high edges clamped to
+ * N/2 - 1), the bins [floor(lo), ceil(hi)) take the amplitude
+ * sqrt(0.5 (median power of the 200 bins from lo - 300 + median power of the
+ * 200 bins from hi - 100) / ln 2) with phase 0; birdies below 301 bins are
+ * left alone.  Bit-exact with the reference.  spectrum: numbins complex64 on
+ * the device; lobins/hibins: host arrays (the reference's get_birdies
+ * output).  Asynchronous on stream; allocates nothing. */
+int jerk_zap_birdies(void *spectrum, long long numbins, long long N, const double *lobins,
+                     const double *hibins, int nbirds, void *stream);
 long long jerk_spectrum_scratch_bytes(long long n);
 int jerk_spectrum_from_timeseries(const float *timeseries, long long n, void *spectrum,
                                   void *scratch, long long scratch_bytes, void *stream);

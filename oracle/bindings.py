@@ -351,6 +351,39 @@ def deredden(spectrum: np.ndarray, reference: bool = False) -> np.ndarray:
     return a
 
 
+def zap_list(spectrum: np.ndarray, N: int, lobins, hibins) -> np.ndarray:
+    """The oracle's birdie zapping (zapbirds over a birdie list, as the
+    reference's CPU1 applies it) on a copy of a complex64 spectrum."""
+    f = _orc().orc_zap_list
+    f.restype = None
+    f.argtypes = [C.c_void_p, C.c_long, C.c_longlong, C.c_void_p, C.c_void_p, C.c_int]
+    a = np.array(spectrum, dtype=np.complex64)
+    lo = np.ascontiguousarray(lobins, dtype=np.float64)
+    hi = np.ascontiguousarray(hibins, dtype=np.float64)
+    f(a.ctypes.data, len(a), N, lo.ctypes.data, hi.ctypes.data, len(lo))
+    return a
+
+
+def zapbirds(spectrum: np.ndarray, lobin: float, hibin: float, reference: bool = False):
+    """One zapbirds (src/zapping.c:29-81) on a copy of a spectrum, by the
+    oracle or by the reference build (which reads up to 100 bins past the end:
+    the copy is zero-padded there, as the reference's .dat buffer is)."""
+    n = len(spectrum)
+    pad = np.zeros(n + 2000, dtype=np.complex64)
+    pad[1000:1000 + n] = spectrum
+    if reference:
+        f = _ref().zapbirds
+        f.restype = None
+        f.argtypes = [C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+        f(lobin, hibin, None, pad[1000:].ctypes.data)
+    else:
+        f = _orc().orc_zapbirds
+        f.restype = None
+        f.argtypes = [C.c_void_p, C.c_long, C.c_double, C.c_double]
+        f(pad[1000:].ctypes.data, n, lobin, hibin)
+    return pad[1000:1000 + n].copy()
+
+
 def ref_realfft(series: np.ndarray) -> np.ndarray:
     """The reference's forward realfft (src/fastffts.c:163-235, isign -1) on a
     copy of a float32 series, as built here (its complex FFT is the FFTW

@@ -906,3 +906,58 @@ void orc_deredden(float *fft, int numamps)
     free(pw);
     free(tmp);
 }
+
+/* ------------------------------------------------------------------ */
+/* Birdie zapping of a spectrum held in memory                          */
+
+#define ZAP_MEDIANBINS 200 /* MEDIANBINS, src/zapping.c:3 */
+
+/* Median power (rank (n-1)/2) of n bins from fft + first; bins at or past
+ * numamps read as zeros (the reference's .dat buffer is zero-padded there,
+ * ACCEL_PADDING, include/accel.h:35). */
+static float zap_median(const float *fft, long numamps, long first, int n)
+{
+    float *p = malloc(sizeof(float) * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        const long b = first + i;
+        const float r = (b >= 0 && b < numamps) ? fft[2 * b] : 0.0f;
+        const float im = (b >= 0 && b < numamps) ? fft[2 * b + 1] : 0.0f;
+        p[i] = r * r + im * im;
+    }
+    const float m = median_of(p, n);
+    free(p);
+    return m;
+}
+
+/* zapbirds from memory (src/zapping.c:29-81): when the birdie starts above
+ * 1.5 MEDIANBINS + 1, the bins [floor(lobin), ceil(hibin)) take the amplitude
+ * sqrt(mean of the median powers below and above it / ln 2), phase 0. */
+void orc_zapbirds(float *fft, long numamps, double lobin, double hibin)
+{
+    const long ilobin = (long)floor(lobin), ihibin = (long)ceil(hibin);
+    if (!(lobin - 1.5 * ZAP_MEDIANBINS > 1))
+        return;
+    const float mlo = zap_median(fft, numamps, (long)(lobin - 3 * ZAP_MEDIANBINS / 2),
+                                 ZAP_MEDIANBINS);
+    const float mhi = zap_median(fft, numamps, (long)(hibin - ZAP_MEDIANBINS / 2),
+                                 ZAP_MEDIANBINS);
+    const float avgamp = (float)sqrt(0.5 * (mlo + mhi) / -log(0.5));
+    for (long b = ilobin; b < ihibin; b++) {
+        fft[2 * b] = avgamp;
+        fft[2 * b + 1] = 0.0f;
+    }
+}
+
+/* The caller's loop (src/accelsearch_lib.c:393-418): birdies in list order,
+ * stopping at the first one at or above N/2 bins, high edges clamped to
+ * N/2 - 1. */
+void orc_zap_list(float *fft, long numamps, long long N, const double *lobins,
+                  const double *hibins, int nbirds)
+{
+    const double top = (double)(N / 2);
+    for (int i = 0; i < nbirds; i++) {
+        if (lobins[i] >= top)
+            break;
+        orc_zapbirds(fft, numamps, lobins[i], hibins[i] >= top ? top - 1 : hibins[i]);
+    }
+}

@@ -498,6 +498,56 @@ size_t dr_scratch(int numamps)
     return align256(sizeof(float) * (size_t)(numamps / kDrInit + 2));
 }
 
+// ---------------------------------------------------------------------------
+// birdie zapping (zapbirds from memory, src/zapping.c:29-81)
+
+constexpr int kZapBins = 200;  // MEDIANBINS (src/zapping.c:3)
+constexpr int kZapThreads = 256;
+
+// One birdie.  The median powers (rank 99 of 200) of the bins
+// [lobin - 300, lobin - 100) and [hibin - 100, hibin + 100), read before any
+// bin is written (bins at or past numamps read as zeros, as the reference's
+// zero-padded buffer gives them), set avgamp = sqrt(0.5 (mlo + mhi) / ln 2);
+// bins [floor(lobin), ceil(hibin)) become (avgamp, 0).
+__global__ void __launch_bounds__(kZapThreads)
+    zap_kernel(float2 *__restrict__ x, long long numamps, double lobin, double hibin,
+               double neg_log_half)
+{
+    __shared__ float p[2][kZapBins];
+    __shared__ float med[2];
+    const int tid = threadIdx.x;
+    const long long first[2] = {(long long)(lobin - 3 * kZapBins / 2),
+                                (long long)(hibin - kZapBins / 2)};
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+        for (int i = tid; i < kZapBins; i += kZapThreads) {
+            const long long b = first[w] + i;
+            const float2 v = (b >= 0 && b < numamps) ? x[b] : make_float2(0.f, 0.f);
+            p[w][i] = dr_power(v);
+        }
+    __syncthreads();
+    constexpr int k = (kZapBins - 1) / 2;
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+        for (int i = tid; i < kZapBins; i += kZapThreads) {
+            const float v = p[w][i];
+            int pos = 0;
+            for (int j = 0; j < kZapBins; j++) {
+                const float u = p[w][j];
+                pos += (u < v) | ((u == v) & (j < i));
+            }
+            if (pos == k)
+                med[w] = v;
+        }
+    __syncthreads();
+    const float avgamp =
+        (float)__dsqrt_rn(__ddiv_rn(0.5 * (double)__fadd_rn(med[0], med[1]), neg_log_half));
+    const long long lo = (long long)floor(lobin), hi = (long long)ceil(hibin);
+    for (long long b = lo + tid; b < hi; b += kZapThreads)
+        if (b >= 0 && b < numamps)
+            x[b] = make_float2(avgamp, 0.f);
+}
+
 }  // namespace
 }  // namespace jerk
 
@@ -611,4 +661,32 @@ extern "C" int jerk_spectrum_from_timeseries(const float *timeseries, long long 
     // create_accelobs then sets bin 0 of a .dat input to (1, 1) when the
     // powers are not photon-normalised (src/accel_utils.c:1829-1834)
     return deredden_impl(spectrum, n / 2, scratch, scratch_bytes, stream, 1.0f);
+}
+
+// The caller's loop around zapbirds (src/accelsearch_lib.c:393-418): birdies
+// in list order, stopping at the first one at or above N/2, high edges
+// clamped to N/2 - 1; birdies at or below 1.5 * 200 + 1 bins are left alone.
+extern "C" int jerk_zap_birdies(void *spectrum, long long numbins, long long N,
+                                const double *lobins, const double *hibins, int nbirds,
+                                void *stream)
+{
+    if (!spectrum || numbins < 1 || N < 2 || nbirds < 0 || (nbirds && (!lobins || !hibins)))
+        return set_error(JERK_EINVAL, "jerk_zap_birdies: bad argument");
+    if ((uintptr_t)spectrum & 7)
+        return set_error(JERK_EINVAL, "jerk_zap_birdies: misaligned spectrum");
+    cudaStream_t st = (cudaStream_t)stream;
+    const double top = (double)(N / 2);
+    const double neg_log_half = -std::log(0.5);
+    for (int i = 0; i < nbirds; i++) {
+        if (lobins[i] >= top)
+            break;
+        const double lo = lobins[i], hi = hibins[i] >= top ? top - 1 : hibins[i];
+        if (!(lo - 1.5 * kZapBins > 1))
+            continue;
+        zap_kernel<<<1, kZapThreads, 0, st>>>((float2 *)spectrum, numbins, lo, hi, neg_log_half);
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return set_error(JERK_ECUDA, cudaGetErrorString(e));
+    return JERK_OK;
 }

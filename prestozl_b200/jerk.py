@@ -112,7 +112,7 @@ EXPORTS = [
     "jerk_server_destroy", "jerk_realfft_scratch_bytes", "jerk_realfft",
     "jerk_deredden_scratch_bytes", "jerk_deredden", "jerk_spectrum_scratch_bytes",
     "jerk_spectrum_from_timeseries", "jerk_polisher_create", "jerk_polisher_destroy",
-    "jerk_polish_rzw",
+    "jerk_polish_rzw", "jerk_zap_birdies",
 ]
 
 
@@ -188,6 +188,8 @@ def lib() -> C.CDLL:
         getattr(L, f).argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
                                   C.c_void_p]
     L.jerk_deredden.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
+    L.jerk_zap_birdies.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p,
+                                   C.c_void_p, C.c_int, C.c_void_p]
     L.jerk_polisher_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p]
     L.jerk_polisher_destroy.argtypes = [C.c_void_p]
     L.jerk_polisher_destroy.restype = None
@@ -385,6 +387,23 @@ class Polisher:
             self.close()
         except Exception:
             pass
+
+
+def zap_birdies(spec, N: int, lobins, hibins):
+    """The reference's birdie zapping of an in-memory spectrum
+    (src/accelsearch_lib.c:393-418, zapbirds src/zapping.c:29-81), in place on
+    a complex64 CUDA tensor; lobins/hibins in Fourier bins, in list order.
+    Bit-exact with the reference."""
+    import torch
+
+    if not (getattr(spec, "is_cuda", False) and spec.is_contiguous()):
+        raise JerkError(JERK_EINVAL, "zap_birdies: expects a contiguous CUDA tensor")
+    lo = np.ascontiguousarray(lobins, dtype=np.float64)
+    hi = np.ascontiguousarray(hibins, dtype=np.float64)
+    stream = torch.cuda.current_stream(spec.device).cuda_stream
+    _check(lib().jerk_zap_birdies(spec.data_ptr(), spec.numel(), N, lo.ctypes.data,
+                                  hi.ctypes.data, len(lo), stream or None))
+    return spec
 
 
 def _spectrum_arg(spectrum):

@@ -169,3 +169,24 @@ def test_search_from_dat_file_matches_reference(tmp_path):
     probs = H.compare_cands(got, want, list(obs.powcut))
     assert not probs, probs[:10]
     print(f".dat search: {len(got)} candidates (reference {len(want)})")
+
+
+def test_zap_birdies_bit_exact():
+    """Birdie zapping on the GPU equals the oracle's zapbirds loop bitwise on
+    a spectrum made on the GPU from a 2^20-sample series: ordinary and
+    overlapping birdies, one clamped at the top, one below 301 bins (left
+    alone), one at N/2 (stops the list) and one after it (not zapped)."""
+    N = 1 << 20
+    x = red_series(N, 77)
+    spec = jerk.spectrum_from_timeseries(torch.from_numpy(x).cuda())
+    torch.cuda.synchronize()
+    before = spec.cpu().numpy()
+    lob = [1000.3, 1030.0, 250.0, 88888.25, 200000.0, N / 2 - 20.5, N / 2, 300000.0]
+    hib = [1040.7, 1060.2, 260.0, 88890.0, 200000.0, N / 2 + 30.0, N / 2 + 5, 300010.0]
+    jerk.zap_birdies(spec, N, lob, hib)
+    got = spec.cpu().numpy()
+    want = ob.zap_list(before, N, lob, hib)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert got[1020] == got[1000] and got[1020].imag == 0  # zapped
+    assert got[300005] == before[300005]  # after the stop
+    assert got[255] == before[255]  # below the threshold

@@ -255,3 +255,21 @@ def test_dat_input_is_realfft_then_deredden_then_bin0(tmp_path):
         want = ob.deredden(raw, reference=reference)
         want[0] = 1.0 + 1.0j
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), reference
+
+
+def test_zapbirds_restatement_matches_reference():
+    """The oracle's zapbirds (src/zapping.c:29-81, from memory) is bit-exact
+    with the reference build's: random spectra and birdies, including
+    birdies below the 301-bin threshold and median windows reaching past the
+    spectrum's end (zero padding, as the reference's .dat buffer has)."""
+    if not ob.have_reference():
+        pytest.skip("reference build absent")
+    rng = np.random.default_rng(1)
+    for t in range(200):
+        n = int(rng.integers(2000, 100000))
+        spec = ((rng.standard_normal(n) + 1j * rng.standard_normal(n)) *
+                rng.uniform(0.5, 30)).astype(np.complex64)
+        lo = float(rng.uniform(250, n - 2)) if t % 5 else float(rng.uniform(0, 400))
+        hi = min(lo + float(rng.uniform(0, 50)), n - 1)
+        a, b = ob.zapbirds(spec, lo, hi), ob.zapbirds(spec, lo, hi, reference=True)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (n, lo, hi)
