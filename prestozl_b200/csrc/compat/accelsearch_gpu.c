@@ -34,6 +34,7 @@
 
 #include "accel.h"
 #include "jerk.h"
+#include "jerk_compat.h"
 
 static int gather_kernels(const subharminfo *s, float **out)
 {
@@ -57,7 +58,8 @@ int accelsearch_GPU(accelobs obs, subharminfo **subharminfs, GSList **cands_ptr,
     jerk_plan *plan = NULL;
     jerk_cand *cands = NULL;
     long long ncands = 0;
-    int nsubs, rc = 0, idx = 0;
+    int nsubs, rc = 0, idx = 0, gpu_bank = 0;
+    void *bank = NULL;
     GSList *list = NULL;
 
     *cands_ptr = NULL;
@@ -66,23 +68,7 @@ int accelsearch_GPU(accelobs obs, subharminfo **subharminfs, GSList **cands_ptr,
         rc = -1;
         goto done;
     }
-    memset(&o, 0, sizeof(o));
-    o.numbins = obs.numbins;
-    o.lobin = obs.lobin;
-    o.highestbin = obs.highestbin;
-    o.rlo = obs.rlo;
-    o.zlo = obs.zlo;
-    o.wlo = obs.wlo;
-    o.corr_uselen = obs.corr_uselen;
-    o.numz = obs.numz;
-    o.numw = obs.numw;
-    o.numharmstages = obs.numharmstages;
-    o.norm_type = obs.norm_type;
-    o.nph = obs.nph;
-    for (int ii = 0; ii < obs.numharmstages && ii < JERK_MAX_STAGES; ii++) {
-        o.powcut[ii] = obs.powcut[ii];
-        o.numindep[ii] = obs.numindep[ii];
-    }
+    jerk_obs_of_accelobs(&obs, &o);
 
     nsubs = jerk_subharm_count(obs.numharmstages);
     subs = (jerk_subharm *)calloc(nsubs, sizeof(jerk_subharm));
@@ -106,6 +92,10 @@ int accelsearch_GPU(accelobs obs, subharminfo **subharminfs, GSList **cands_ptr,
             d->numw = s->numkern_wdim;
             d->fftlen = s->kern[0][0].fftlen;
             d->halfwidth = s->kern[0][0].kern_half_width;
+            if (!s->kern[0][0].data) {
+                gpu_bank = 1;  /* the drop-in's create_subharminfos left the kernels out */
+                continue;
+            }
             if (gather_kernels(s, &kbufs[idx]) != 0) {
                 rc = -1;
                 goto done;
@@ -118,6 +108,20 @@ int accelsearch_GPU(accelobs obs, subharminfo **subharminfs, GSList **cands_ptr,
         jerk_config cfg;
         memset(&cfg, 0, sizeof(cfg));
         cfg.batch_rsteps = cmd && cmd->batchsize > 0 ? cmd->batchsize : 8;
+        if (gpu_bank) {
+            /* the kernel bank made on the GPU (src/accel_utils.c:151-282 restated
+               in jerk_bank.cu) instead of uploaded from the host */
+            for (int i = 0; i < nsubs; i++)
+                subs[i].kernels = NULL;
+            rc = jerk_device_alloc(8 * jerk_bank_elements(subs, nsubs), &bank);
+            if (rc == JERK_OK)
+                rc = jerk_bank_generate(subs, nsubs, bank, NULL);
+            if (rc != JERK_OK) {
+                fprintf(stderr, "accelsearch_GPU: %s\n", jerk_last_error());
+                goto done;
+            }
+            cfg.device_bank = bank;
+        }
         rc = jerk_plan_create(&plan, &o, subs, nsubs, &cfg);
         if (rc != JERK_OK) {
             fprintf(stderr, "accelsearch_GPU: %s\n", jerk_last_error());
@@ -150,6 +154,8 @@ int accelsearch_GPU(accelobs obs, subharminfo **subharminfs, GSList **cands_ptr,
 done:
     if (plan)
         jerk_plan_destroy(plan);
+    if (bank)
+        jerk_device_free(bank);
     jerk_free(cands);
     if (kbufs)
         for (int i = 0; i < nsubs; i++)
