@@ -491,6 +491,9 @@ __global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
 {
     constexpr int kHarmZ = ZU;
     static_assert(ZU == 4 || ZU == 8, "whole int4s of z offsets");
+    // the crossing mask hm holds one bit per (stage, row): with more than 32
+    // the shifts would be undefined and the compiler may drop whole stages
+    static_assert(S * ZU <= 32, "hit mask wider than 32 bits");
     constexpr int NS = 1 << (S - 1);
     extern __shared__ int hsm[];
     __shared__ unsigned int s_base[NS];
