@@ -24,6 +24,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 REF_LIB = os.path.join(REF_DIR, "libprestoref.so")
 REF_CLI = os.path.join(REF_DIR, "accelsearch")
 DROPIN_CLI = os.path.join(REF_DIR, "accelsearch_b200")
+DROPIN_MANY_CLI = os.path.join(REF_DIR, "accelsearch_b200_many")
 REFGPU_CLI = os.path.join(REF_DIR, "accelsearch_refgpu")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REFERENCE_SOURCES = "/root/reference"

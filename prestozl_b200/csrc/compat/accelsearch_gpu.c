@@ -36,6 +36,55 @@
 #include "jerk.h"
 #include "jerk_compat.h"
 
+/* The last GPU-generated kernel bank and the geometry it was made for.  A
+ * process that searches many spectra of one geometry -- the reference's
+ * worker pool (bin/accelsearch_pipeline_cu.py) calls accelsearch_GPU once per
+ * .fft file -- generates it once; it stays on the device until the geometry
+ * changes or the process exits. */
+static void *g_bank;
+static jerk_subharm *g_bank_subs;
+static int g_bank_nsubs;
+
+static int same_geometry(const jerk_subharm *a, const jerk_subharm *b, int n)
+{
+    for (int i = 0; i < n; i++)
+        if (a[i].numharm != b[i].numharm || a[i].harmnum != b[i].harmnum ||
+            a[i].zmax != b[i].zmax || a[i].wmax != b[i].wmax || a[i].numz != b[i].numz ||
+            a[i].numw != b[i].numw || a[i].fftlen != b[i].fftlen ||
+            a[i].halfwidth != b[i].halfwidth)
+            return 0;
+    return 1;
+}
+
+static int resident_bank(const jerk_subharm *subs, int nsubs, void **bank)
+{
+    if (g_bank && g_bank_nsubs == nsubs && same_geometry(g_bank_subs, subs, nsubs)) {
+        *bank = g_bank;
+        return JERK_OK;
+    }
+    if (g_bank) {
+        jerk_device_free(g_bank);
+        free(g_bank_subs);
+        g_bank = NULL;
+        g_bank_subs = NULL;
+    }
+    void *b = NULL;
+    int rc = jerk_device_alloc(8 * jerk_bank_elements(subs, nsubs), &b);
+    if (rc == JERK_OK)
+        rc = jerk_bank_generate(subs, nsubs, b, NULL);
+    if (rc != JERK_OK) {
+        if (b)
+            jerk_device_free(b);
+        return rc;
+    }
+    g_bank_subs = (jerk_subharm *)malloc(sizeof(jerk_subharm) * nsubs);
+    memcpy(g_bank_subs, subs, sizeof(jerk_subharm) * nsubs);
+    g_bank_nsubs = nsubs;
+    g_bank = b;
+    *bank = b;
+    return JERK_OK;
+}
+
 static int gather_kernels(const subharminfo *s, float **out)
 {
     const int fftlen = s->kern[0][0].fftlen;
@@ -110,12 +159,11 @@ int accelsearch_GPU(accelobs obs, subharminfo **subharminfs, GSList **cands_ptr,
         cfg.batch_rsteps = cmd && cmd->batchsize > 0 ? cmd->batchsize : 8;
         if (gpu_bank) {
             /* the kernel bank made on the GPU (src/accel_utils.c:151-282 restated
-               in jerk_bank.cu) instead of uploaded from the host */
+               in jerk_bank.cu) instead of uploaded from the host, kept for the
+               next call of the same geometry */
             for (int i = 0; i < nsubs; i++)
                 subs[i].kernels = NULL;
-            rc = jerk_device_alloc(8 * jerk_bank_elements(subs, nsubs), &bank);
-            if (rc == JERK_OK)
-                rc = jerk_bank_generate(subs, nsubs, bank, NULL);
+            rc = resident_bank(subs, nsubs, &bank);
             if (rc != JERK_OK) {
                 fprintf(stderr, "accelsearch_GPU: %s\n", jerk_last_error());
                 goto done;
@@ -154,8 +202,6 @@ int accelsearch_GPU(accelobs obs, subharminfo **subharminfs, GSList **cands_ptr,
 done:
     if (plan)
         jerk_plan_destroy(plan);
-    if (bank)
-        jerk_device_free(bank);
     jerk_free(cands);
     if (kbufs)
         for (int i = 0; i < nsubs; i++)

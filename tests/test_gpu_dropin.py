@@ -57,3 +57,47 @@ def test_dropin_accel_matches_reference(tmp_path):
             assert abs(float(a) - float(b)) <= 0.011, (g, w)
         if len(g) > 12 and g[1].isdigit():
             fund = False  # second table rows start "cand harm"
+
+
+def test_dropin_many_spectra_in_one_process(tmp_path):
+    """A pool worker searches many spectra in one process
+    (bin/accelsearch_pipeline_cu.py): the drop-in keeps its GPU kernel bank
+    between calls of one geometry.  Three spectra searched in one process
+    write the ACCEL files that three separate runs write."""
+    import numpy as np
+
+    build.build()
+    if not (os.path.exists(ob.DROPIN_CLI) and os.path.exists(ob.DROPIN_MANY_CLI)):
+        pytest.skip("drop-in binaries not built (reference sources absent at build time)")
+    args = H.golden("small_cands.json")["args"]
+    N, dt = 1 << 20, 64e-6
+    names = []
+    many = tmp_path / "many"
+    many.mkdir()
+    for i, seed in enumerate((20241203, 5, 6)):
+        if i == 0:
+            spec, N, dt = synth.small_spectrum()
+        else:
+            rng = np.random.default_rng(seed)
+            ps = synth.random_pulsars(rng, 2, zmax=16.0, wmax=48.0, fmax=200.0)
+            spec = synth.presto_fft(synth.timeseries(N, dt, ps, seed))
+        name = f"s{i}"
+        names.append(name)
+        one = tmp_path / name
+        one.mkdir()
+        for d in (one, many):
+            synth.write_fft(str(d / name), spec, N, dt)
+        env = dict(os.environ, PRESTO=str(one), OMP_NUM_THREADS="1")
+        out = subprocess.run([ob.DROPIN_CLI, *args, name + ".fft"], cwd=one, env=env,
+                             capture_output=True, text=True, timeout=600)
+        assert out.returncode == 0, out.stderr[-2000:]
+    env = dict(os.environ, PRESTO=str(many), OMP_NUM_THREADS="1")
+    out = subprocess.run([ob.DROPIN_MANY_CLI, *args, "--", *[n + ".fft" for n in names]],
+                         cwd=many, env=env, capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0, out.stderr[-2000:]
+    print(out.stderr.strip())
+    for n in names:
+        a = (tmp_path / n / f"{n}_ACCEL_20_JERK_60").read_text()
+        b = (many / f"{n}_ACCEL_20_JERK_60").read_text()
+        assert a == b, n
+    assert len(accel_rows((many / "s0_ACCEL_20_JERK_60").read_text())) > 0
