@@ -503,31 +503,26 @@ def main():
         graph_info = {"value": world * args.steps / g_s * 3600.0,
                       "ms_per_spectrum": statistics.mean(g_ms)}
 
-    # ---- plain drop-in: what accelsearch_GPU does per spectrum -- upload the
-    # host kernel bank, allocate a plan (-batchsize 8), copy the host spectrum,
-    # search, build the list, free everything
+    # ---- plain drop-in: what accelsearch_GPU does per spectrum -- allocate a
+    # plan (-batchsize 8, the reference's default) over the kernel bank it keeps
+    # resident between calls of one geometry, copy the host spectrum, search,
+    # build the list, free the plan
     dropin = None
     if served:
-        host_subs = []
-        for i, sb in enumerate(subs):
-            d = dict(sb)
-            d["kern"] = bank.rows(subs, i, range(sb["numw"] * sb["numz"])).reshape(
-                sb["numw"], sb["numz"], sb["fftlen"])
-            host_subs.append(d)
         hspec = [specs[i % nspec].cpu().numpy() for i in range(2)]
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for hs in hspec:
-            p1 = jerk.JerkPlan(obs, host_subs, batch=8)
+            p1 = jerk.JerkPlan(obs, subs, batch=8, device_bank=bank.ptr.value)
             p1.search(hs)
             p1.close()
         e1.record()
         torch.cuda.synchronize()
         dropin_s = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0, dist, "cuda")
         dropin = {"value": world * len(hspec) / dropin_s * 3600.0,
-                  "ms_per_spectrum": dropin_s * 1000.0 / len(hspec), "batch_rsteps": 8}
-        del host_subs
+                  "ms_per_spectrum": dropin_s * 1000.0 / len(hspec), "batch_rsteps": 8,
+                  "bank": "resident on the device, as the drop-in keeps it"}
 
     # ---- served: the request loop, every spectrum of the job submitted at once
     served_info = None
