@@ -227,3 +227,55 @@ def test_few_harmonics_match_reference(numharm, tmp_path):
     assert len(want) > 0
     probs = H.compare_cands(got, want, list(prob.obs.powcut))
     assert not probs, probs[:10]
+
+
+def test_photon_normalisation_matches_reference(tmp_path):
+    """-photon (powers over the photon count, the DC bin of the .fft,
+    src/accel_utils.c:1798-1808): Poisson counts of mean 4 whose rate
+    carries the small spectrum's pulsar; volumes against the FP64 oracle and
+    the whole search against the reference CPU search run with -photon.
+
+    The DC bin of photon counts (normalised power about 4e6 here) lies inside
+    rstep 0, whose volumes then carry FP32 rounding in proportion to that
+    peak, as the reference's FP32 FFTs do: there the bound is
+    1e-5 max(oracle, 1) + 1e-6 (the volume's peak); elsewhere the usual
+    per-cell 1e-5."""
+    build.build()
+    H.ensure_oracle()
+    if not H.have_ref():
+        pytest.skip("the reference build (oracle/_ref) provides the kernel bank")
+    from prestozl_b200 import synth
+
+    N, dt, seed = 1 << 20, 64e-6, 99
+    pulsar = synth.timeseries(N, dt, synth.small_pulsar(), seed) - synth.timeseries(N, dt, [],
+                                                                                    seed)
+    rate = np.maximum(4.0 + 2.0 * pulsar.astype(np.float64), 0.0)
+    counts = np.random.default_rng(seed).poisson(rate).astype(np.float32)
+    spec = synth.presto_fft(counts)
+    args = list(H.golden("small_cands.json")["args"]) + ["-photon"]
+    prob = H.Problem(str(tmp_path), spec, N, dt, args)
+    assert prob.obs.nph > 0
+    obs = jerk.obs_from_refobs(prob.obs)
+    assert obs.nph == prob.obs.nph
+    p = jerk.JerkPlan(obs, prob.subs, batch=8)
+    worst = 0.0
+    for k in (0, prob.rstep_of(8281.0), p.num_rsteps - 1):
+        startr = prob.startr(k)
+        for i in range(len(prob.subs)):
+            got, rlo = p.volume(prob.spec, k, i)
+            h, want, _, _ = prob.oracle.fderivs(i, startr, startr + prob.rstep - 0.5)
+            diff = np.abs(got.astype(np.float64) - want)
+            floor = 1e-6 * float(want.max()) if k == 0 else 0.0
+            bound = POW_TOL * np.maximum(want, 1.0) + floor
+            assert np.all(diff <= bound), (k, i, float((diff / bound).max()))
+            if k:
+                worst = max(worst, float((diff / np.maximum(want, 1.0)).max()))
+    got = p.search(prob.spec)
+    p.close()
+    prob.ref.make_bank()
+    want, _ = prob.ref.search()
+    probs = H.compare_cands(got, want, list(prob.obs.powcut))
+    assert not probs, probs[:10]
+    assert len(want) > 0
+    print(f"-photon: nph {prob.obs.nph:.0f}, max FP32 power error vs FP64 oracle past rstep 0 "
+          f"{worst:.3e}, {len(want)} candidates")
