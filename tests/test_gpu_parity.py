@@ -279,3 +279,30 @@ def test_photon_normalisation_matches_reference(tmp_path):
     assert len(want) > 0
     print(f"-photon: nph {prob.obs.nph:.0f}, max FP32 power error vs FP64 oracle past rstep 0 "
           f"{worst:.3e}, {len(want)} candidates")
+
+
+def test_frequency_band_matches_reference(tmp_path):
+    """-flo 10 -fhi 400 on the small spectrum: the band limits set the first
+    and last rsteps and the number of independent trials (and so the power
+    cutoffs, src/accel_utils.c:1906-1984); the candidate list equals the
+    reference CPU search's with the same flags."""
+    build.build()
+    H.ensure_oracle()
+    if not H.have_ref():
+        pytest.skip("the reference build (oracle/_ref) provides the kernel bank")
+    from prestozl_b200 import synth
+
+    spec, N, dt = synth.small_spectrum()
+    args = list(H.golden("small_cands.json")["args"]) + ["-flo", "10", "-fhi", "400"]
+    prob = H.Problem(str(tmp_path), spec, N, dt, args)
+    obs = jerk.obs_from_refobs(prob.obs)
+    assert prob.obs.rlo > 600 and prob.obs.highestbin < 30000
+    p = jerk.JerkPlan(obs, prob.subs, batch=8)
+    got = p.search(prob.spec)
+    p.close()
+    prob.ref.make_bank()
+    want, _ = prob.ref.search()
+    assert len(want) > 0
+    probs = H.compare_cands(got, want, list(prob.obs.powcut))
+    assert not probs, probs[:10]
+    assert got["r"].min() >= prob.obs.rlo and got["r"].max() <= prob.obs.highestbin
