@@ -246,7 +246,10 @@ int jerk_polish_rzw(jerk_polisher *polisher, const void *spectrum, long long num
  * jerk_realfft replaces realfft(idata, n, -1) (src/fastffts.c:163-235): the
  * forward real FFT of n float samples, unnormalised, packed as the reference
  * packs it -- n/2 complex64 values, value 0 = (DC, Nyquist), value k = bin k.
- * n must be a power of two from 2^15 to 2^27 (JERK_EUNSUPPORTED otherwise).
+ * n must be 2 R1 R2 with R1, R2 in {128, 192, 256, 384, 512, 768, 1024, 1280,
+ * 2048, 4096, 5120, 7680, 8192, 10240} -- powers of two from 2^15 to 2^27
+ * and lengths with factors 3 and 5 such as 3 * 2^20 or 15 * 2^20
+ * (JERK_EUNSUPPORTED otherwise; jerk_realfft_scratch_bytes returns 0).
  * FP32 like the reference's, so results agree to FP32 rounding.
  *
  * jerk_deredden replaces deredden(fft, numamps) (src/accel_utils.c:1557-1633)
@@ -320,7 +323,7 @@ typedef struct jerk_request {
                                     series (a dedispersed trial), and the server makes the
                                     spectrum on the GPU as the reference does for a .dat
                                     input (jerk_spectrum_from_timeseries); numbins is taken
-                                    as N / 2.  N: a power of two from 2^15 to 2^27 */
+                                    as N / 2.  N: a length jerk_realfft takes */
 } jerk_request;
 
 typedef struct jerk_result {

@@ -5,8 +5,9 @@
 //
 // Real FFT of n = 2M samples.  The samples are read as M complex values
 // z[m] = x[2m] + i x[2m+1]; their M-point FFT Z is taken in four steps with
-// M = R1 * R2 (both powers of two, 128..8192), each step one block-wide FFT
-// per CTA from jerk_fft.cuh:
+// M = R1 * R2 (R1, R2 block-FFT sizes from 128 to 10240: powers of two and
+// products with 3 and 5), each step one block-wide FFT per CTA from
+// jerk_fft.cuh:
 //   1. columns: for each m2 < R2, the R1-point FFT over m1 of z[m2 + R2 m1],
 //      times exp(-2 pi i m2 k1 / M), stored as row k1 of an R1 x R2 scratch;
 //   2. rows: for each k1 < R1, the R2-point FFT of that row, stored to
@@ -47,7 +48,10 @@
 namespace jerk {
 namespace {
 
-constexpr int kRfMinLog = 7, kRfMaxLog = 13;  // R1, R2 in 128..8192
+// R1, R2: the block-FFT sizes from 128 to 10240 (powers of two and the mixed
+// sizes with factors 3 and 5 that jerk_fft.cuh plans)
+constexpr int kRfSizes[] = {128, 192, 256, 384, 512, 768, 1024, 1280, 2048,
+                            4096, 5120, 7680, 8192, 10240};
 
 // ---------------------------------------------------------------------------
 // real FFT kernels
@@ -100,8 +104,8 @@ __global__ void __launch_bounds__(FftPlan<R1>::T)
     const int m2 = blockIdx.x;
     const long long M = (long long)R1 * R2;
     for (int i = tid; i < kTwLo + NHI; i += T) {
-        const long long e = i < kTwLo ? ((long long)m2 * i) & (M - 1)
-                                      : ((long long)m2 * kTwLo * (i - kTwLo)) & (M - 1);
+        const long long e = i < kTwLo ? ((long long)m2 * i) % M
+                                      : ((long long)m2 * kTwLo * (i - kTwLo)) % M;
         double s, c;
         sincospi(-2.0 * (double)e / (double)M, &s, &c);
         if (i < kTwLo)
@@ -196,18 +200,25 @@ cudaError_t rf_launch_rows(const float2 *a, int R1, const float2 *tw, float2 *zo
     return cudaGetLastError();
 }
 
-// Runtime dispatch over the power-of-two sizes 128..8192.
+// Runtime dispatch over kRfSizes.
 template <template <int> class F, class... A>
 cudaError_t rf_dispatch(int R, A... args)
 {
     switch (R) {
     case 128: return F<128>::run(args...);
+    case 192: return F<192>::run(args...);
     case 256: return F<256>::run(args...);
+    case 384: return F<384>::run(args...);
     case 512: return F<512>::run(args...);
+    case 768: return F<768>::run(args...);
     case 1024: return F<1024>::run(args...);
+    case 1280: return F<1280>::run(args...);
     case 2048: return F<2048>::run(args...);
     case 4096: return F<4096>::run(args...);
+    case 5120: return F<5120>::run(args...);
+    case 7680: return F<7680>::run(args...);
     case 8192: return F<8192>::run(args...);
+    case 10240: return F<10240>::run(args...);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -227,35 +238,38 @@ template <int R> struct RfRow {
     }
 };
 
+template <int R> struct RfTwSize {
+    static cudaError_t run(int *out)
+    {
+        *out = FftPlan<R>::twsize();
+        return cudaSuccess;
+    }
+};
+
 int rf_twsize(int R)
 {
-    switch (R) {
-    case 128: return FftPlan<128>::twsize();
-    case 256: return FftPlan<256>::twsize();
-    case 512: return FftPlan<512>::twsize();
-    case 1024: return FftPlan<1024>::twsize();
-    case 2048: return FftPlan<2048>::twsize();
-    case 4096: return FftPlan<4096>::twsize();
-    case 8192: return FftPlan<8192>::twsize();
-    default: return -1;
-    }
+    int n = -1;
+    return rf_dispatch<RfTwSize>(R, &n) == cudaSuccess ? n : -1;
 }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// M = R1 * R2 for n = 2M a power of two with 2^14 <= M <= 2^26.
+// M = n / 2 = R1 * R2 with R1, R2 in kRfSizes, the most balanced pair
+// (R1 >= R2); false when n is odd or M has no such factorisation.
 bool rf_split(long long n, int *R1, int *R2)
 {
-    if (n < 2 || (n & (n - 1)))
+    if (n < 2 || (n & 1))
         return false;
-    int p = 0;
-    while ((2LL << p) < n)
-        p++;  // M = n / 2 = 2^p
-    if (p < 2 * kRfMinLog || p > 2 * kRfMaxLog)
-        return false;
-    *R1 = 1 << ((p + 1) / 2);
-    *R2 = 1 << (p / 2);
-    return true;
+    const long long M = n / 2;
+    bool found = false;
+    for (int a : kRfSizes)
+        for (int b : kRfSizes)
+            if (a >= b && (long long)a * b == M && (!found || a - b < *R1 - *R2)) {
+                *R1 = a;
+                *R2 = b;
+                found = true;
+            }
+    return found;
 }
 
 // scratch: [M float2 | R1 twiddles | R2 twiddles], each region 256-aligned
@@ -567,7 +581,8 @@ extern "C" int jerk_realfft(const float *timeseries, long long n, void *spectrum
     int R1, R2;
     if (!rf_split(n, &R1, &R2))
         return set_error(JERK_EUNSUPPORTED,
-                         "jerk_realfft: n must be a power of two from 2^15 to 2^27");
+                         "jerk_realfft: n must be 2 R1 R2 with R1, R2 in {128, 192, 256, 384, "
+                         "512, 768, 1024, 1280, 2048, 4096, 5120, 7680, 8192, 10240}");
     if (!timeseries || !spectrum || !scratch)
         return set_error(JERK_EINVAL, "jerk_realfft: null pointer");
     if (((uintptr_t)timeseries | (uintptr_t)spectrum) & 7 || (uintptr_t)scratch & 255)

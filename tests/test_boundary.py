@@ -142,15 +142,18 @@ def test_input_entry_points_size_and_reject_before_any_device_work():
     M = 1 << 24
     # the four-step scratch: M complex values plus two twiddle tables
     assert L.jerk_realfft_scratch_bytes(1 << 25) >= 8 * M
-    for bad in (0, 3, 1 << 14, (1 << 25) + 2, 1 << 28, 3 << 20):
+    for bad in (0, 3, 1 << 14, (1 << 25) + 2, 1 << 28, 7 << 20, (1 << 20) + 2):
         assert L.jerk_realfft_scratch_bytes(bad) == 0, bad
+    # lengths with factors 3 and 5: M = n / 2 = R1 R2 over the block-FFT sizes
+    for good in (3 << 20, 5 << 21, 15 << 20, 2 * 10240 * 10240):
+        assert L.jerk_realfft_scratch_bytes(good) >= 4 * good, good
     assert L.jerk_deredden_scratch_bytes(7) == 0
     assert L.jerk_deredden_scratch_bytes(8) > 0
     assert L.jerk_deredden_scratch_bytes(1 << 24) >= 4 * ((1 << 24) // 100)
     assert L.jerk_spectrum_scratch_bytes(1 << 25) == max(
         L.jerk_realfft_scratch_bytes(1 << 25), L.jerk_deredden_scratch_bytes(1 << 24))
     big = L.jerk_realfft_scratch_bytes(1 << 20)
-    assert L.jerk_realfft(4096, 3 << 20, 4096, 4096, big, None) == jerk.JERK_EUNSUPPORTED
+    assert L.jerk_realfft(4096, 7 << 20, 4096, 4096, big, None) == jerk.JERK_EUNSUPPORTED
     assert L.jerk_realfft(None, 1 << 20, 4096, 4096, big, None) == jerk.JERK_EINVAL
     assert L.jerk_realfft(4100, 1 << 20, 4096, 4096, big, None) == jerk.JERK_EINVAL  # misaligned
     assert L.jerk_realfft(4096, 1 << 20, 4096, 4096, big - 1, None) == jerk.JERK_EINVAL

@@ -203,7 +203,7 @@ def test_time_series_requests_equal_their_spectra():
     with pytest.raises(jerk.JerkError):  # not a supported series length
         s2 = jerk.JerkServer(max_active=1)
         try:
-            s2.submit(np.zeros(3 << 16, np.float32), 3 << 16, dt, 20, 60, 8, 2.0,
+            s2.submit(np.zeros(7 << 16, np.float32), 7 << 16, dt, 20, 60, 8, 2.0,
                       timeseries=True)
         finally:
             s2.close()
