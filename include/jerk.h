@@ -324,6 +324,10 @@ typedef struct jerk_request {
                                     spectrum on the GPU as the reference does for a .dat
                                     input (jerk_spectrum_from_timeseries); numbins is taken
                                     as N / 2.  N: a length jerk_realfft takes */
+    const double *bird_lobins;   /* time-series requests: birdies to zap after the      */
+    const double *bird_hibins;   /* preparation (jerk_zap_birdies; host arrays of        */
+    int numbirds;                /* numbirds, valid until the result is polled), as a    */
+                                 /* -zaplist run zaps them; 0 = none                     */
 } jerk_request;
 
 typedef struct jerk_result {

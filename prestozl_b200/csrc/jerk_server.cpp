@@ -208,9 +208,13 @@ static int prepare_series(jerk_server *s, Slot &sl)
                         sl.req.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                         s->stream) != cudaSuccess)
         return JERK_ECUDA;
-    return jerk_spectrum_from_timeseries((const float *)sl.series, sl.req.N, sl.series,
-                                         (char *)sl.series + off, sl.series_bytes - off,
-                                         s->stream);
+    int rc = jerk_spectrum_from_timeseries((const float *)sl.series, sl.req.N, sl.series,
+                                           (char *)sl.series + off, sl.series_bytes - off,
+                                           s->stream);
+    if (rc == JERK_OK && sl.req.numbirds > 0)
+        rc = jerk_zap_birdies(sl.series, sl.req.N / 2, sl.req.N, sl.req.bird_lobins,
+                              sl.req.bird_hibins, sl.req.numbirds, s->stream);
+    return rc;
 }
 
 static void release_bank(jerk_server *s, const BankKey &k)
@@ -514,7 +518,11 @@ extern "C" int jerk_server_submit(jerk_server *s, const jerk_request *req)
     if (r.timeseries) {
         if (jerk_spectrum_scratch_bytes(r.N) <= 0)
             return JERK_EUNSUPPORTED;
+        if (r.numbirds < 0 || (r.numbirds > 0 && (!r.bird_lobins || !r.bird_hibins)))
+            return JERK_EINVAL;
         r.numbins = r.N / 2;
+    } else {
+        r.numbirds = 0;
     }
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop)

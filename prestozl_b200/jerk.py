@@ -80,7 +80,8 @@ class Request(C.Structure):
                 ("N", C.c_longlong), ("dt", C.c_double), ("zmax", C.c_int), ("wmax", C.c_int),
                 ("wmax_given", C.c_int), ("numharm", C.c_int), ("sigma", C.c_float),
                 ("flo", C.c_double), ("fhi", C.c_double), ("tag", C.c_longlong),
-                ("timeseries", C.c_int)]
+                ("timeseries", C.c_int), ("bird_lobins", C.c_void_p), ("bird_hibins", C.c_void_p),
+                ("numbirds", C.c_int)]
 
 
 class Result(C.Structure):
@@ -548,11 +549,12 @@ class JerkServer:
 
     def submit(self, spectrum, N: int, dt: float, zmax: int, wmax: int, numharm: int,
                sigma: float, wmax_given: bool = True, flo: float = 1.0, fhi: float = 10000.0,
-               tag: Optional[int] = None, timeseries: bool = False) -> int:
+               tag: Optional[int] = None, timeseries: bool = False, birdies=None) -> int:
         """Queue one search.  ``spectrum``: the complex64 spectrum (numpy or a
         CUDA tensor), or with ``timeseries=True`` the N float32 samples of a
         time series, which the server turns into its spectrum on the GPU as
-        the reference does for a .dat input."""
+        the reference does for a .dat input; ``birdies`` = (lobins, hibins)
+        are then zapped after it, as a -zaplist run zaps them."""
         if timeseries:
             if getattr(spectrum, "is_cuda", False):
                 ptr, dev, keep = C.c_void_p(spectrum.data_ptr()), 1, spectrum
@@ -569,9 +571,14 @@ class JerkServer:
         if tag is None:
             tag = self._next
         self._next = max(self._next, tag) + 1
-        self._keep[tag] = keep
         req = Request(ptr, dev, numbins, N, dt, zmax, wmax, int(wmax_given), numharm, sigma,
                       flo, fhi, tag, int(timeseries))
+        if birdies is not None:
+            lo = np.ascontiguousarray(birdies[0], dtype=np.float64)
+            hi = np.ascontiguousarray(birdies[1], dtype=np.float64)
+            keep = (keep, lo, hi)
+            req.bird_lobins, req.bird_hibins, req.numbirds = lo.ctypes.data, hi.ctypes.data, len(lo)
+        self._keep[tag] = keep  # alive until the result is polled
         _check(lib().jerk_server_submit(self._s, C.byref(req)))
         return tag
 

@@ -207,3 +207,35 @@ def test_time_series_requests_equal_their_spectra():
                       timeseries=True)
         finally:
             s2.close()
+
+
+def test_time_series_request_with_birdies():
+    """A time-series request carrying a birdie list: the server zaps the
+    birdies after making the spectrum, as a -zaplist run does, and the
+    candidates equal those of the spectrum prepared and zapped beforehand
+    (jerk_spectrum_from_timeseries then jerk_zap_birdies)."""
+    torch = pytest.importorskip("torch")
+    build.build()
+    N, dt = 1 << 20, 64e-6
+    rng = np.random.default_rng(41)
+    ps = synth.random_pulsars(rng, 2, zmax=16.0, wmax=48.0, fmax=200.0)
+    ts = np.ascontiguousarray(synth.timeseries(N, dt, ps, 41), dtype=np.float32)
+    # zap the strongest pulsar's fundamental region and an empty band
+    r0 = ps[0].f * N * dt
+    lob, hib = [r0 - 40.0, 120000.0], [r0 + 40.0, 120050.0]
+    spec = jerk.spectrum_from_timeseries(torch.from_numpy(ts).cuda())
+    jerk.zap_birdies(spec, N, lob, hib)
+    torch.cuda.synchronize()
+    params = (N, dt, 20, 60, 8, 2.0)
+    srv = jerk.JerkServer(max_active=2, batch=16)
+    srv.submit(ts, *params, tag=0, timeseries=True, birdies=(lob, hib))
+    srv.submit(spec, *params, tag=1)
+    srv.submit(ts, *params, tag=2, timeseries=True)  # no birdies
+    got = {}
+    while len(got) < 3:
+        r = srv.poll(60000)
+        assert r is not None, "server stalled"
+        got[r[0]] = r[1]
+    srv.close()
+    assert np.array_equal(got[0], got[1])
+    assert not np.array_equal(got[0], got[2])  # the zapping changed the result
