@@ -141,6 +141,14 @@ struct BankGroup {
     int first, count;  // rows [first, first + count) of one fftlen
 };
 
+// Twiddle tables beside the buffer in shared memory, except where they do not
+// fit (15360): read from global memory there.
+template <int N>
+struct BankTwInSmem {
+    static constexpr bool value =
+        (size_t)(fft_buf_len<N>() + FftPlan<N>::twsize()) * 8 <= 200 * 1024;
+};
+
 template <int N>
 __global__ void __launch_bounds__(FftPlan<N>::T)
     bank_fft_kernel(const BankRow *rows, int first, const float2 *twiddles, int twoff,
@@ -150,12 +158,15 @@ __global__ void __launch_bounds__(FftPlan<N>::T)
     constexpr int T = FftPlan<N>::T;
     constexpr int TWN = FftPlan<N>::twsize();
     extern __shared__ float2 smb[];
-    float2 *buf = smb, *tw = smb + fft_buf_len<N>();
+    float2 *buf = smb;
+    const float2 *tw = BankTwInSmem<N>::value ? smb + fft_buf_len<N>() : twiddles + twoff;
     const int tid = threadIdx.x;
     const BankRow R = rows[first + blockIdx.x];
     float2 *row = bank + R.off;
-    for (int i = tid; i < TWN; i += T)
-        tw[i] = twiddles[twoff + i];
+    if constexpr (BankTwInSmem<N>::value) {
+        for (int i = tid; i < TWN; i += T)
+            smb[fft_buf_len<N>() + i] = twiddles[twoff + i];
+    }
     __syncthreads();
     auto in = [&](int r) -> float2 { return row[tid + r * (N / R0)]; };
     auto out = [&](int m, float2 y) { row[m] = y; };
@@ -166,7 +177,8 @@ template <int N>
 static cudaError_t launch_bank_fft(const BankRow *rows, int first, int count, const float2 *tw,
                                    int twoff, float2 *bank, cudaStream_t st)
 {
-    const size_t smem = sizeof(float2) * (fft_buf_len<N>() + FftPlan<N>::twsize());
+    const size_t smem =
+        sizeof(float2) * (fft_buf_len<N>() + (BankTwInSmem<N>::value ? FftPlan<N>::twsize() : 0));
     cudaError_t e = cudaFuncSetAttribute(bank_fft_kernel<N>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
@@ -193,6 +205,7 @@ cudaError_t launch_bank_fft_any(int N, const BankRow *rows, int first, int count
     case 7680: return launch_bank_fft<7680>(rows, first, count, tw, twoff, bank, st);
     case 8192: return launch_bank_fft<8192>(rows, first, count, tw, twoff, bank, st);
     case 10240: return launch_bank_fft<10240>(rows, first, count, tw, twoff, bank, st);
+    case 15360: return launch_bank_fft<15360>(rows, first, count, tw, twoff, bank, st);
     default: return cudaErrorInvalidValue;
     }
 }

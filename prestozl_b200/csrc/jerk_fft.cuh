@@ -200,6 +200,7 @@ JERK_FFT_PLAN(5120, 16, 16, 4, 5)
 JERK_FFT_PLAN(7680, 16, 16, 2, 3, 5)
 JERK_FFT_PLAN(8192, 16, 16, 16, 2)
 JERK_FFT_PLAN(10240, 16, 16, 8, 5)
+JERK_FFT_PLAN(15360, 16, 16, 4, 3, 5)
 #undef JERK_FFT_PLAN
 
 template <int SIGN>

@@ -208,7 +208,7 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
     }
 }
 
-__global__ void prep_kernel(const SearchDev P)
+__global__ void __launch_bounds__(1024) prep_kernel(const SearchDev P)
 {
     extern __shared__ float smem[];
     const int b = blockIdx.x, s = blockIdx.y;
@@ -230,6 +230,7 @@ __global__ void prep_kernel(const SearchDev P)
         JERK_PREP_CASE(5120)
         JERK_PREP_CASE(7680)
         JERK_PREP_CASE(10240)
+        JERK_PREP_CASE(15360)
 #undef JERK_PREP_CASE
     default:
         break;
@@ -251,9 +252,19 @@ struct CorrOcc {
 // Shared memory of corr_kernel<N>, in float2: the FFT buffer, the twiddle
 // tables and (when that still leaves CorrOcc CTAs per SM) a staging row for
 // the next rstep's prepared data.
+// Lengths whose twiddle tables do not fit beside the buffer (15360: 158 KB of
+// tables) read twiddles and kernel rows from global memory (L1/L2) instead of
+// shared memory and registers; 960 threads leave 68 registers a thread.
+template <int N>
+struct CorrBig {
+    static constexpr bool value =
+        (size_t)(fft_buf_len<N>() + FftPlan<N>::twsize()) * 8 > 200 * 1024;
+};
+
 template <int N>
 struct CorrSmem {
-    static constexpr int kBase = (fft_buf_len<N>() + FftPlan<N>::twsize() + 1) & ~1;
+    static constexpr int kBase =
+        (fft_buf_len<N>() + (CorrBig<N>::value ? 0 : FftPlan<N>::twsize()) + 1) & ~1;
     static constexpr bool kStage = (size_t)(kBase + N) * 8 * CorrOcc<N>::value <= 220 * 1024;
     static constexpr int value = kBase + (kStage ? N : 0);
 };
@@ -303,10 +314,11 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     constexpr int T = FftPlan<N>::T;
     constexpr int TWN = FftPlan<N>::twsize();
     constexpr bool kStage = CorrSmem<N>::kStage;
+    constexpr bool kBig = CorrBig<N>::value;
     extern __shared__ __align__(16) float2 sm2[];
     __shared__ uint64_t s_bar;
     float2 *buf = sm2;
-    float2 *tw = sm2 + fft_buf_len<N>();
+    float2 *tws = sm2 + fft_buf_len<N>();
     float2 *dsm = sm2 + CorrSmem<N>::kBase;  // staged data row (kStage)
     const int tid = threadIdx.x;
     const int row = blockIdx.x;
@@ -332,15 +344,21 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
             bulk_row_load(dsm, D0 + (long long)b0 * N, N * sizeof(float2), &s_bar);
     }
 
-    for (int i = tid; i < TWN; i += T)
-        tw[i] = P.twiddles[sd.twoff + i];
+    const float2 *tw = kBig ? P.twiddles + sd.twoff : tws;
+    if constexpr (!kBig) {
+        for (int i = tid; i < TWN; i += T)
+            tws[i] = P.twiddles[sd.twoff + i];
+    }
 
     // the kernel row, in the order this thread's first-stage butterfly reads it
+    // (kBig: read from global memory at every rstep instead)
     float2 kreg[R0];
     const float2 *K = P.bank + sd.kern_off + (long long)lrow * N;
+    if constexpr (!kBig) {
 #pragma unroll
-    for (int r = 0; r < R0; r++)
-        kreg[r] = K[tid + r * (N / R0)];
+        for (int r = 0; r < R0; r++)
+            kreg[r] = K[tid + r * (N / R0)];
+    }
     __syncthreads();
 
     const int offset = sd.halfwidth * 2;  // binoffset * ACCEL_NUMBETWEEN
@@ -375,7 +393,10 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
             fft_block<N, +1>(buf, tw, tid, in, out, mid);
         } else {
             const float2 *D = D0 + (long long)b * N;
-            auto in = [&](int r) -> float2 { return cmulconj(D[tid + r * (N / R0)], kreg[r]); };
+            auto in = [&](int r) -> float2 {
+                const int m = tid + r * (N / R0);
+                return cmulconj(D[m], kBig ? K[m] : kreg[r]);
+            };
             fft_block<N, +1>(buf, tw, tid, in, out);
         }
         __syncthreads();
@@ -861,7 +882,7 @@ size_t prep_smem_bytes(int maxfft)
     if (NN <= maxfft && prep_bytes_n<NN>() > b)      \
         b = prep_bytes_n<NN>();
     JERK_PB(128) JERK_PB(192) JERK_PB(256) JERK_PB(384) JERK_PB(512) JERK_PB(768)
-    JERK_PB(1024) JERK_PB(1280) JERK_PB(2048) JERK_PB(4096) JERK_PB(5120) JERK_PB(7680) JERK_PB(10240)
+    JERK_PB(1024) JERK_PB(1280) JERK_PB(2048) JERK_PB(4096) JERK_PB(5120) JERK_PB(7680) JERK_PB(10240) JERK_PB(15360)
 #undef JERK_PB
     return b;
 }
@@ -872,7 +893,7 @@ int fft_twiddle_size(int N)
     switch (N) {
 #define JERK_TS(NN) case NN: return FftPlan<NN>::twsize();
     JERK_TS(128) JERK_TS(192) JERK_TS(256) JERK_TS(384) JERK_TS(512) JERK_TS(768)
-    JERK_TS(1024) JERK_TS(1280) JERK_TS(2048) JERK_TS(4096) JERK_TS(5120) JERK_TS(7680) JERK_TS(10240)
+    JERK_TS(1024) JERK_TS(1280) JERK_TS(2048) JERK_TS(4096) JERK_TS(5120) JERK_TS(7680) JERK_TS(10240) JERK_TS(15360)
 #undef JERK_TS
     default: return -1;
     }
@@ -883,7 +904,7 @@ void fft_twiddle_table(int N, float2 *out)
     switch (N) {
 #define JERK_TT(NN) case NN: fft_stage_twiddles<NN>(out); break;
     JERK_TT(128) JERK_TT(192) JERK_TT(256) JERK_TT(384) JERK_TT(512) JERK_TT(768)
-    JERK_TT(1024) JERK_TT(1280) JERK_TT(2048) JERK_TT(4096) JERK_TT(5120) JERK_TT(7680) JERK_TT(10240)
+    JERK_TT(1024) JERK_TT(1280) JERK_TT(2048) JERK_TT(4096) JERK_TT(5120) JERK_TT(7680) JERK_TT(10240) JERK_TT(15360)
 #undef JERK_TT
     default: break;
     }
@@ -897,7 +918,7 @@ int prep_threads(int maxfft)
     if (NN <= maxfft && FftPlan<NN>::T > t)          \
         t = FftPlan<NN>::T;
     JERK_PT(128) JERK_PT(192) JERK_PT(256) JERK_PT(384) JERK_PT(512) JERK_PT(768)
-    JERK_PT(1024) JERK_PT(1280) JERK_PT(2048) JERK_PT(4096) JERK_PT(5120) JERK_PT(7680) JERK_PT(10240)
+    JERK_PT(1024) JERK_PT(1280) JERK_PT(2048) JERK_PT(4096) JERK_PT(5120) JERK_PT(7680) JERK_PT(10240) JERK_PT(15360)
 #undef JERK_PT
     return (t + 31) / 32 * 32;
 }
@@ -950,7 +971,7 @@ bool fftlen_supported(int n)
 {
     switch (n) {
     case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 1280:
-    case 2048: case 4096: case 5120: case 7680: case 10240:
+    case 2048: case 4096: case 5120: case 7680: case 10240: case 15360:
         return true;
     default:
         return false;
@@ -974,6 +995,7 @@ cudaError_t launch_corr(const SearchDev &P, int fftlen, const RowGroup &G, int r
     case 5120: return launch_corr_n<5120>(P, G, rows, st);
     case 7680: return launch_corr_n<7680>(P, G, rows, st);
     case 10240: return launch_corr_n<10240>(P, G, rows, st);
+    case 15360: return launch_corr_n<15360>(P, G, rows, st);
     default: return cudaErrorInvalidValue;
     }
 }

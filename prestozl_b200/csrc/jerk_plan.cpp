@@ -1040,7 +1040,7 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     for (int s = 0; s < nsubs; s++)  // before any device work
         if (!fftlen_supported(subs[s].fftlen))
             return fail(JERK_EUNSUPPORTED, "unsupported fftlen " + std::to_string(subs[s].fftlen) +
-                                               " (at most 10240 here)");
+                                               " (at most 15360 here)");
 
     jerk_plan *p = new jerk_plan();
     cudaGetDevice(&p->device);

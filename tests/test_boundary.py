@@ -125,13 +125,13 @@ def test_bad_tuning_knob_is_rejected_before_any_device_work():
 
 
 def test_unsupported_fft_length_is_rejected_before_any_device_work():
-    # zmax 1200, wmax 1500 needs fftlen 15360 (the longest supported is 10240)
-    obs, fftlen, _ = jerk.obs_from_params(1 << 24, 1 << 25, 54.6e-6, 1200, 1500, 16, 3.0)
-    assert fftlen == 15360
+    # zmax 1400, wmax 1500 needs fftlen 25600 (the longest supported is 15360)
+    obs, fftlen, _ = jerk.obs_from_params(1 << 24, 1 << 25, 54.6e-6, 1400, 1500, 16, 3.0)
+    assert fftlen == 25600
     subs = jerk.subharm_sizes(obs, fftlen)
     with pytest.raises(jerk.JerkError) as ei:
         jerk.JerkPlan(obs, subs, batch=4)
-    assert ei.value.code == jerk.JERK_EUNSUPPORTED and "15360" in str(ei.value)
+    assert ei.value.code == jerk.JERK_EUNSUPPORTED and "25600" in str(ei.value)
 
 
 def test_input_entry_points_size_and_reject_before_any_device_work():

@@ -112,3 +112,51 @@ def test_paper_scale_bank_samples_match_reference(tmp_path):
     bank.close()
     ref.close()
     print(f"worst sampled kernel-row error (z200 w300 h16): {worst:.2e}")
+
+
+def _reference_kernel_row(z: float, w: float, fftlen: int) -> np.ndarray:
+    """One bank row as the reference's init_kernel (src/accel_utils.c:151-168)
+    makes it: gen_w_response from the reference build, placed wrapped around
+    fftlen (src/corr_prep.c:92-114), forward FFT (here in FP64)."""
+    import ctypes as C
+
+    lib = ob._ref()
+    lib.ref_w_resp_halfwidth.restype = C.c_int
+    khw = lib.ref_w_resp_halfwidth(float(z), float(w), 0)  # LOWACC
+    numkern = 2 * 2 * khw
+    resp = np.zeros(numkern, dtype=np.complex64)
+    lib.ref_gen_w_response(0.0, 2, float(z), float(w), numkern, resp.ctypes.data)
+    row = np.zeros(fftlen, dtype=np.complex128)
+    row[fftlen - numkern // 2:] = resp[: numkern // 2]
+    row[: numkern // 2] = resp[numkern // 2:]
+    return np.fft.fft(row)
+
+
+def test_longest_fft_bank_samples_match_reference():
+    """-zmax 1200 -wmax 1500 -numharm 2: the fundamental's kernels need fftlen
+    15360 (1201 x 151 rows, 22 GB), the subharmonic's 10240.  Sampled rows of
+    both against the reference's gen_w_response, placed and FFT'd as
+    init_kernel does (the reference's own bank of this size would take hours
+    on the CPU)."""
+    build.build()
+    H.ensure_oracle()
+    if not H.have_ref():
+        pytest.skip("reference build missing")
+    obs, fftlen, _ = jerk.obs_from_params(1 << 21, 1 << 22, 64e-6, 1200, 1500, 2, 3.0)
+    assert fftlen == 15360
+    subs = jerk.subharm_sizes(obs, fftlen)
+    bank = jerk.DeviceBank(subs)
+    rng = np.random.default_rng(3)
+    worst = 0.0
+    for i, s in enumerate(subs):
+        n = s["numw"] * s["numz"]
+        pick = sorted(set([0, n - 1, n // 2] + [int(v) for v in rng.integers(0, n, 5)]))
+        got = bank.rows(subs, i, pick)
+        for g, r in zip(got, pick):
+            ii, jj = divmod(r, s["numz"])
+            want = _reference_kernel_row(-s["zmax"] + 2 * jj, -s["wmax"] + 20 * ii, s["fftlen"])
+            e = _rel_err(g.astype(np.complex128), want)
+            worst = max(worst, e)
+            assert e <= ROW_TOL, (i, r, e)
+    bank.close()
+    print(f"worst sampled kernel-row error (z1200 w1500, fftlen 15360): {worst:.2e}")

@@ -37,8 +37,11 @@ CONFIGS = {
     "n22_z100_w0_h16": (22, 100, 0, 16, 2.0, 8),
     "n24_z200_w300_h8": (24, 200, 300, 8, 2.0, 3),
     "n25_z300_w600_h32": (25, 300, 600, 32, 4.0, 0),
-    # the longest supported FFT length (10240)
+    # FFT length 10240
     "n22_z600_w1200_h8": (22, 600, 1200, 8, 3.0, 0),
+    # the longest supported FFT length (15360; one rstep per batch under the
+    # 32-bit volume limit)
+    "n22_z1200_w1500_h2": (22, 1200, 1500, 2, 3.0, 0),
 }
 POW_TOL = 1e-5
 
