@@ -240,6 +240,37 @@ int jerk_polish_rzw(jerk_polisher *polisher, const void *spectrum, long long num
                     double rin, double zin, double win, const float *locpow, double *rout,
                     double *zout, double *wout, float *maxpow);
 
+/* The reference's rderivs (include/presto.h:161-169): power and phase at a
+ * point of the f / f-dot / f-dotdot volume, their first and second
+ * derivatives in r, and the local power level. */
+typedef struct jerk_rderivs {
+    double pow, phs, dpow, dphs, d2pow, d2phs, locpow;
+} jerk_rderivs;
+
+/* get_localpower3d (src/characteristics.c:75-135) at n points (r relative
+ * to the spectrum's value 0): the mean power of the complex interpolations
+ * (rzw_interp, src/rzwinterp.c:151-228) at the 10 bins either side, 5 bins
+ * away.  On the GPU; results agree with the reference's to FP32 rounding. */
+int jerk_local_power(jerk_polisher *polisher, const void *spectrum, long long numdata, int n,
+                     const double *r, const double *z, const double *w, double *out);
+/* get_derivs3d (src/characteristics.c:138-191) at n points with the given
+ * local powers: interpolations 0.003 bins apart at HIGHACC, then the finite
+ * differences of power and phase. */
+int jerk_derivs(jerk_polisher *polisher, const void *spectrum, long long numdata, int n,
+                const double *r, const double *z, const double *w, const double *locpow,
+                jerk_rderivs *out);
+/* The reference's default candidate optimisation (optimize_accelcand with
+ * harmonic polishing, src/accel_utils.c:573-657) wholly on the GPU: local
+ * powers, jerk_polish_rzw, then per harmonic h = 1..numharm the local power
+ * and derivatives at (h r, h z, h w).  rzw_out[3] = polished r (relative to
+ * value 0), z, w; derivs[numharm]; locpow_used[numharm] (optional) = the local
+ * powers the volume search divided by.  Without the reference's host
+ * routines the derivatives agree with its to FP32 rounding (the drop-in
+ * keeps the reference's own routines for byte-identical ACCEL files). */
+int jerk_optimize_cand(jerk_polisher *polisher, const void *spectrum, long long numdata,
+                       int numharm, double rin, double zin, double win, double *rzw_out,
+                       jerk_rderivs *derivs, float *locpow_used);
+
 /* The search's input from a time series, on the GPU: the steps the reference
  * takes for a ".dat" input (src/accel_utils.c:1696-1753) before it searches.
  *

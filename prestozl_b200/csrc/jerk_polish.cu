@@ -885,3 +885,491 @@ extern "C" int jerk_polish_rzw(jerk_polisher *p, const void *spectrum, long long
         *maxpow = bpow;
     return JERK_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Complex interpolation at single points: the reference's rzw_interp
+// (src/rzwinterp.c:151-228) and rz_interp (src/rzinterp.c:144-235), on
+// which its local power (get_localpower3d, src/characteristics.c:75-135)
+// and peak derivatives (get_derivs3d, src/characteristics.c:138-191) stand.
+// A point correlates 2 khw spectrum bins around floor(r) with the response
+// of (frac(r), z, w) at one point per bin: gen_w_response (the cosine series
+// and real FFT, as above, with the fractional offset) where |w| >= 1e-4,
+// else gen_z_response / gen_r_response.  One CTA per point; the products
+// are summed in double and rounded to the float answer.
+
+namespace jerk {
+namespace {
+
+struct InterpPoint {
+    long long win;  // float2 offset of the staged data window (numkern bins)
+    double frac, z, w;
+    int numkern;    // 2 kern_half_width
+    int npts;       // w responses: the cosine series' length (M = npts / 2)
+};
+
+constexpr int kInterpThreads = 256;
+
+template <int NT>
+__device__ __forceinline__ void block_sum2(double &a, double &b)
+{
+    __shared__ double red[2][NT / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][wid] = a;
+        red[1][wid] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a = 0.0;
+        b = 0.0;
+        for (int i = 0; i < NT / 32; i++) {
+            a += red[0][i];
+            b += red[1][i];
+        }
+    }
+}
+
+// the reference's sum for one bin: ans += data x conj(response)
+__device__ __forceinline__ void corr_acc(float2 d, float re, float im, double &ar, double &ai)
+{
+    ar += (double)d.x * re + (double)d.y * im;
+    ai += (double)d.y * re - (double)im * d.x;
+}
+
+__global__ void __launch_bounds__(kInterpThreads)
+    interp_zr_kernel(const InterpPoint *__restrict__ pts, const int *__restrict__ list,
+                     const float2 *__restrict__ windows, float2 *__restrict__ ans)
+{
+    const int pi = list[blockIdx.x];
+    const InterpPoint P = pts[pi];
+    const float2 *d = windows + P.win;
+    const int tid = threadIdx.x, numkern = P.numkern;
+    const double z = P.z, roff = P.frac;
+    double ar = 0.0, ai = 0.0;
+    if (fabs(z) >= 1e-4) {
+        // gen_z_response(roff, 1, z, numkern) (src/responses.c:228-313)
+        const double absz = fabs(z);
+        const double startr0 = roff - 0.5 * z;
+        double ipart;
+        const double startroffset =
+            startr0 < 0.0 ? 1.0 + modf(startr0, &ipart) : modf(startr0, &ipart);
+        const int signz = z < 0.0 ? -1 : 1;
+        const double zd = signz * 1.4142135623730950488016887242096980785696718753769 / sqrt(absz);
+        const double cons = zd / 2.0;
+        const double pibyz = M_PI / z;
+        const double startr = startr0 + numkern / 2.0;
+        for (int ii = tid; ii < numkern; ii += kInterpThreads) {
+            const double r = startr - (double)ii;
+            const double yy = __dmul_rn(r, zd);
+            const double zz = __dadd_rn(yy, __dmul_rn(z, zd));
+            const double xx = __dmul_rn(__dmul_rn(pibyz, r), r);
+            double sn, cs, fsy, fcy, fsz, fcz;
+            sincos(xx, &sn, &cs);
+            fresnel(yy, &fsy, &fcy);
+            fresnel(zz, &fsz, &fcz);
+            const double tmprl = signz * (fcz - fcy);
+            const double tmpim = fsy - fsz;
+            float re = (float)__dmul_rn(__dsub_rn(__dmul_rn(tmprl, cs), __dmul_rn(tmpim, sn)), cons);
+            float im = (float)-__dmul_rn(__dadd_rn(__dmul_rn(tmprl, sn), __dmul_rn(tmpim, cs)), cons);
+            if (ii == numkern / 2 && startroffset < 1e-3 && absz < 1e-3) {
+                const double z2 = z * z, x2 = startroffset * startroffset;
+                double cr = 1.0 - 0.16449340668482264365 * z2;
+                double ci = -0.5235987755982988731 * z;
+                cr += startroffset * 1.6449340668482264365 * z;
+                ci += startroffset * (M_PI - 0.5167712780049970029 * z2);
+                cr += x2 * (-6.579736267392905746 + 0.9277056288952613070 * z2);
+                ci += x2 * (3.1006276680299820175 * z);
+                re = (float)cr;
+                im = (float)ci;
+            }
+            corr_acc(d[ii], re, im, ar, ai);
+        }
+    } else {
+        // gen_r_response(roff, 1, numkern) (src/responses.c:158-226): value ii
+        // is exp(i r) sin(r) / r at r = pi (numkern / 2 + roff - ii)
+        for (int ii = tid; ii < numkern; ii += kInterpThreads) {
+            const double q = numkern / 2.0 + roff - (double)ii;
+            float re = 1.0f, im = 0.0f;
+            if (q != 0.0) {
+                double sn, cs;
+                sincospi(q, &sn, &cs);
+                const double sinc = sn / (M_PI * q);
+                re = (float)(cs * sinc);
+                im = (float)(sn * sinc);
+            }
+            if (ii == numkern / 2 && roff < 1e-3) {
+                const double x2 = roff * roff;
+                re = (float)(1.0 - 6.579736267392905746 * x2);
+                im = (float)(roff * (M_PI - 10.335425560099940058 * x2));
+            }
+            corr_acc(d[ii], re, im, ar, ai);
+        }
+    }
+    block_sum2<kInterpThreads>(ar, ai);
+    if (tid == 0)
+        ans[pi] = make_float2((float)ar, (float)ai);
+}
+
+// gen_w_response(roff, 1, z, w, numkern) (src/responses.c:333-418): the
+// cosine series of npts = 2M samples read as M complex values, FFT'd, and
+// the numkern bins around M / 2 split out of the window that the last stage
+// drops into shared memory; then the correlation with the data window.
+template <int M>
+__global__ void __launch_bounds__(FftPlan<M>::T)
+    interp_w_kernel(const InterpPoint *__restrict__ pts, const int *__restrict__ list,
+                    const float2 *__restrict__ tw, const float2 *__restrict__ windows,
+                    float2 *__restrict__ ans)
+{
+    constexpr int T = FftPlan<M>::T;
+    extern __shared__ float2 iw_smem[];
+    float2 *buf = iw_smem;
+    float2 *win = iw_smem + fft_buf_len<M>();
+    const int pi = list[blockIdx.x];
+    const InterpPoint P = pts[pi];
+    const int tid = threadIdx.x, numkern = P.numkern, npts = P.npts;
+    const double z = P.z, w = P.w;
+    const double dt = 1.0 / (double)npts;
+    const double amp = 2.0 * dt;
+    const int fbar = npts / 4;
+    const double dfbar = (double)fbar + P.frac;
+    const double f = __dadd_rn(__dsub_rn(dfbar, 0.5 * z), w / 12.0);
+    const double fd = (z - 0.5 * w) / 2.0;
+    const double fdd = w / 6.0;
+    auto xval = [&](int n) -> float {
+        const double t = __dmul_rn((double)n, dt);
+        const double in1 = __dadd_rn(__dmul_rn(t, fdd), fd);
+        const double in2 = __dadd_rn(__dmul_rn(t, in1), f);
+        const double ph = __dmul_rn(6.2831853071795864769252867665590057683943387987502,
+                                    __dmul_rn(t, in2));
+        return (float)__dmul_rn(amp, cos(ph));
+    };
+    auto in = [&](int r) -> float2 {
+        const int m = tid + r * T;
+        return make_float2(xval(2 * m), xval(2 * m + 1));
+    };
+    const int lo = M / 2 - numkern / 2;
+    auto out = [&](int k, float2 y) {
+        if (k >= lo && k <= lo + numkern)
+            win[k - lo] = y;
+    };
+    fft_block<M, -1>(buf, tw, tid, in, out);
+    __syncthreads();
+    const float2 *d = windows + P.win;
+    double ar = 0.0, ai = 0.0;
+    for (int k = tid; k < numkern; k += T) {
+        const int kc = lo + k;
+        const float2 a = win[k], b = win[numkern - k];
+        const double hx = 0.5 * ((double)a.x + (double)b.x);
+        const double hy = 0.5 * ((double)a.y - (double)b.y);
+        const double dx = (double)a.x - (double)b.x;
+        const double dy = (double)a.y + (double)b.y;
+        double s, c;
+        sincospi(-(double)kc / (double)M, &s, &c);
+        const double gx = c * dx - s * dy, gy = c * dy + s * dx;
+        corr_acc(d[k], (float)(hx + 0.5 * gy), (float)(hy - 0.5 * gx), ar, ai);
+    }
+    block_sum2<T>(ar, ai);
+    if (tid == 0)
+        ans[pi] = make_float2((float)ar, (float)ai);
+}
+
+template <int M> struct PI {
+    static cudaError_t run(const InterpPoint *pts, const int *list, int count, const float2 *tw,
+                           const float2 *windows, float2 *ans, int maxkern, cudaStream_t st)
+    {
+        const int smem = (int)(sizeof(float2) * (fft_buf_len<M>() + maxkern + 1));
+        cudaError_t e = cudaFuncSetAttribute(interp_w_kernel<M>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess)
+            return e;
+        interp_w_kernel<M><<<count, FftPlan<M>::T, smem, st>>>(pts, list, tw, windows, ans);
+        return cudaGetLastError();
+    }
+};
+
+int whw_high(double z, double w) { return w_resp_halfwidth_lowacc(z, w) + 32; }
+
+}  // namespace
+}  // namespace jerk
+
+namespace {
+
+// rzw_interp at n points: answers (the reference's float fcomplex) in ans.
+int interp_points(jerk_polisher *p, const float2 *data, long long numdata, int n,
+                  const double *r, const double *z, const double *w, const int *khw,
+                  float2 *ans)
+{
+    std::vector<InterpPoint> pts(n);
+    std::vector<int> zr, wl[kNumSizes];
+    int maxkern[kNumSizes] = {};
+    long long win_len = 0;
+    std::vector<long long> first(n, 0);
+    for (int i = 0; i < n; i++) {
+        ans[i] = make_float2(0.f, 0.f);
+        pts[i].numkern = 0;
+        if (r[i] > numdata - 1.0 || r[i] < 0.0)
+            continue;  // the reference answers 0 out of range
+        double ip;
+        const double frac = modf(r[i], &ip);
+        const long long intfreq = (long long)ip;
+        if (fabs(w[i]) < 1e-4 && fabs(z[i]) < 1e-4) {
+            if (frac < 1e-5) {
+                ans[i] = data[intfreq];
+                continue;
+            }
+            if ((1.0 - frac) < 1e-5) {
+                ans[i] = data[intfreq + 1];
+                continue;
+            }
+        }
+        InterpPoint &P = pts[i];
+        P.frac = frac;
+        P.z = z[i];
+        P.w = w[i];
+        P.numkern = 2 * khw[i];
+        P.win = win_len;
+        first[i] = intfreq - khw[i];
+        win_len += P.numkern;
+        P.npts = 0;
+        if (fabs(w[i]) >= 1e-4) {
+            P.npts = (int)next2(6 * w_resp_halfwidth_lowacc(z[i], w[i]) + 200 + P.numkern);
+            const int M = P.npts / 2;
+            const int si = size_index(M);
+            if (si < 0 || P.numkern / 2 >= M / 2)
+                return p_fail(JERK_EUNSUPPORTED, "rzw_interp: response FFT beyond 8192 points");
+            wl[si].push_back(i);
+            maxkern[si] = std::max(maxkern[si], P.numkern);
+        } else {
+            zr.push_back(i);
+        }
+    }
+    std::vector<int> lists(zr);
+    int wfirst[kNumSizes], wcount[kNumSizes];
+    for (int s = 0; s < kNumSizes; s++) {
+        wfirst[s] = (int)lists.size();
+        lists.insert(lists.end(), wl[s].begin(), wl[s].end());
+        wcount[s] = (int)wl[s].size();
+    }
+    if (lists.empty())
+        return JERK_OK;
+    const size_t b_pts = sizeof(InterpPoint) * n, b_lists = sizeof(int) * lists.size();
+    const size_t b_win = sizeof(float2) * win_len, b_ans = sizeof(float2) * n;
+    const long long stage = (long long)(b_pts + b_lists + b_win + b_ans);
+    cudaError_t e = cudaStreamSynchronize(p->stream);
+    if (e == cudaSuccess && stage > p->stage_cap) {
+        if (p->h_stage)
+            cudaFreeHost(p->h_stage);
+        p->h_stage = nullptr;
+        p->stage_cap = 0;
+        e = cudaMallocHost(&p->h_stage, stage * 2);
+        if (e == cudaSuccess)
+            p->stage_cap = stage * 2;
+    }
+    if (e != cudaSuccess)
+        return p_cuda(e, "rzw_interp: staging");
+    unsigned char *hs = p->h_stage;
+    memcpy(hs, pts.data(), b_pts);
+    memcpy(hs + b_pts, lists.data(), b_lists);
+    float2 *hw = (float2 *)(hs + b_pts + b_lists);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < pts[i].numkern; k++) {
+            const long long b = first[i] + k;
+            hw[pts[i].win + k] = (b >= 0 && b < numdata) ? data[b] : make_float2(0.f, 0.f);
+        }
+    // device layout in the polisher's buffers: points in d_rows, lists in
+    // d_lists, windows in windows, answers in dfft
+    const long long rows_need = (long long)((b_pts + sizeof(PolishRow) - 1) / sizeof(PolishRow));
+    if ((e = grow(&p->d_rows, &p->rows_cap, rows_need)) != cudaSuccess ||
+        (e = grow(&p->d_lists, &p->lists_cap, (long long)lists.size())) != cudaSuccess ||
+        (e = grow(&p->windows, &p->win_cap, std::max(win_len, 1LL))) != cudaSuccess ||
+        (e = grow(&p->dfft, &p->dfft_cap, (long long)n)) != cudaSuccess)
+        return p_cuda(e, "rzw_interp: device buffers");
+    cudaStream_t st = p->stream;
+    const InterpPoint *d_pts = (const InterpPoint *)p->d_rows;
+    e = cudaMemcpyAsync(p->d_rows, hs, b_pts, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p->d_lists, hs + b_pts, b_lists, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && b_win)
+        e = cudaMemcpyAsync(p->windows, hw, b_win, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !zr.empty()) {
+        interp_zr_kernel<<<(int)zr.size(), kInterpThreads, 0, st>>>(d_pts, p->d_lists, p->windows,
+                                                                     p->dfft);
+        e = cudaGetLastError();
+    }
+    for (int s = 0; s < kNumSizes && e == cudaSuccess; s++)
+        if (wcount[s])
+            e = p_dispatch<PI>(kSizes[s], d_pts, (const int *)p->d_lists + wfirst[s], wcount[s],
+                               (const float2 *)(p->tw + p->twoff[s]), (const float2 *)p->windows,
+                               p->dfft, maxkern[s], st);
+    float2 *hans = (float2 *)(hs + b_pts + b_lists + b_win);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hans, p->dfft, b_ans, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return p_cuda(e, "rzw_interp");
+    for (int i = 0; i < n; i++)
+        if (pts[i].numkern)
+            ans[i] = hans[i];
+    return JERK_OK;
+}
+
+// get_localpower3d's points (src/characteristics.c:95-125): 10 bins either
+// side, 5 bins away from r, clamped to the spectrum; freq advances by 1.0.
+void localpower_points(double r, long long numdata, std::vector<double> &out)
+{
+    double lo1 = r - 5 - 10, hi1 = lo1 + 10, lo2 = r + 5, hi2 = lo2 + 10;
+    auto clamp = [&](double v) { return v < 0.0 ? 0.0 : (v > (double)numdata ? (double)numdata : v); };
+    lo1 = clamp(lo1);
+    hi1 = clamp(hi1);
+    lo2 = clamp(lo2);
+    hi2 = clamp(hi2);
+    for (double f = lo1; f < hi1; f += 1.0)
+        out.push_back(f);
+    for (double f = lo2; f < hi2; f += 1.0)
+        out.push_back(f);
+}
+
+int local_powers(jerk_polisher *p, const float2 *data, long long numdata, int n, const double *r,
+                 const double *z, const double *w, double *out)
+{
+    std::vector<double> pr, pz, pw;
+    std::vector<int> pk, owner;
+    for (int i = 0; i < n; i++) {
+        std::vector<double> f;
+        localpower_points(r[i], numdata, f);
+        const int khw = w_resp_halfwidth_lowacc(z[i], w[i]);
+        for (double v : f) {
+            pr.push_back(v);
+            pz.push_back(z[i]);
+            pw.push_back(w[i]);
+            pk.push_back(khw);
+            owner.push_back(i);
+        }
+    }
+    std::vector<float2> a(pr.size());
+    if (!pr.empty()) {
+        const int rc = interp_points(p, data, numdata, (int)pr.size(), pr.data(), pz.data(),
+                                     pw.data(), pk.data(), a.data());
+        if (rc != JERK_OK)
+            return rc;
+    }
+    for (int i = 0; i < n; i++)
+        out[i] = 0.0;
+    for (size_t j = 0; j < pr.size(); j++) {
+        const double ar = a[j].x, ai = a[j].y;
+        out[owner[j]] += ar * ar + ai * ai;
+    }
+    for (int i = 0; i < n; i++)
+        out[i] /= 20.0;  // NUMLOCPOWAVG
+    return JERK_OK;
+}
+
+}  // namespace
+
+extern "C" int jerk_local_power(jerk_polisher *p, const void *spectrum, long long numdata, int n,
+                                const double *r, const double *z, const double *w, double *out)
+{
+    if (!p || !spectrum || n < 0 || (n && (!r || !z || !w || !out)))
+        return p_fail(JERK_EINVAL, "jerk_local_power: bad argument");
+    return local_powers(p, (const float2 *)spectrum, numdata, n, r, z, w, out);
+}
+
+extern "C" int jerk_derivs(jerk_polisher *p, const void *spectrum, long long numdata, int n,
+                           const double *r, const double *z, const double *w,
+                           const double *locpow, jerk_rderivs *out)
+{
+    if (!p || !spectrum || n < 0 || (n && (!r || !z || !w || !locpow || !out)))
+        return p_fail(JERK_EINVAL, "jerk_derivs: bad argument");
+    // get_derivs3d (src/characteristics.c:138-191): 5 points 0.003 apart
+    // around r at HIGHACC, powers and phases, finite differences
+    const double h = 0.003, twoh = 0.006, twohsqrd = 0.000036;
+    std::vector<double> pr(5 * (size_t)n), pz(5 * (size_t)n), pw(5 * (size_t)n);
+    std::vector<int> pk(5 * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        const int khw = whw_high(z[i], w[i]);
+        double f = r[i] - twoh;
+        for (int k = 0; k < 5; k++, f += h) {
+            pr[5 * i + k] = f;
+            pz[5 * i + k] = z[i];
+            pw[5 * i + k] = w[i];
+            pk[5 * i + k] = khw;
+        }
+    }
+    std::vector<float2> a(pr.size());
+    if (n) {
+        const int rc = interp_points(p, (const float2 *)spectrum, numdata, 5 * n, pr.data(),
+                                     pz.data(), pw.data(), pk.data(), a.data());
+        if (rc != JERK_OK)
+            return rc;
+    }
+    const double twopi = 6.2831853071795864769252867665590057683943387987502;
+    for (int i = 0; i < n; i++) {
+        double pwr[5], phs[5];
+        for (int k = 0; k < 5; k++) {
+            const double ar = a[5 * i + k].x, ai = a[5 * i + k].y;
+            pwr[k] = ar * ar + ai * ai;
+            const double t = atan2(ai, ar);
+            phs[k] = t > 0.0 ? t : t + twopi;
+        }
+        for (int k = 0; k < 4; k++)
+            if (fabs(phs[k + 1] - phs[k]) > M_PI)
+                phs[k + 1] -= twopi;
+        jerk_rderivs &d = out[i];
+        d.pow = pwr[2];
+        d.phs = phs[2];
+        d.dpow = (pwr[3] - pwr[1]) / twoh;
+        d.dphs = (phs[3] - phs[1]) / twoh;
+        d.d2pow = (pwr[4] - 2.0 * pwr[2] + pwr[0]) / twohsqrd;
+        d.d2phs = (phs[4] - 2.0 * phs[2] + phs[0]) / twohsqrd;
+        d.locpow = locpow[i];
+    }
+    return JERK_OK;
+}
+
+// The whole default optimisation of one candidate on the GPU, as
+// optimize_accelcand runs it with harmonic polishing (src/accel_utils.c:
+// 573-657, src/maximize_rzw.c:84-190): local powers, the volume search, then
+// for every harmonic the local power and derivatives at the polished point.
+extern "C" int jerk_optimize_cand(jerk_polisher *p, const void *spectrum, long long numdata,
+                                  int numharm, double rin, double zin, double win,
+                                  double *rzw_out, jerk_rderivs *derivs, float *locpow_used)
+{
+    if (!p || !spectrum || !rzw_out || !derivs || numharm < 1 || numharm > kMaxHarm)
+        return p_fail(JERK_EINVAL, "jerk_optimize_cand: bad argument");
+    double r[kMaxHarm], z[kMaxHarm], w[kMaxHarm], lp[kMaxHarm];
+    for (int i = 0; i < numharm; i++) {
+        const int n = numharm - i;
+        r[i] = rin * n;
+        z[i] = zin * n;
+        w[i] = win * n;
+    }
+    int rc = jerk_local_power(p, spectrum, numdata, numharm, r, z, w, lp);
+    if (rc != JERK_OK)
+        return rc;
+    float lpf[kMaxHarm];
+    for (int i = 0; i < numharm; i++)
+        lpf[i] = (float)lp[i];
+    if (locpow_used)
+        memcpy(locpow_used, lpf, sizeof(float) * numharm);
+    rc = jerk_polish_rzw(p, spectrum, numdata, numharm, rin, zin, win, lpf, &rzw_out[0],
+                         &rzw_out[1], &rzw_out[2], nullptr);
+    if (rc != JERK_OK)
+        return rc;
+    for (int i = 0; i < numharm; i++) {
+        const int hh = i + 1;
+        r[i] = rzw_out[0] * hh;
+        z[i] = rzw_out[1] * hh;
+        w[i] = rzw_out[2] * hh;
+    }
+    rc = jerk_local_power(p, spectrum, numdata, numharm, r, z, w, lp);
+    if (rc != JERK_OK)
+        return rc;
+    for (int i = 0; i < numharm; i++)
+        lp[i] = (double)(float)lp[i];  // a float there, as the reference holds it
+    return jerk_derivs(p, spectrum, numdata, numharm, r, z, w, lp, derivs);
+}

@@ -113,7 +113,8 @@ EXPORTS = [
     "jerk_server_destroy", "jerk_realfft_scratch_bytes", "jerk_realfft",
     "jerk_deredden_scratch_bytes", "jerk_deredden", "jerk_spectrum_scratch_bytes",
     "jerk_spectrum_from_timeseries", "jerk_polisher_create", "jerk_polisher_destroy",
-    "jerk_polish_rzw", "jerk_zap_birdies",
+    "jerk_polish_rzw", "jerk_zap_birdies", "jerk_local_power", "jerk_derivs",
+    "jerk_optimize_cand",
 ]
 
 
@@ -189,6 +190,12 @@ def lib() -> C.CDLL:
         getattr(L, f).argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
                                   C.c_void_p]
     L.jerk_deredden.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
+    L.jerk_local_power.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]
+    L.jerk_derivs.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.jerk_optimize_cand.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_double,
+                                     C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jerk_zap_birdies.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p,
                                    C.c_void_p, C.c_int, C.c_void_p]
     L.jerk_polisher_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p]
@@ -358,6 +365,11 @@ def spectrum_from_timeseries(ts, out=None):
                        ts.numel(), out)
 
 
+RDERIVS_DTYPE = np.dtype([("pow", np.float64), ("phs", np.float64), ("dpow", np.float64),
+                          ("dphs", np.float64), ("d2pow", np.float64), ("d2phs", np.float64),
+                          ("locpow", np.float64)])
+
+
 class Polisher:
     """Candidate polishing on the GPU (jerk_polish_rzw): the volume search of
     the reference's harmonic polishing (src/maximize_rzw.c:84-190)."""
@@ -377,6 +389,28 @@ class Polisher:
                                      lp.ctypes.data, C.byref(ro), C.byref(zo), C.byref(wo),
                                      C.byref(mp)))
         return ro.value, zo.value, wo.value, mp.value
+
+    def optimize(self, spectrum: np.ndarray, numharm: int, r: float, z: float, w: float):
+        """The reference's default candidate optimisation wholly on the GPU
+        (jerk_optimize_cand): ((r, z, w) polished, r relative to the
+        spectrum's bin 0; the per-harmonic derivatives, RDERIVS_DTYPE; the
+        local powers the volume search used)."""
+        spec = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        rzw = np.zeros(3)
+        d = np.zeros(numharm, dtype=RDERIVS_DTYPE)
+        lp = np.zeros(numharm, dtype=np.float32)
+        _check(lib().jerk_optimize_cand(self.ptr, spec.ctypes.data, len(spec), numharm, r, z, w,
+                                        rzw.ctypes.data, d.ctypes.data, lp.ctypes.data))
+        return tuple(float(v) for v in rzw), d, lp
+
+    def local_power(self, spectrum: np.ndarray, r, z, w) -> np.ndarray:
+        """get_localpower3d at the given points (jerk_local_power)."""
+        spec = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        r, z, w = (np.ascontiguousarray(v, dtype=np.float64) for v in (r, z, w))
+        out = np.zeros(len(r))
+        _check(lib().jerk_local_power(self.ptr, spec.ctypes.data, len(spec), len(r), r.ctypes.data,
+                                      z.ctypes.data, w.ctypes.data, out.ctypes.data))
+        return out
 
     def close(self):
         if self.ptr:

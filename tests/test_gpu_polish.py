@@ -115,3 +115,61 @@ def test_polish_rejects_before_device_work():
         pol.polish(spec, 2, 0.2, 0.0, 0.0, [1.0, 1.0])
     assert ei.value.code == jerk.JERK_EINVAL
     pol.close()
+
+
+def _ref_optimize(ref, nh, r, z, w, power=20.0):
+    """The reference's optimize_accelcand on one candidate: (r, z, w) of the
+    fundamental (r absolute) and its per-harmonic derivatives."""
+    import ctypes as C
+
+    f = ob._ref().ref_optimize_cand
+    f.argtypes = [C.c_void_p, C.c_float, C.c_int, C.c_double, C.c_double, C.c_double,
+                  C.c_void_p, C.POINTER(C.c_float)]
+    out = np.zeros(11 * nh)
+    sig = C.c_float()
+    assert f(ref.ctx, power, nh, r, z, w, out.ctypes.data, C.byref(sig)) == 0
+    o = out.reshape(nh, 11)
+    return (o[0, 1], o[0, 2], o[0, 3]), o[:, 4:11]
+
+
+def test_optimize_wholly_on_gpu_matches_reference(tmp_path):
+    """jerk_optimize_cand -- local powers, the volume search and the peak
+    derivatives all on the GPU -- against the reference's optimize_accelcand
+    on the golden small-problem candidates.
+
+    Tolerances: polished r, z, w equal; power at the peak and local power to
+    2e-5 relative (FP32 rounding of the interpolations, whose responses come
+    from FFTs of other rounding); phase to 1e-4 rad; the finite differences
+    (steps of 0.003 bins) amplify that rounding by 1 / 0.006 and
+    1 / 0.000036, so dpow to 1e-3 and d2pow to 0.1 of the power (the
+    reference's own float interpolations carry noise of that order)."""
+    spec, N, dt = synth.small_spectrum()
+    root = str(tmp_path / "small")
+    synth.write_fft(root, spec, N, dt)
+    g = H.golden("small_cands.json")
+    ref = ob.RefSearch(root + ".fft", g["args"])
+    lobin = ref.obs.lobin
+    pol = jerk.Polisher()
+    worst = {"pow": 0.0, "locpow": 0.0, "phs": 0.0, "dpow": 0.0, "d2pow": 0.0}
+    for c in g["cands"]:
+        nh, r, z, w = int(c[2]), c[3], c[4], c[5]
+        (rr, zz, ww), want = _ref_optimize(ref, nh, r, z, w)
+        (gr, gz, gw), got, _ = pol.optimize(spec, nh, r - lobin, z, w)
+        assert (gr + lobin, gz, gw) == (rr, zz, ww), (c, (gr + lobin, gz, gw), (rr, zz, ww))
+        for h in range(nh):
+            p = want[h, 0]
+            e_pow = abs(got["pow"][h] - p) / p
+            e_lp = abs(got["locpow"][h] - want[h, 6]) / want[h, 6]
+            dphs = abs(got["phs"][h] - want[h, 1])
+            e_phs = min(dphs, abs(dphs - 2 * np.pi))
+            e_dp = abs(got["dpow"][h] - want[h, 2]) / p
+            e_d2 = abs(got["d2pow"][h] - want[h, 4]) / p
+            for k, v in (("pow", e_pow), ("locpow", e_lp), ("phs", e_phs), ("dpow", e_dp),
+                         ("d2pow", e_d2)):
+                worst[k] = max(worst[k], v)
+            assert e_pow <= 2e-5 and e_lp <= 2e-5 and e_phs <= 1e-4, (c, h, e_pow, e_lp, e_phs)
+            assert e_dp <= 1e-3 and e_d2 <= 0.1, (c, h, e_dp, e_d2)
+    pol.close()
+    ref.close()
+    print("worst GPU-optimisation differences vs the reference:",
+          {k: f"{v:.2e}" for k, v in worst.items()})
