@@ -223,8 +223,14 @@ int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
  * takes the first strict maximum; *rout, *zout, *wout are the polished
  * fundamental values as the reference computes them, *maxpow the summed
  * power there.
- *   spectrum  numdata complex64 values on the HOST (the searched spectrum;
- *             value 0 is obs.lobin), read around each harmonic only
+ *   spectrum  numdata complex64 values (the searched spectrum; value 0 is
+ *             obs.lobin), read around each harmonic only: on the host (the
+ *             reference's obs->fft), or in device memory, where a kernel
+ *             gathers the windows and nothing of the spectrum crosses PCIe
+ *             (the polisher asks the driver which; a device spectrum must be
+ *             complete when the call is made, or written on its stream).
+ *             The same holds for jerk_local_power, jerk_derivs and
+ *             jerk_optimize_cand below.
  *   rin       the candidate's r minus obs.lobin; zin, win its z and w
  *   locpow    numharm floats: get_localpower3d (src/characteristics.c:75-135)
  *             of harmonic n = numharm - i at (n rin, n zin, n win), as float

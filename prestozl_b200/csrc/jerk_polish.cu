@@ -507,6 +507,41 @@ long long next2(long long x)
     return n;
 }
 
+// One run of spectrum values read from a spectrum held on the device:
+// count values from index src (zero outside [0, numdata)) to dst[off] with
+// dst = the windows, or the answers where to_ans is set.
+struct WinSeg {
+    long long src, off;
+    int count, to_ans;
+};
+
+constexpr int kGatherThreads = 128;
+
+__global__ void __launch_bounds__(kGatherThreads)
+gather_windows_kernel(const float2 *__restrict__ spec, long long numdata,
+                      const WinSeg *__restrict__ segs, float2 *__restrict__ win,
+                      float2 *__restrict__ ans)
+{
+    const WinSeg s = segs[blockIdx.x];
+    float2 *dst = (s.to_ans ? ans : win) + s.off;
+    for (int i = threadIdx.x; i < s.count; i += kGatherThreads) {
+        const long long b = s.src + i;
+        dst[i] = (b >= 0 && b < numdata) ? spec[b] : make_float2(0.f, 0.f);
+    }
+}
+
+// Where the spectrum lives: device (or managed) memory is read on the GPU by
+// gather_windows_kernel, anything else on the host.
+bool spectrum_on_device(const void *spectrum)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, spectrum) != cudaSuccess) {
+        cudaGetLastError();  // a plain host pointer on an old runtime
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 }  // namespace
 }  // namespace jerk
 
@@ -527,6 +562,8 @@ struct jerk_polisher {
     PolishRow *d_rows = nullptr;
     int *d_lists = nullptr;
     long long rows_cap = 0, lists_cap = 0;
+    WinSeg *d_segs = nullptr;  // window runs of a spectrum held on the device
+    long long segs_cap = 0;
     PolishHarm *d_harms = nullptr;
     int *d_best = nullptr;
     float *d_bestpow = nullptr;
@@ -616,6 +653,7 @@ extern "C" void jerk_polisher_destroy(jerk_polisher *p)
     cudaFree(p->tails);
     cudaFree(p->d_rows);
     cudaFree(p->d_lists);
+    cudaFree(p->d_segs);
     cudaFree(p->d_harms);
     cudaFree(p->d_best);
     cudaFree(p->d_bestpow);
@@ -775,10 +813,14 @@ extern "C" int jerk_polish_rzw(jerk_polisher *p, const void *spectrum, long long
     const int nzr = P.nzr;
     const int *mfirst = P.mfirst, *mcount = P.mcount, *maxkern = P.maxkern;
 
-    // ---- staging: rows | lists | harms | data windows (zero outside the spectrum)
+    // ---- staging: rows | lists | harms | data windows (zero outside the
+    // spectrum), or for a spectrum on the device the windows' runs in it
+    const bool dev = spectrum_on_device(spectrum);
     const size_t b_rows = sizeof(PolishRow) * nrows, b_lists = sizeof(int) * lists.size();
-    const size_t b_harms = sizeof(PolishHarm) * numharm, b_win = sizeof(float2) * win_len;
-    const long long stage = (long long)(b_rows + b_lists + b_harms + b_win);
+    const size_t b_harms = sizeof(PolishHarm) * numharm;
+    const size_t b_win = dev ? sizeof(WinSeg) * numharm : sizeof(float2) * win_len;
+    const size_t o_win = (b_rows + b_lists + b_harms + 15) & ~(size_t)15;
+    const long long stage = (long long)(o_win + b_win);
     cudaError_t e = cudaSuccess;
     if (stage > p->stage_cap) {
         if (p->h_stage)
@@ -797,7 +839,8 @@ extern "C" int jerk_polish_rzw(jerk_polisher *p, const void *spectrum, long long
     memcpy(hs, rows.data(), b_rows);
     memcpy(hs + b_rows, lists.data(), b_lists);
     memcpy(hs + b_rows + b_lists, H.data(), b_harms);
-    float2 *hw = (float2 *)(hs + b_rows + b_lists + b_harms);
+    float2 *hw = (float2 *)(hs + o_win);
+    WinSeg *hseg = (WinSeg *)hw;
     for (int hind = 0; hind < numharm; hind++) {
         const PolishHarm &h = H[hind];
         const int n = numharm - hind;
@@ -805,6 +848,10 @@ extern "C" int jerk_polish_rzw(jerk_polisher *p, const void *spectrum, long long
         modf(rin * n, &rh_int);
         const long long begin = (long long)rh_int - 1 - h.khw;
         const int nb = h.fftlen / kNb;
+        if (dev) {
+            hseg[hind] = WinSeg{begin, h.win, nb, 0};
+            continue;
+        }
         for (int i = 0; i < nb; i++) {
             const long long b = begin + i;
             hw[h.win + i] = (b >= 0 && b < numdata) ? data[b] : make_float2(0.f, 0.f);
@@ -816,7 +863,8 @@ extern "C" int jerk_polish_rzw(jerk_polisher *p, const void *spectrum, long long
         (e = grow(&p->terms, &p->terms_cap, nrows * kNumR)) != cudaSuccess ||
         (e = grow(&p->tails, &p->tails_cap, nrows * kTail)) != cudaSuccess ||
         (e = grow(&p->d_rows, &p->rows_cap, nrows)) != cudaSuccess ||
-        (e = grow(&p->d_lists, &p->lists_cap, (long long)lists.size())) != cudaSuccess)
+        (e = grow(&p->d_lists, &p->lists_cap, (long long)lists.size())) != cudaSuccess ||
+        (dev && (e = grow(&p->d_segs, &p->segs_cap, (long long)numharm)) != cudaSuccess))
         return p_cuda(e, "jerk_polish_rzw: device buffers");
     cudaStream_t st = p->stream;
     e = cudaMemcpyAsync(p->d_rows, hs, b_rows, cudaMemcpyHostToDevice, st);
@@ -825,7 +873,13 @@ extern "C" int jerk_polish_rzw(jerk_polisher *p, const void *spectrum, long long
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(p->d_harms, hs + b_rows + b_lists, b_harms, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(p->windows, hw, b_win, cudaMemcpyHostToDevice, st);
+        e = cudaMemcpyAsync(dev ? (void *)p->d_segs : (void *)p->windows, hw, b_win,
+                            cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && dev) {
+        gather_windows_kernel<<<numharm, kGatherThreads, 0, st>>>(data, numdata, p->d_segs,
+                                                                  p->windows, nullptr);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess)
         return p_cuda(e, "jerk_polish_rzw: upload");
 
@@ -1103,11 +1157,13 @@ int interp_points(jerk_polisher *p, const float2 *data, long long numdata, int n
                   const double *r, const double *z, const double *w, const int *khw,
                   float2 *ans)
 {
+    const bool dev = spectrum_on_device(data);
     std::vector<InterpPoint> pts(n);
     std::vector<int> zr, wl[kNumSizes];
     int maxkern[kNumSizes] = {};
     long long win_len = 0;
     std::vector<long long> first(n, 0);
+    std::vector<WinSeg> segs;  // a spectrum on the device: the runs to read
     for (int i = 0; i < n; i++) {
         ans[i] = make_float2(0.f, 0.f);
         pts[i].numkern = 0;
@@ -1117,12 +1173,17 @@ int interp_points(jerk_polisher *p, const float2 *data, long long numdata, int n
         const double frac = modf(r[i], &ip);
         const long long intfreq = (long long)ip;
         if (fabs(w[i]) < 1e-4 && fabs(z[i]) < 1e-4) {
-            if (frac < 1e-5) {
-                ans[i] = data[intfreq];
-                continue;
-            }
-            if ((1.0 - frac) < 1e-5) {
-                ans[i] = data[intfreq + 1];
+            // on a bin: the value itself
+            long long b = -1;
+            if (frac < 1e-5)
+                b = intfreq;
+            else if ((1.0 - frac) < 1e-5)
+                b = intfreq + 1;
+            if (b >= 0) {
+                if (dev)
+                    segs.push_back(WinSeg{b, i, 1, 1});
+                else
+                    ans[i] = data[b];
                 continue;
             }
         }
@@ -1154,11 +1215,18 @@ int interp_points(jerk_polisher *p, const float2 *data, long long numdata, int n
         lists.insert(lists.end(), wl[s].begin(), wl[s].end());
         wcount[s] = (int)wl[s].size();
     }
-    if (lists.empty())
+    if (lists.empty() && segs.empty())
         return JERK_OK;
+    const size_t nbin = segs.size();  // answers that are bin values
+    if (dev)
+        for (int i : lists)
+            segs.push_back(WinSeg{first[i], pts[i].win, pts[i].numkern, 0});
+    // staging: points | lists | windows, or their runs | answers
     const size_t b_pts = sizeof(InterpPoint) * n, b_lists = sizeof(int) * lists.size();
-    const size_t b_win = sizeof(float2) * win_len, b_ans = sizeof(float2) * n;
-    const long long stage = (long long)(b_pts + b_lists + b_win + b_ans);
+    const size_t o_win = (b_pts + b_lists + 15) & ~(size_t)15;
+    const size_t b_win = dev ? sizeof(WinSeg) * segs.size() : sizeof(float2) * win_len;
+    const size_t o_ans = (o_win + b_win + 15) & ~(size_t)15, b_ans = sizeof(float2) * n;
+    const long long stage = (long long)(o_ans + b_ans);
     cudaError_t e = cudaStreamSynchronize(p->stream);
     if (e == cudaSuccess && stage > p->stage_cap) {
         if (p->h_stage)
@@ -1174,27 +1242,37 @@ int interp_points(jerk_polisher *p, const float2 *data, long long numdata, int n
     unsigned char *hs = p->h_stage;
     memcpy(hs, pts.data(), b_pts);
     memcpy(hs + b_pts, lists.data(), b_lists);
-    float2 *hw = (float2 *)(hs + b_pts + b_lists);
-    for (int i = 0; i < n; i++)
-        for (int k = 0; k < pts[i].numkern; k++) {
-            const long long b = first[i] + k;
-            hw[pts[i].win + k] = (b >= 0 && b < numdata) ? data[b] : make_float2(0.f, 0.f);
-        }
+    float2 *hw = (float2 *)(hs + o_win);
+    if (dev)
+        memcpy(hw, segs.data(), b_win);
+    else
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < pts[i].numkern; k++) {
+                const long long b = first[i] + k;
+                hw[pts[i].win + k] = (b >= 0 && b < numdata) ? data[b] : make_float2(0.f, 0.f);
+            }
     // device layout in the polisher's buffers: points in d_rows, lists in
     // d_lists, windows in windows, answers in dfft
     const long long rows_need = (long long)((b_pts + sizeof(PolishRow) - 1) / sizeof(PolishRow));
     if ((e = grow(&p->d_rows, &p->rows_cap, rows_need)) != cudaSuccess ||
         (e = grow(&p->d_lists, &p->lists_cap, (long long)lists.size())) != cudaSuccess ||
         (e = grow(&p->windows, &p->win_cap, std::max(win_len, 1LL))) != cudaSuccess ||
-        (e = grow(&p->dfft, &p->dfft_cap, (long long)n)) != cudaSuccess)
+        (e = grow(&p->dfft, &p->dfft_cap, (long long)n)) != cudaSuccess ||
+        (dev && (e = grow(&p->d_segs, &p->segs_cap, (long long)segs.size())) != cudaSuccess))
         return p_cuda(e, "rzw_interp: device buffers");
     cudaStream_t st = p->stream;
     const InterpPoint *d_pts = (const InterpPoint *)p->d_rows;
     e = cudaMemcpyAsync(p->d_rows, hs, b_pts, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && b_lists)
         e = cudaMemcpyAsync(p->d_lists, hs + b_pts, b_lists, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && b_win)
-        e = cudaMemcpyAsync(p->windows, hw, b_win, cudaMemcpyHostToDevice, st);
+        e = cudaMemcpyAsync(dev ? (void *)p->d_segs : (void *)p->windows, hw, b_win,
+                            cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && dev) {
+        gather_windows_kernel<<<(int)segs.size(), kGatherThreads, 0, st>>>(
+            data, numdata, p->d_segs, p->windows, p->dfft);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess && !zr.empty()) {
         interp_zr_kernel<<<(int)zr.size(), kInterpThreads, 0, st>>>(d_pts, p->d_lists, p->windows,
                                                                      p->dfft);
@@ -1205,7 +1283,7 @@ int interp_points(jerk_polisher *p, const float2 *data, long long numdata, int n
             e = p_dispatch<PI>(kSizes[s], d_pts, (const int *)p->d_lists + wfirst[s], wcount[s],
                                (const float2 *)(p->tw + p->twoff[s]), (const float2 *)p->windows,
                                p->dfft, maxkern[s], st);
-    float2 *hans = (float2 *)(hs + b_pts + b_lists + b_win);
+    float2 *hans = (float2 *)(hs + o_ans);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(hans, p->dfft, b_ans, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)
@@ -1215,6 +1293,8 @@ int interp_points(jerk_polisher *p, const float2 *data, long long numdata, int n
     for (int i = 0; i < n; i++)
         if (pts[i].numkern)
             ans[i] = hans[i];
+    for (size_t j = 0; j < nbin; j++)
+        ans[segs[j].off] = hans[segs[j].off];
     return JERK_OK;
 }
 

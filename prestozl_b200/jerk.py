@@ -378,14 +378,30 @@ class Polisher:
         self.ptr = C.c_void_p()
         _check(lib().jerk_polisher_create(C.byref(self.ptr), None))
 
+    @staticmethod
+    def _spectrum(spectrum):
+        """(pointer, numdata, keepalive): a numpy spectrum is read on the host;
+        a complex64 CUDA tensor on the GPU, once the work that wrote it on
+        torch's current stream has finished (the polisher has its own
+        stream)."""
+        if getattr(spectrum, "is_cuda", False):
+            import torch
+
+            if spectrum.dtype != torch.complex64 or not spectrum.is_contiguous():
+                raise JerkError(JERK_EINVAL, "polisher: expects a contiguous complex64 tensor")
+            torch.cuda.current_stream(spectrum.device).synchronize()
+            return C.c_void_p(spectrum.data_ptr()), spectrum.numel(), spectrum
+        a = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        return C.c_void_p(a.ctypes.data), len(a), a
+
     def polish(self, spectrum: np.ndarray, numharm: int, r: float, z: float, w: float,
                locpow) -> Tuple[float, float, float, float]:
         """(r, z, w, summed power) polished; r relative to the spectrum's bin
         0; locpow[i] the local power of harmonic numharm - i."""
-        spec = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        sp, n, _keep = self._spectrum(spectrum)
         lp = np.ascontiguousarray(locpow, dtype=np.float32)
         ro, zo, wo, mp = C.c_double(), C.c_double(), C.c_double(), C.c_float()
-        _check(lib().jerk_polish_rzw(self.ptr, spec.ctypes.data, len(spec), numharm, r, z, w,
+        _check(lib().jerk_polish_rzw(self.ptr, sp, n, numharm, r, z, w,
                                      lp.ctypes.data, C.byref(ro), C.byref(zo), C.byref(wo),
                                      C.byref(mp)))
         return ro.value, zo.value, wo.value, mp.value
@@ -395,20 +411,20 @@ class Polisher:
         (jerk_optimize_cand): ((r, z, w) polished, r relative to the
         spectrum's bin 0; the per-harmonic derivatives, RDERIVS_DTYPE; the
         local powers the volume search used)."""
-        spec = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        sp, n, _keep = self._spectrum(spectrum)
         rzw = np.zeros(3)
         d = np.zeros(numharm, dtype=RDERIVS_DTYPE)
         lp = np.zeros(numharm, dtype=np.float32)
-        _check(lib().jerk_optimize_cand(self.ptr, spec.ctypes.data, len(spec), numharm, r, z, w,
+        _check(lib().jerk_optimize_cand(self.ptr, sp, n, numharm, r, z, w,
                                         rzw.ctypes.data, d.ctypes.data, lp.ctypes.data))
         return tuple(float(v) for v in rzw), d, lp
 
     def local_power(self, spectrum: np.ndarray, r, z, w) -> np.ndarray:
         """get_localpower3d at the given points (jerk_local_power)."""
-        spec = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        sp, n, _keep = self._spectrum(spectrum)
         r, z, w = (np.ascontiguousarray(v, dtype=np.float64) for v in (r, z, w))
         out = np.zeros(len(r))
-        _check(lib().jerk_local_power(self.ptr, spec.ctypes.data, len(spec), len(r), r.ctypes.data,
+        _check(lib().jerk_local_power(self.ptr, sp, n, len(r), r.ctypes.data,
                                       z.ctypes.data, w.ctypes.data, out.ctypes.data))
         return out
 

@@ -173,3 +173,36 @@ def test_optimize_wholly_on_gpu_matches_reference(tmp_path):
     ref.close()
     print("worst GPU-optimisation differences vs the reference:",
           {k: f"{v:.2e}" for k, v in worst.items()})
+
+
+def test_device_spectrum_equals_host_spectrum(tmp_path):
+    """The polisher on a spectrum held in device memory (a CUDA tensor: a
+    kernel gathers the windows) gives the same bits as on the same spectrum
+    in host memory: golden candidates, candidates at the spectrum's two ends
+    (windows reaching past them read zeros) and local powers on bin values
+    (z = w = 0 at whole r, answered by the values themselves)."""
+    torch = pytest.importorskip("torch")
+    spec, N, dt = synth.small_spectrum()
+    root = str(tmp_path / "small")
+    synth.write_fft(root, spec, N, dt)
+    g = H.golden("small_cands.json")
+    ref = ob.RefSearch(root + ".fft", g["args"])
+    lobin = ref.obs.lobin
+    ref.close()
+    n = len(spec)
+    dspec = torch.from_numpy(spec).cuda()
+    pol = jerk.Polisher()
+    cands = [(int(c[2]), c[3] - lobin, c[4], c[5]) for c in g["cands"]]
+    cands += [(2, 3.0, 0.0, 0.0), (1, 40.5, 2.0, -20.0), (1, n - 30.5, -4.0, 20.0)]
+    for nh, r, z, w in cands:
+        h_rzw, h_d, h_lp = pol.optimize(spec, nh, r, z, w)
+        d_rzw, d_d, d_lp = pol.optimize(dspec, nh, r, z, w)
+        assert h_rzw == d_rzw, (nh, r, z, w)
+        assert h_d.tobytes() == d_d.tobytes() and h_lp.tobytes() == d_lp.tobytes()
+        assert pol.polish(spec, nh, r, z, w, h_lp) == pol.polish(dspec, nh, r, z, w, h_lp)
+    r = np.array([0.0, 1.0, 17.0, 1000.0, n - 25.0, n - 1.0, 5.5, n + 3.0])
+    zw = np.zeros_like(r)
+    assert np.array_equal(pol.local_power(spec, r, zw, zw), pol.local_power(dspec, r, zw, zw))
+    with pytest.raises(jerk.JerkError):
+        pol.optimize(dspec.view(torch.float32), 1, 1000.0, 0.0, 0.0)
+    pol.close()
