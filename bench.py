@@ -218,6 +218,82 @@ def input_prep_leg(device, reps: int = 5):
                     "bytes; one-off per series (about 0.02 % of its search)"}
 
 
+def dedisp_leg(device, reps: int = 5, worklen: int = 65536, nsub: int = 64,
+               numdms: int = 512, bs: int = 4):
+    """prepsubband_cu's GPU steps on one block (jerk_downsample_subbands of
+    bs x worklen samples, then jerk_dedisp_subbands into numdms series),
+    inputs in HBM, CUDA events on torch's current stream; beside them the
+    reference's own DownsampDataArray / getDedisp (src/prepsubband_kernels.cu,
+    compiled for sm_100a into oracle/_ref) on the same buffers when present.
+    Offsets follow the cold-plasma law over 1200-1600 MHz for DMs 0..255.5 at
+    dt = 256 us (the largest under a block)."""
+    import ctypes as C
+
+    import torch
+
+    from prestozl_b200 import jerk
+
+    f = 1200.0 + (np.arange(nsub) + 0.5) * 400.0 / nsub
+    dms = 0.5 * np.arange(numdms)
+    off = np.rint(4.148808e3 * dms[:, None] * (f[None, :] ** -2 - f[-1] ** -2) / 256e-6)
+    off = np.minimum(off, worklen).astype(np.int32)
+    g = torch.Generator(device=device)
+    g.manual_seed(12)
+    raw = torch.randn((worklen * bs, nsub), device=device, generator=g)
+    cur = torch.randn((worklen, nsub), device=device, generator=g)
+    last = torch.randn((worklen, nsub), device=device, generator=g)
+    ds = torch.empty((worklen, nsub), device=device)
+    out = torch.empty((numdms, worklen), device=device)
+    dd = jerk.Dedisperser(worklen, nsub, off)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_ds = timed(lambda: jerk.downsample_subbands(raw, bs, out=ds))
+    ms_dd = timed(lambda: dd(cur, last, out=out))
+    shape = dd.shape
+    dd.close()
+    adds = float(numdms) * worklen * nsub
+    dd_bytes = 4.0 * (2 * worklen * nsub + numdms * worklen)
+    ds_bytes = 4.0 * (worklen * bs * nsub + worklen * nsub)
+    res = {"worklen": worklen, "nsub": nsub, "numdms": numdms, "downsamp": bs,
+           "tiling_dms_x_samples": list(shape),
+           "dedisp_ms": ms_dd, "dedisp_gadds_per_s": adds / ms_dd / 1e6,
+           "dedisp_algorithmic_bytes": dd_bytes, "dedisp_achieved_gbs": dd_bytes / ms_dd / 1e6,
+           "downsample_ms": ms_ds, "downsample_achieved_gbs": ds_bytes / ms_ds / 1e6,
+           "bound": "dedisp: shared-memory loads (1.25 per add); downsample: HBM"}
+    try:
+        from oracle import bindings as ob
+
+        path = getattr(ob, "REF_DEDISP_GPU_LIB", "")
+        if os.path.exists(path):
+            lib = C.CDLL(path)
+            lib.DownsampDataArray.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+            lib.getDedisp.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                      C.c_int, C.c_void_p]
+            doff = torch.from_numpy(off).to(device)
+            ref = torch.empty_like(out)
+            res["reference_downsample_ms"] = timed(lambda: lib.DownsampDataArray(
+                ds.data_ptr(), raw.data_ptr(), worklen, bs, nsub))
+            res["reference_dedisp_ms"] = timed(lambda: lib.getDedisp(
+                cur.data_ptr(), last.data_ptr(), ref.data_ptr(), worklen, nsub, numdms,
+                doff.data_ptr()))
+            torch.cuda.synchronize()
+            res["equal_to_reference"] = bool(torch.equal(ref, out))
+    except OSError as e:
+        res["reference"] = f"not loaded: {e}"
+    return res
+
+
 def polish_leg(spec_np, cands, max_cands: int = 64):
     """GPU polishing (jerk_polish_rzw) of a search's final candidates.  The
     local powers only scale the per-harmonic sums, so 1.0 is passed: the
@@ -269,7 +345,9 @@ def run_extras(args):
     pol = polish_leg(spec_np, cands, max_cands=len(cands))
     prep = input_prep_leg("cuda", reps=args.extras_reps)
     prep["frac_of_hbm"] = prep["achieved_gbs"] / peaks()[0]
-    print(json.dumps({"impl": "ours", "mode": "extras-only", "input_prep": prep, "polish": pol}))
+    dedisp = dedisp_leg("cuda", reps=args.extras_reps)
+    print(json.dumps({"impl": "ours", "mode": "extras-only", "input_prep": prep, "polish": pol,
+                      "dedisp": dedisp}))
 
 
 def reference_gpu(spec_np):
@@ -392,6 +470,9 @@ def main():
                     help="skip the input-preparation and candidate-polishing legs")
     ap.add_argument("--extras-only", action="store_true",
                     help="only the input-preparation and polishing legs (small footprint)")
+    ap.add_argument("--dedisp-only", action="store_true",
+                    help="only the subband-dedispersion leg (one block; the form profiled "
+                         "with ncu)")
     ap.add_argument("--extras-cands", type=int, default=4,
                     help="--extras-only: candidates per harmonic count (16, 8, 4, 2)")
     ap.add_argument("--extras-reps", type=int, default=5,
@@ -407,6 +488,16 @@ def main():
 
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.dedisp_only:
+        import torch
+
+        from prestozl_b200 import build
+
+        build.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"impl": "ours", "mode": "dedisp-only",
+                          "dedisp": dedisp_leg("cuda", reps=args.extras_reps)}))
         return
     if args.extras_only:
         run_extras(args)
@@ -600,6 +691,7 @@ def main():
     if not args.no_extras:
         extras["input_prep"] = input_prep_leg("cuda")
         extras["input_prep"]["frac_of_hbm"] = extras["input_prep"]["achieved_gbs"] / peaks()[0]
+        extras["dedisp"] = dedisp_leg("cuda")
         spec0_np = specs[0].cpu().numpy()
         extras["polish"] = polish_leg(spec0_np, cands0)
     timed_spectra = args.steps * (2 if served else 1)

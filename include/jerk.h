@@ -324,6 +324,41 @@ long long jerk_spectrum_scratch_bytes(long long n);
 int jerk_spectrum_from_timeseries(const float *timeseries, long long n, void *spectrum,
                                   void *scratch, long long scratch_bytes, void *stream);
 
+/* Subband dedispersion: the GPU steps of prepsubband_cu, which makes the DM
+ * trials' time series that the search takes (src/prepsubband_cu.c:1140-1165).
+ * Data are blocks of worklen samples of nsub subbands, time-major
+ * ([t][s], subband fastest), float32, on the device.
+ *
+ * jerk_downsample_subbands replaces DownsampDataArray
+ * (src/prepsubband_kernels.cu:23-46, 76-80): out[t][s] = the mean of
+ * in[t bs + k][s] over k < bs, for t < worklen (the output length).
+ *
+ * jerk_dedisp_subbands replaces getDedisp (src/prepsubband_kernels.cu:48-74,
+ * 82-87; the CPU form float_dedisp, src/dispersion.c:208-231): out[dm][t]
+ * (numdms rows of worklen) = the sum over s of x[t + offsets[dm][s]][s], where
+ * x is last (the previous block) followed by cur (this one).  The offsets
+ * (prepsubband_cu's offsets[numdms][nsub], in downsampled samples, each in
+ * [0, worklen]) are fixed for a run, so they are given once, on the host or
+ * the device (getDedisp's offsets_gpu), to jerk_dedisperser_create, which
+ * checks them and plans the tiling.  jerk_dedisperser_matches returns 1 when
+ * a dedisperser was made for these sizes and offsets.
+ *
+ * Both sum in the reference's order in FP32, bit-exact with the reference.
+ * Asynchronous on stream (NULL: the legacy default stream, as the reference
+ * launches); no allocation per call. */
+int jerk_downsample_subbands(float *out, const float *in, int worklen, int bs, int nsub,
+                             void *stream);
+typedef struct jerk_dedisperser jerk_dedisperser;
+int jerk_dedisperser_create(jerk_dedisperser **dedisperser, int worklen, int nsub, int numdms,
+                            const int *offsets);
+void jerk_dedisperser_destroy(jerk_dedisperser *dedisperser);
+/* the tiling chosen: DMs per CTA group and samples per tile */
+int jerk_dedisperser_shape(const jerk_dedisperser *dedisperser, int *group_dms, int *tile_samples);
+int jerk_dedisperser_matches(const jerk_dedisperser *dedisperser, int worklen, int nsub, int numdms,
+                             const int *offsets);
+int jerk_dedisp_subbands(jerk_dedisperser *dedisperser, const float *cur, const float *last,
+                         float *out, void *stream);
+
 /* The served form: a request loop on one GPU (continuous batching).
  * Submitted spectra wait in a queue; a worker thread that owns the device
  * admits them while fewer than max_active searches run and their device

@@ -26,6 +26,8 @@ REF_CLI = os.path.join(REF_DIR, "accelsearch")
 DROPIN_CLI = os.path.join(REF_DIR, "accelsearch_b200")
 DROPIN_MANY_CLI = os.path.join(REF_DIR, "accelsearch_b200_many")
 REFGPU_CLI = os.path.join(REF_DIR, "accelsearch_refgpu")
+REF_DEDISP_GPU_LIB = os.path.join(REF_DIR, "libprestodedisp_gpu.so")
+PREPSUBBAND_DROPIN_LIB = os.path.join(REF_DIR, "libprepsubband_dropin.so")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REFERENCE_SOURCES = "/root/reference"
 
@@ -35,7 +37,7 @@ def build(reference: Optional[bool] = None) -> None:
     reference sources are present)."""
     if reference is None:
         reference = os.path.isdir(os.path.join(REFERENCE_SOURCES, "src"))
-    targets = ["oracle"] + (["ref", "dropin", "refgpu"] if reference else [])
+    targets = ["oracle"] + (["ref", "dropin", "refgpu", "dedispgpu"] if reference else [])
     subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
 
 
@@ -301,6 +303,10 @@ def _orc():
         lib.orc_calc_required_r.argtypes = [C.c_double, C.c_double]
         lib.orc_calc_required_z.argtypes = [C.c_double, C.c_double]
         lib.orc_calc_required_w.argtypes = [C.c_double, C.c_double]
+        lib.orc_downsample_subbands.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                C.c_int]
+        lib.orc_dedisp_subbands.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                            C.c_int, C.c_void_p]
         _orclib = lib
     return _orclib
 
@@ -413,6 +419,40 @@ def pair_magnitude(packed: np.ndarray) -> np.ndarray:
     FFT leaves in bin k."""
     a = np.abs(np.asarray(packed))
     return a + np.concatenate([a[:1], a[:0:-1]])
+
+
+def downsample_subbands(data: np.ndarray, bs: int) -> np.ndarray:
+    """Subband downsampling (orc_downsample_subbands): data [worklen * bs,
+    nsub] float32, time-major -> [worklen, nsub]."""
+    x = np.ascontiguousarray(data, dtype=np.float32)
+    worklen, nsub = x.shape[0] // bs, x.shape[1]
+    out = np.empty((worklen, nsub), dtype=np.float32)
+    _orc().orc_downsample_subbands(out.ctypes.data, x.ctypes.data, worklen, bs, nsub)
+    return out
+
+
+def dedisp_subbands(cur: np.ndarray, last: np.ndarray, offsets: np.ndarray,
+                    reference: bool = False) -> np.ndarray:
+    """Subband dedispersion of one block: cur and last [worklen, nsub]
+    float32, offsets [numdms, nsub] -> [numdms, worklen].  The oracle's
+    restatement, or with reference=True the reference's own float_dedisp
+    (src/dispersion.c:208-231) once per DM, as prepsubband calls it."""
+    c = np.ascontiguousarray(cur, dtype=np.float32)
+    l = np.ascontiguousarray(last, dtype=np.float32)
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    worklen, nsub = c.shape
+    numdms = off.shape[0]
+    out = np.empty((numdms, worklen), dtype=np.float32)
+    if reference:
+        f = _ref().float_dedisp
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_float, C.c_void_p]
+        for d in range(numdms):
+            f(c.ctypes.data, l.ctypes.data, worklen, nsub, off[d].ctypes.data, 0.0,
+              out[d].ctypes.data)
+    else:
+        _orc().orc_dedisp_subbands(c.ctypes.data, l.ctypes.data, out.ctypes.data, worklen, nsub,
+                                   numdms, off.ctypes.data)
+    return out
 
 
 def invsqrtf(x: float, reference: bool = False) -> float:

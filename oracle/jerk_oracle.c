@@ -961,3 +961,40 @@ void orc_zap_list(float *fft, long numamps, long long N, const double *lobins,
         orc_zapbirds(fft, numamps, lobins[i], hibins[i] >= top ? top - 1 : hibins[i]);
     }
 }
+
+/* Subband downsampling (prepsubband's get_data, src/prepsubband.c:984-1001;
+ * on the GPU DownsampDataArray, src/prepsubband_kernels.cu:23-46): blocks of
+ * worklen output samples of nsub subbands, time-major; each output the FP32
+ * sum of bs consecutive inputs of its subband, in time order, divided by bs. */
+void orc_downsample_subbands(float *out, const float *in, int worklen, int bs, int nsub)
+{
+    for (long t = 0; t < worklen; t++)
+        for (int s = 0; s < nsub; s++) {
+            float acc = 0.0f;
+            for (int k = 0; k < bs; k++)
+                acc += in[((long)t * bs + k) * nsub + s];
+            out[t * nsub + s] = acc / (float)bs;
+        }
+}
+
+/* Subband dedispersion (float_dedisp with approx_mean 0, src/dispersion.c:
+ * 208-231, as prepsubband calls it per DM, src/prepsubband.c:1010-1013): for
+ * DM d, out[d][t] starts at -0.0f and adds, subband by subband in ascending
+ * order, sample t + offsets[d][s] of the previous block (last) followed by
+ * the current one (cur). */
+void orc_dedisp_subbands(const float *cur, const float *last, float *out, int worklen, int nsub,
+                         int numdms, const int *offsets)
+{
+    for (int d = 0; d < numdms; d++) {
+        float *row = out + (long)d * worklen;
+        for (long t = 0; t < worklen; t++)
+            row[t] = -0.0f;
+        for (int s = 0; s < nsub; s++) {
+            const long off = offsets[(long)d * nsub + s];
+            for (long t = 0; t < worklen; t++) {
+                const long tau = t + off;
+                row[t] += tau < worklen ? last[tau * nsub + s] : cur[(tau - worklen) * nsub + s];
+            }
+        }
+    }
+}

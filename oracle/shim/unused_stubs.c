@@ -36,3 +36,18 @@ int transpose_fcomplex(void *a, int nx, int ny, unsigned char *move, int move_si
     unreachable("transpose_fcomplex");
     return 0;
 }
+
+/* src/dispersion.c (linked for float_dedisp) refers to these two from
+ * subband_delays and combine_subbands, which the oracle never calls. */
+double doppler(double freq_observed, double voverc)
+{
+    (void)freq_observed; (void)voverc;
+    unreachable("doppler");
+    return 0.0;
+}
+
+void initialize_foldstats(void *stats)
+{
+    (void)stats;
+    unreachable("initialize_foldstats");
+}

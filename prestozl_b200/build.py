@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["jerk_kernels.cu", "jerk_bank.cu", "jerk_realfft.cu", "jerk_polish.cu", "jerk_plan.cpp", "jerk_server.cpp"]
+SOURCES = ["jerk_kernels.cu", "jerk_bank.cu", "jerk_realfft.cu", "jerk_polish.cu", "jerk_dedisp.cu", "jerk_plan.cpp", "jerk_server.cpp"]
 HEADERS = ["jerk_fft.cuh", "jerk_kernels.cuh", "jerk_resp.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -114,7 +114,9 @@ EXPORTS = [
     "jerk_deredden_scratch_bytes", "jerk_deredden", "jerk_spectrum_scratch_bytes",
     "jerk_spectrum_from_timeseries", "jerk_polisher_create", "jerk_polisher_destroy",
     "jerk_polish_rzw", "jerk_zap_birdies", "jerk_local_power", "jerk_derivs",
-    "jerk_optimize_cand",
+    "jerk_optimize_cand", "jerk_downsample_subbands", "jerk_dedisperser_create",
+    "jerk_dedisperser_destroy", "jerk_dedisperser_shape", "jerk_dedisperser_matches",
+    "jerk_dedisp_subbands",
 ]
 
 
@@ -198,6 +200,16 @@ def lib() -> C.CDLL:
                                      C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     L.jerk_zap_birdies.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p,
                                    C.c_void_p, C.c_int, C.c_void_p]
+    L.jerk_downsample_subbands.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                           C.c_void_p]
+    L.jerk_dedisperser_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int,
+                                          C.c_void_p]
+    L.jerk_dedisperser_destroy.argtypes = [C.c_void_p]
+    L.jerk_dedisperser_destroy.restype = None
+    L.jerk_dedisperser_shape.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.jerk_dedisperser_matches.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    L.jerk_dedisp_subbands.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]
     L.jerk_polisher_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p]
     L.jerk_polisher_destroy.argtypes = [C.c_void_p]
     L.jerk_polisher_destroy.restype = None
@@ -455,6 +467,91 @@ def zap_birdies(spec, N: int, lobins, hibins):
     _check(lib().jerk_zap_birdies(spec.data_ptr(), spec.numel(), N, lo.ctypes.data,
                                   hi.ctypes.data, len(lo), stream or None))
     return spec
+
+
+def _stream_of(t):
+    import torch
+
+    return torch.cuda.current_stream(t.device).cuda_stream or None
+
+
+def _check_subbands(t, what: str):
+    import torch
+
+    if not (getattr(t, "is_cuda", False) and t.dtype == torch.float32 and t.is_contiguous()
+            and t.dim() == 2):
+        raise JerkError(JERK_EINVAL, f"{what}: expects a contiguous 2-D float32 CUDA tensor")
+
+
+def downsample_subbands(data, bs: int, out=None):
+    """prepsubband_cu's DownsampDataArray (jerk_downsample_subbands): data
+    [worklen * bs, nsub] float32 on the GPU, time-major -> [worklen, nsub],
+    each the mean of bs consecutive samples; on torch's current stream."""
+    import torch
+
+    _check_subbands(data, "downsample_subbands")
+    worklen, nsub = data.shape[0] // bs, data.shape[1]
+    if out is None:
+        out = torch.empty((worklen, nsub), dtype=torch.float32, device=data.device)
+    _check_subbands(out, "downsample_subbands")
+    if tuple(out.shape) != (worklen, nsub):
+        raise JerkError(JERK_EINVAL, "downsample_subbands: out must be [worklen, nsub]")
+    _check(lib().jerk_downsample_subbands(C.c_void_p(out.data_ptr()),
+                                          C.c_void_p(data.data_ptr()), worklen, bs, nsub,
+                                          C.c_void_p(_stream_of(data))))
+    return out
+
+
+class Dedisperser:
+    """prepsubband_cu's getDedisp (jerk_dedisp_subbands) for one offsets
+    table: offsets [numdms, nsub] (in samples, each in [0, worklen])."""
+
+    def __init__(self, worklen: int, nsub: int, offsets):
+        off = np.ascontiguousarray(offsets, dtype=np.int32)
+        if off.ndim != 2 or off.shape[1] != nsub:
+            raise JerkError(JERK_EINVAL, "Dedisperser: offsets must be [numdms, nsub]")
+        self.worklen, self.nsub, self.numdms = worklen, nsub, off.shape[0]
+        self.ptr = C.c_void_p()
+        _check(lib().jerk_dedisperser_create(C.byref(self.ptr), worklen, nsub, self.numdms,
+                                             off.ctypes.data_as(C.c_void_p)))
+
+    @property
+    def shape(self) -> Tuple[int, int]:
+        """(DMs per CTA group, samples per tile) that the plan chose."""
+        g, t = C.c_int(), C.c_int()
+        _check(lib().jerk_dedisperser_shape(self.ptr, C.byref(g), C.byref(t)))
+        return g.value, t.value
+
+    def __call__(self, cur, last, out=None):
+        """[numdms, worklen] series from the current and the previous block
+        ([worklen, nsub] each); on torch's current stream."""
+        import torch
+
+        for t in (cur, last):
+            _check_subbands(t, "Dedisperser")
+            if tuple(t.shape) != (self.worklen, self.nsub):
+                raise JerkError(JERK_EINVAL, "Dedisperser: blocks must be [worklen, nsub]")
+        if out is None:
+            out = torch.empty((self.numdms, self.worklen), dtype=torch.float32, device=cur.device)
+        _check_subbands(out, "Dedisperser")
+        if tuple(out.shape) != (self.numdms, self.worklen):
+            raise JerkError(JERK_EINVAL, "Dedisperser: out must be [numdms, worklen]")
+        _check(lib().jerk_dedisp_subbands(self.ptr, C.c_void_p(cur.data_ptr()),
+                                          C.c_void_p(last.data_ptr()),
+                                          C.c_void_p(out.data_ptr()),
+                                          C.c_void_p(_stream_of(cur))))
+        return out
+
+    def close(self):
+        if self.ptr:
+            lib().jerk_dedisperser_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _spectrum_arg(spectrum):

@@ -273,3 +273,34 @@ def test_zapbirds_restatement_matches_reference():
         hi = min(lo + float(rng.uniform(0, 50)), n - 1)
         a, b = ob.zapbirds(spec, lo, hi), ob.zapbirds(spec, lo, hi, reference=True)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (n, lo, hi)
+
+
+@pytest.mark.parametrize("worklen,nsub,numdms", [(1000, 32, 20), (257, 13, 7), (64, 1, 3)])
+def test_dedisp_oracle_equals_reference_float_dedisp(worklen, nsub, numdms):
+    """The oracle's subband dedispersion against the reference's own
+    float_dedisp (src/dispersion.c:208-231), called once per DM as
+    prepsubband does, bitwise; offsets anywhere in [0, worklen]."""
+    if not H.have_ref():
+        pytest.skip("the reference build (oracle/_ref) is the comparator")
+    rng = np.random.default_rng(worklen + nsub)
+    cur = (rng.standard_normal((worklen, nsub)) * 30 + 100).astype(np.float32)
+    last = (rng.standard_normal((worklen, nsub)) * 30 + 100).astype(np.float32)
+    off = rng.integers(0, worklen + 1, (numdms, nsub)).astype(np.int32)
+    off[0] = 0
+    off[-1, 0] = worklen
+    a = ob.dedisp_subbands(cur, last, off)
+    b = ob.dedisp_subbands(cur, last, off, reference=True)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_downsample_oracle_is_the_block_mean():
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((600, 5)).astype(np.float32)
+    got = ob.downsample_subbands(x, 3)
+    want = np.empty((200, 5), dtype=np.float32)
+    for t in range(200):
+        acc = np.zeros(5, dtype=np.float32)
+        for k in range(3):
+            acc = (acc + x[3 * t + k]).astype(np.float32)
+        want[t] = acc / np.float32(3)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
