@@ -195,3 +195,57 @@ def test_dropin_symbols_equal_reference_gpu_kernels():
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     for a, b in zip(res["ref"][1], res["ours"][1]):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_dedispersed_trials_feed_the_search():
+    """prepsubband_cu's GPU steps feeding the search with no file in between.
+    Raw subband blocks carry a pulsar dispersed at DM 100 (1200-1600 MHz, 16
+    subbands, 32 us samples).  Each block is downsampled 2x and dedispersed
+    against the previous one into 9 DM trials (DM 0 to 200), block after
+    block, into 2^20-sample series in HBM.  Each series then goes to the
+    served loop as a time-series request.  The pulsar's best candidate sits
+    at its frequency and is strongest in the DM-100 trial."""
+    nsub, bs, worklen, nblocks = 16, 2, 1 << 16, 16
+    dt_raw, dt = 32e-6, 64e-6
+    dm_true, dms = 100.0, np.arange(9) * 25.0
+    f_psr = 123.4
+    freqs = 1200.0 + (np.arange(nsub) + 0.5) * 400.0 / nsub
+
+    def delay(dm):  # seconds, relative to the top subband
+        return 4.148808e3 * dm * (freqs ** -2 - freqs[-1] ** -2)
+
+    off = np.rint(np.array([delay(dm) for dm in dms]) / dt).astype(np.int32)
+    dd = jerk.Dedisperser(worklen, nsub, off)
+    rng = np.random.default_rng(2024)
+    d_true = delay(dm_true)
+    raw_len = worklen * bs
+    prev = None
+    series = torch.empty((len(dms), nblocks * worklen), dtype=torch.float32, device="cuda")
+    for k in range(nblocks + 1):
+        t = (k * raw_len + np.arange(raw_len))[:, None] * dt_raw - d_true[None, :]
+        sig = sum(a * np.cos(2 * np.pi * h * f_psr * t) for h, a in ((1, 1.0), (2, 0.5), (3, 0.3)))
+        raw = (rng.standard_normal((raw_len, nsub)) + 0.01 * sig).astype(np.float32)
+        ds = jerk.downsample_subbands(torch.from_numpy(raw).cuda(), bs)
+        if prev is not None:
+            series[:, (k - 1) * worklen: k * worklen] = dd(ds, prev)
+        prev = ds
+    torch.cuda.synchronize()
+    dd.close()
+    N = nblocks * worklen
+    srv = jerk.JerkServer(max_active=3, batch=16)
+    for i in range(len(dms)):
+        srv.submit(series[i].contiguous(), N, dt, 20, 60, 8, 2.0, tag=i, timeseries=True)
+    r0 = f_psr * N * dt
+    best = {}
+    for _ in range(len(dms)):
+        tag, cands, _ = srv.poll(120000)
+        near = cands[np.abs(cands["r"] - r0) < 2.0] if len(cands) else cands
+        best[tag] = float(near["sigma"].max()) if len(near) else 0.0
+    st = srv.stats()
+    srv.close()
+    print("best sigma at the pulsar by DM trial:", {float(dms[k]): round(v, 1)
+                                                     for k, v in sorted(best.items())})
+    assert st["failed"] == 0
+    peak = int(np.argmax([best[i] for i in range(len(dms))]))
+    assert dms[peak] == dm_true
+    assert best[peak] > 10.0 and best[peak] > 2 * max(best[0], best[len(dms) - 1])
