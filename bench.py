@@ -691,7 +691,10 @@ def main():
     if not args.no_extras:
         extras["input_prep"] = input_prep_leg("cuda")
         extras["input_prep"]["frac_of_hbm"] = extras["input_prep"]["achieved_gbs"] / peaks()[0]
-        extras["dedisp"] = dedisp_leg("cuda")
+        try:
+            extras["dedisp"] = dedisp_leg("cuda")
+        except Exception as e:  # a side leg: report it, keep the search's line
+            extras["dedisp"] = {"error": f"{type(e).__name__}: {e}"}
         spec0_np = specs[0].cpu().numpy()
         extras["polish"] = polish_leg(spec0_np, cands0)
     timed_spectra = args.steps * (2 if served else 1)
