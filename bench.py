@@ -270,7 +270,8 @@ def dedisp_leg(device, reps: int = 5, worklen: int = 65536, nsub: int = 64,
            "dedisp_ms": ms_dd, "dedisp_gadds_per_s": adds / ms_dd / 1e6,
            "dedisp_algorithmic_bytes": dd_bytes, "dedisp_achieved_gbs": dd_bytes / ms_dd / 1e6,
            "downsample_ms": ms_ds, "downsample_achieved_gbs": ds_bytes / ms_ds / 1e6,
-           "bound": "dedisp: shared-memory loads (1.25 per add); downsample: HBM"}
+           "bound": "dedisp: shared-memory load wavefronts (about 1.03 per 32 adds in the "
+                    "sums, plus the window staging); downsample: HBM"}
     try:
         from oracle import bindings as ob
 

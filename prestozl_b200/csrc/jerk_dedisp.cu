@@ -74,14 +74,20 @@ dedisp_kernel(const float *__restrict__ cur, const float *__restrict__ last,
     }
     // x[tau] = last[tau] for tau < worklen, cur[tau - worklen] after
     const long long tau_end = 2LL * worklen;
+    // (the window stores share the array with lo and base, so the loops
+    // below keep what they need of those in registers)
     if (V == 4) {
         for (int q = 0; q < nsub / 4; q++) {
+            int slo[4], sw[4], sb[4];
             int qlo = INT_MAX, qend = INT_MIN;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int s = 4 * q + j;
-                qlo = min(qlo, lo[s]);
-                qend = max(qend, lo[s] + base[s + 1] - base[s]);
+                slo[j] = lo[s];
+                sb[j] = base[s];
+                sw[j] = base[s + 1] - sb[j];
+                qlo = min(qlo, slo[j]);
+                qend = max(qend, slo[j] + sw[j]);
             }
             for (int i = threadIdx.x; i < qend - qlo; i += kDdThreads) {
                 const long long tau = (long long)t0 + qlo + i;
@@ -94,23 +100,23 @@ dedisp_kernel(const float *__restrict__ cur, const float *__restrict__ last,
                 const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    const int s = 4 * q + j;
-                    const int p = qlo + i - lo[s];
-                    if (p >= 0 && p < base[s + 1] - base[s])
-                        win[base[s] + p] = vv[j];
+                    const int p = qlo + i - slo[j];
+                    if (p >= 0 && p < sw[j])
+                        win[sb[j] + p] = vv[j];
                 }
             }
         }
     } else {
         for (int s = 0; s < nsub; s++) {
-            const int W = base[s + 1] - base[s];
+            const int b = base[s], W = base[s + 1] - b;
+            const long long tau0 = (long long)t0 + lo[s];
             for (int i = threadIdx.x; i < W; i += kDdThreads) {
-                const long long tau = (long long)t0 + lo[s] + i;
+                const long long tau = tau0 + i;
                 float v = 0.f;
                 if (tau < tau_end)
                     v = tau < worklen ? __ldg(last + tau * nsub + s)
                                       : __ldg(cur + (tau - worklen) * nsub + s);
-                win[base[s] + i] = v;
+                win[b + i] = v;
             }
         }
     }
