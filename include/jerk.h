@@ -354,6 +354,11 @@ int jerk_dedisperser_create(jerk_dedisperser **dedisperser, int worklen, int nsu
 void jerk_dedisperser_destroy(jerk_dedisperser *dedisperser);
 /* the tiling chosen: DMs per CTA group and samples per tile */
 int jerk_dedisperser_shape(const jerk_dedisperser *dedisperser, int *group_dms, int *tile_samples);
+/* Host only (no CUDA call): the checks and the tiling choice of
+ * jerk_dedisperser_create for a host offsets table, with the shared memory a
+ * CTA takes. */
+int jerk_dedisp_plan(int worklen, int nsub, int numdms, const int *offsets, int *group_dms,
+                     int *tile_samples, long long *smem_bytes);
 int jerk_dedisperser_matches(const jerk_dedisperser *dedisperser, int worklen, int nsub, int numdms,
                              const int *offsets);
 int jerk_dedisp_subbands(jerk_dedisperser *dedisperser, const float *cur, const float *last,

@@ -265,53 +265,68 @@ int host_offsets(const int *offsets, long long n, std::vector<int> &buf, const i
 
 }  // namespace
 
+// Host only: checks the sizes and a host offsets table and chooses the
+// tiling -- the widest tile (256, 128), then the largest DM group, whose
+// shared memory fits two CTAs per SM; else tiles of 64 or 32 samples with up
+// to 227 KB.
+extern "C" int jerk_dedisp_plan(int worklen, int nsub, int numdms, const int *offsets,
+                                int *group_dms, int *tile_samples, long long *smem_bytes)
+{
+    if (!offsets)
+        return set_error(JERK_EINVAL, "jerk_dedisp_plan: null pointer");
+    if (worklen < 1 || nsub < 1 || numdms < 1)
+        return set_error(JERK_EINVAL, "jerk_dedisp_plan: worklen, nsub, numdms must be > 0");
+    if ((long long)worklen * nsub * 2 >= (1LL << 40) || (long long)numdms * nsub > INT_MAX)
+        return set_error(JERK_EINVAL, "jerk_dedisp_plan: sizes too large");
+    for (long long i = 0; i < (long long)numdms * nsub; i++)
+        if (offsets[i] < 0 || offsets[i] > worklen)
+            return set_error(JERK_EINVAL, "jerk_dedisp_plan: every offset must lie in [0, worklen]");
+    int G = 0, T = 0;
+    size_t smem = 0;
+    for (int t : {256, 128, 64, 32}) {
+        const size_t cap = t >= 128 ? kSmemPreferred : kSmemMax;
+        for (int gsz : {32, 16, 8, 4, 2, 1}) {
+            const size_t b = dd_tables(offsets, numdms, nsub, gsz, t, nullptr, nullptr);
+            if (b <= cap) {
+                G = gsz;
+                T = t;
+                smem = b;
+                break;
+            }
+        }
+        if (G)
+            break;
+    }
+    if (!G)
+        return set_error(JERK_EUNSUPPORTED,
+                         "jerk_dedisp_plan: a subband window does not fit in shared memory");
+    if ((numdms + G - 1) / G > 65535)
+        return set_error(JERK_EUNSUPPORTED, "jerk_dedisp_plan: too many DM groups");
+    if (group_dms)
+        *group_dms = G;
+    if (tile_samples)
+        *tile_samples = T;
+    if (smem_bytes)
+        *smem_bytes = (long long)smem;
+    return JERK_OK;
+}
+
 extern "C" int jerk_dedisperser_create(jerk_dedisperser **out, int worklen, int nsub, int numdms,
                                        const int *offsets_in)
 {
     if (!out || !offsets_in)
         return set_error(JERK_EINVAL, "jerk_dedisperser_create: null pointer");
     *out = nullptr;
-    if (worklen < 1 || nsub < 1 || numdms < 1)
-        return set_error(JERK_EINVAL, "jerk_dedisperser_create: worklen, nsub, numdms must be > 0");
-    if ((long long)worklen * nsub * 2 >= (1LL << 40) || (long long)numdms * nsub > INT_MAX)
-        return set_error(JERK_EINVAL, "jerk_dedisperser_create: sizes too large");
+    if (worklen < 1 || nsub < 1 || numdms < 1 || (long long)numdms * nsub > INT_MAX)
+        return set_error(JERK_EINVAL, "jerk_dedisperser_create: bad sizes");
     std::vector<int> hbuf;
     const int *offsets = nullptr;
-    const int rc = host_offsets(offsets_in, (long long)numdms * nsub, hbuf, &offsets);
+    int rc = host_offsets(offsets_in, (long long)numdms * nsub, hbuf, &offsets);
     if (rc != JERK_OK)
         return rc;
-    for (long long i = 0; i < (long long)numdms * nsub; i++)
-        if (offsets[i] < 0 || offsets[i] > worklen)
-            return set_error(JERK_EINVAL,
-                             "jerk_dedisperser_create: every offset must lie in [0, worklen]");
-    // the widest tile, then the largest DM group, that fits two CTAs per SM;
-    // else one CTA per SM with narrower tiles
     int G = 0, T = 0;
-    for (int t : {256, 128}) {
-        for (int gsz : {32, 16, 8, 4, 2, 1})
-            if (dd_tables(offsets, numdms, nsub, gsz, t, nullptr, nullptr) <= kSmemPreferred) {
-                G = gsz;
-                T = t;
-                break;
-            }
-        if (G)
-            break;
-    }
-    for (int t : {64, 32}) {
-        if (G)
-            break;
-        for (int gsz : {32, 16, 8, 4, 2, 1})
-            if (dd_tables(offsets, numdms, nsub, gsz, t, nullptr, nullptr) <= kSmemMax) {
-                G = gsz;
-                T = t;
-                break;
-            }
-    }
-    if (!G)
-        return set_error(JERK_EUNSUPPORTED,
-                         "jerk_dedisperser_create: a subband window does not fit in shared memory");
-    if ((numdms + G - 1) / G > 65535)
-        return set_error(JERK_EUNSUPPORTED, "jerk_dedisperser_create: too many DM groups");
+    if ((rc = jerk_dedisp_plan(worklen, nsub, numdms, offsets, &G, &T, nullptr)) != JERK_OK)
+        return rc;
     jerk_dedisperser *d = new jerk_dedisperser;
     d->worklen = worklen;
     d->nsub = nsub;

@@ -116,7 +116,7 @@ EXPORTS = [
     "jerk_polish_rzw", "jerk_zap_birdies", "jerk_local_power", "jerk_derivs",
     "jerk_optimize_cand", "jerk_downsample_subbands", "jerk_dedisperser_create",
     "jerk_dedisperser_destroy", "jerk_dedisperser_shape", "jerk_dedisperser_matches",
-    "jerk_dedisp_subbands",
+    "jerk_dedisp_subbands", "jerk_dedisp_plan",
 ]
 
 
@@ -210,6 +210,8 @@ def lib() -> C.CDLL:
     L.jerk_dedisperser_matches.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
     L.jerk_dedisp_subbands.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p]
+    L.jerk_dedisp_plan.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
     L.jerk_polisher_create.argtypes = [C.POINTER(C.c_void_p), C.c_void_p]
     L.jerk_polisher_destroy.argtypes = [C.c_void_p]
     L.jerk_polisher_destroy.restype = None
@@ -500,6 +502,19 @@ def downsample_subbands(data, bs: int, out=None):
                                           C.c_void_p(data.data_ptr()), worklen, bs, nsub,
                                           C.c_void_p(_stream_of(data))))
     return out
+
+
+def dedisp_plan(worklen: int, nsub: int, offsets) -> Tuple[int, int, int]:
+    """The tiling a Dedisperser would choose for these offsets (host only,
+    jerk_dedisp_plan): (DMs per CTA group, samples per tile, shared-memory
+    bytes per CTA).  Raises JerkError on offsets outside [0, worklen]."""
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    if off.ndim != 2 or off.shape[1] != nsub:
+        raise JerkError(JERK_EINVAL, "dedisp_plan: offsets must be [numdms, nsub]")
+    g, t, b = C.c_int(), C.c_int(), C.c_longlong()
+    _check(lib().jerk_dedisp_plan(worklen, nsub, off.shape[0], off.ctypes.data_as(C.c_void_p),
+                                  C.byref(g), C.byref(t), C.byref(b)))
+    return g.value, t.value, b.value
 
 
 class Dedisperser:

@@ -161,3 +161,38 @@ def test_input_entry_points_size_and_reject_before_any_device_work():
     assert L.jerk_deredden(4096, 7, 4096, 1 << 20, None) == jerk.JERK_EINVAL
     assert L.jerk_deredden(4096, 1 << 20, 4096, 16, None) == jerk.JERK_EINVAL
     assert L.jerk_spectrum_from_timeseries(4096, 100, 4096, 4096, big, None) == jerk.JERK_EUNSUPPORTED
+
+
+def _disp_offsets(numdms, nsub, worklen, dm0, ddm, dt=64e-6):
+    f = 1200.0 + (np.arange(nsub) + 0.5) * 400.0 / nsub
+    dms = dm0 + ddm * np.arange(numdms)
+    delay = 4.148808e3 * dms[:, None] * (f[None, :] ** -2 - f[-1] ** -2)
+    return np.minimum(np.rint(delay / dt), worklen).astype(np.int32)
+
+
+def test_dedisp_tiling_choice_on_the_host():
+    """jerk_dedisp_plan (no CUDA call): the widest tile, then the largest DM
+    group, whose subband windows fit two CTAs per SM (100 KB); wide subband
+    counts fall back to narrower tiles with up to 227 KB."""
+    g, t, b = jerk.dedisp_plan(65536, 64, _disp_offsets(512, 64, 65536, 0.0, 0.5, 256e-6))
+    assert (g, t) == (32, 256) and b <= 100 * 1024
+    assert jerk.dedisp_plan(8192, 64, _disp_offsets(96, 64, 8192, 10.0, 0.5))[:2] == (16, 256)
+    g, t, b = jerk.dedisp_plan(2048, 512, _disp_offsets(24, 512, 2048, 10.0, 0.5))
+    assert (g, t) == (8, 64) and 100 * 1024 < b <= 227 * 1024
+    # one window row per subband of the tile plus the DM spread: a wide spread
+    # within a group shrinks the group
+    wide = np.zeros((64, 8), dtype=np.int32)
+    wide[1::2] = 3000
+    assert jerk.dedisp_plan(4096, 8, wide)[0] == 1
+
+
+def test_dedisp_plan_rejects_bad_offsets():
+    for off in (np.array([[0, 1, 2, 101]]), np.array([[0, -1, 2, 3]])):
+        with pytest.raises(jerk.JerkError) as ei:
+            jerk.dedisp_plan(100, 4, off)
+        assert ei.value.code == jerk.JERK_EINVAL
+    with pytest.raises(jerk.JerkError):
+        jerk.dedisp_plan(100, 4, np.zeros((2, 3)))
+    with pytest.raises(jerk.JerkError) as ei:  # 4096 subband rows of 32 samples: too wide
+        jerk.dedisp_plan(64, 4096, np.zeros((1, 4096)))
+    assert ei.value.code == jerk.JERK_EUNSUPPORTED
