@@ -33,16 +33,30 @@ def shard(items: Sequence, rank: int, world: int) -> List:
     return [x for i, x in enumerate(items) if i % world == rank]
 
 
+def contiguous_ranges(n: int, world: int) -> List[Tuple[int, int]]:
+    """(first, count) ranges covering 0..n-1, one per rank, sizes differing by
+    at most one."""
+    base, extra = divmod(n, world)
+    out, first = [], 0
+    for r in range(world):
+        k = base + (1 if r < extra else 0)
+        out.append((first, k))
+        first += k
+    return out
+
+
 def rstep_ranges(nrsteps: int, world: int) -> List[Tuple[int, int]]:
     """Contiguous (first, count) rstep ranges covering one spectrum, one per
     rank, for a spectrum searched by several GPUs."""
-    base, extra = divmod(nrsteps, world)
-    out, first = [], 0
-    for r in range(world):
-        n = base + (1 if r < extra else 0)
-        out.append((first, n))
-        first += n
-    return out
+    return contiguous_ranges(nrsteps, world)
+
+
+def dm_ranges(numdms: int, world: int) -> List[Tuple[int, int]]:
+    """Contiguous (first, count) DM-trial ranges, one per rank, for subband
+    dedispersion over several GPUs: each rank builds its dedisperser from its
+    rows of the offsets table and reads the same subband blocks.  Contiguous
+    rows keep neighbouring DMs, whose windows overlap, in one rank's groups."""
+    return contiguous_ranges(numdms, world)
 
 
 def max_over_ranks(value: float, dist=None, device: Optional[str] = None) -> float:

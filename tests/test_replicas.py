@@ -65,3 +65,60 @@ def test_rstep_ranges_cover_a_spectrum():
         rr = replicas.rstep_ranges(n, w)
         assert sum(c for _, c in rr) == n
         assert all(rr[i][0] + rr[i][1] == rr[i + 1][0] for i in range(w - 1))
+
+
+def _dedisp_worker(rank, world, port, q):
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    from oracle import bindings as ob
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    env = replicas.rank_env()
+    rng = np.random.default_rng(5)  # every rank reads the same subband blocks
+    worklen, nsub, numdms = 500, 12, 11
+    cur = rng.standard_normal((worklen, nsub)).astype(np.float32)
+    last = rng.standard_normal((worklen, nsub)).astype(np.float32)
+    off = rng.integers(0, worklen + 1, (numdms, nsub)).astype(np.int32)
+    first, count = replicas.dm_ranges(numdms, env.world)[env.rank]
+    rows = ob.dedisp_subbands(cur, last, off[first:first + count])
+    local = {first + i: [rows[i].tobytes()] for i in range(count)}
+    merged = replicas.gather_results(local, dist)
+    full = ob.dedisp_subbands(cur, last, off) if env.rank == 0 else None
+    ok = None
+    if env.rank == 0:
+        ok = sorted(merged) == list(range(numdms)) and all(
+            merged[d][0] == full[d].tobytes() for d in range(numdms))
+    q.put((env.rank, (first, count), ok))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_split_dm_trials():
+    """Dedispersion over two ranks: each takes a contiguous range of the DM
+    trials (replicas.dm_ranges) over the same subband blocks, with no data
+    exchange; the trials merged on rank 0 equal the one-rank result bit for
+    bit.  (The oracle's dedispersion stands in for each rank's GPU.)"""
+    from tests import helpers as H
+
+    H.ensure_oracle()
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_dedisp_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in range(world):
+        r, rng_, ok = q.get(timeout=120)
+        out[r] = (rng_, ok)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out[0][0] == (0, 6) and out[1][0] == (6, 5)
+    assert out[0][1] is True
+    assert replicas.dm_ranges(3, 4) == [(0, 1), (1, 1), (2, 1), (3, 0)]
