@@ -14,10 +14,15 @@ drives them on seeded synthetic inputs and stores small results:
 * ``kernels_small.npz``  a few response-kernel FFTs of the small search's bank.
 * ``small_ACCEL.txt``    the reference CLI's ACCEL output for the small search
                          (after its sort / harmonic removal / optimisation).
+* ``dedisp_small.npz``   two seeded blocks of 96 samples x 12 subbands, an
+                         offsets table of 7 DMs (0 and 96 included) and the
+                         reference's float_dedisp (src/dispersion.c:208-231)
+                         of them, one call per DM as prepsubband makes them.
 
 Run from the repository root after ``make -C oracle``:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py dedisp     # only dedisp_small.npz
 """
 
 from __future__ import annotations
@@ -140,8 +145,24 @@ def sigma_grid() -> dict:
     return {"candidate_sigma": rows, "power_for_sigma": cuts}
 
 
+def dedisp_small() -> None:
+    rng = np.random.default_rng(96)
+    worklen, nsub, numdms = 96, 12, 7
+    cur = (rng.standard_normal((worklen, nsub)) * 25 + 80).astype(np.float32)
+    last = (rng.standard_normal((worklen, nsub)) * 25 + 80).astype(np.float32)
+    off = rng.integers(0, worklen + 1, (numdms, nsub)).astype(np.int32)
+    off[0] = 0
+    off[1] = worklen
+    out = ob.dedisp_subbands(cur, last, off, reference=True)
+    np.savez_compressed(os.path.join(HERE, "dedisp_small.npz"), cur=cur, last=last,
+                        offsets=off, out=out)
+
+
 def main() -> None:
     ob.build()
+    if sys.argv[1:] == ["dedisp"]:
+        dedisp_small()
+        return
     with tempfile.TemporaryDirectory() as tmp:
         with open(os.path.join(HERE, "small_cands.json"), "w") as f:
             json.dump(small_cands(tmp), f, indent=1)
@@ -151,6 +172,7 @@ def main() -> None:
         accel_small(tmp)
     with open(os.path.join(HERE, "sigma.json"), "w") as f:
         json.dump(sigma_grid(), f, indent=1)
+    dedisp_small()
 
 
 if __name__ == "__main__":

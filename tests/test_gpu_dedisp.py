@@ -249,3 +249,17 @@ def test_dedispersed_trials_feed_the_search():
     peak = int(np.argmax([best[i] for i in range(len(dms))]))
     assert dms[peak] == dm_true
     assert best[peak] > 10.0 and best[peak] > 2 * max(best[0], best[len(dms) - 1])
+
+
+def test_dedisp_matches_reference_golden():
+    """The GPU against the committed fixture of the reference's float_dedisp
+    (tests/golden/dedisp_small.npz): 96 samples x 12 subbands, 7 DMs with
+    offsets 0 and 96 among them."""
+    import os
+
+    g = np.load(os.path.join(H.GOLDEN, "dedisp_small.npz"))
+    worklen, nsub = g["cur"].shape
+    dd = jerk.Dedisperser(worklen, nsub, g["offsets"])
+    got = dd(torch.from_numpy(g["cur"]).cuda(), torch.from_numpy(g["last"]).cuda()).cpu().numpy()
+    dd.close()
+    assert np.array_equal(got.view(np.uint32), g["out"].view(np.uint32))

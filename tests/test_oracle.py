@@ -304,3 +304,14 @@ def test_downsample_oracle_is_the_block_mean():
             acc = (acc + x[3 * t + k]).astype(np.float32)
         want[t] = acc / np.float32(3)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_dedisp_oracle_matches_golden_from_the_reference():
+    """The committed fixture (tests/golden/dedisp_small.npz, the reference's
+    float_dedisp per DM, made by tests/golden/make_golden.py) pins the
+    oracle's dedispersion without the reference build."""
+    import os
+
+    g = np.load(os.path.join(H.GOLDEN, "dedisp_small.npz"))
+    got = ob.dedisp_subbands(g["cur"], g["last"], g["offsets"])
+    assert np.array_equal(got.view(np.uint32), g["out"].view(np.uint32))
