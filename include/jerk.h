@@ -29,6 +29,19 @@
  *                      (src/characteristics.c:647-705)
  *   jerk_bank_generate the kernel bank of create_subharminfos
  *                      (src/accel_utils.c:151-282, src/responses.c:333-418)
+ *   jerk_polish_rzw / jerk_optimize_cand / jerk_local_power / jerk_derivs
+ *                      optimize_accelcand's harmonic polishing
+ *                      (src/accel_utils.c:573-657, src/maximize_rzw.c:84-190,
+ *                       get_localpower3d / get_derivs3d
+ *                       src/characteristics.c:75-191)
+ *   jerk_realfft / jerk_deredden / jerk_spectrum_from_timeseries /
+ *   jerk_zap_birdies   the .dat input of create_accelobs and CPU1's zapping
+ *                      (src/fastffts.c:163-235, src/accel_utils.c:1557-1633,
+ *                       1696-1753, src/accelsearch_lib.c:393-418)
+ *   jerk_downsample_subbands / jerk_dedisp_subbands
+ *                      prepsubband_cu's DownsampDataArray / getDedisp
+ *                      (src/prepsubband_kernels.cu:21-87)
+ *   jerk_server_*      the served form (no counterpart in the reference)
  *
  * Return codes: JERK_OK, > 0 recoverable, < 0 fatal (no exit() anywhere).
  */
