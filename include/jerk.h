@@ -218,10 +218,15 @@ int jerk_bank_generate(const jerk_subharm *subs, int nsubs, void *device_bank, v
  * (this subharmonic's [numw][numz][fftlen] rows) and volume
  * ([numw][numz][numrs] floats, numrs <= corr_uselen + 8 is enough) are
  * device pointers owned by the caller; fullrlo is the rstep's first
- * fundamental r.  Asynchronous on stream (NULL = default stream).  The first
- * call on each device looks the array up (cudaGetSymbolAddress): make it
- * before any stream capture.  Calls share the array, so calls that overlap
- * on the GPU race; serialise them. */
+ * fundamental r.  Normalisation is the block median, or 1/sqrt(nph) when
+ * nph > 0 (-photon); the local-power normalisation of -locpow is not
+ * offered here (use a plan).  The call only launches kernels on stream
+ * (NULL = default stream): descriptors go as kernel parameters and the FFT
+ * twiddles are computed on the device, so nothing is copied from host
+ * memory.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress): make it before any stream capture.  Calls share
+ * the array, so calls that overlap on the GPU race; serialise them.
+ * Failures set jerk_last_error. */
 int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
                        const jerk_subharm *sub, const void *kernels, double fullrlo,
                        int corr_uselen, float nph, float *volume, int *numrs, long long *rlo,

@@ -1100,7 +1100,10 @@ cudaError_t launch_harmsum_tma(const SearchDev &P, const HarmTma &T, int zt, cud
 // threads -- race on it and must be serialised by the caller.  Host code
 // cannot use the array's name as a device address, so the first call on each
 // device looks the address up with cudaGetSymbolAddress (with that device
-// current); make that first call before any stream capture.
+// current); make that first call before any stream capture.  After that a
+// call only launches kernels on its stream: the descriptors travel as kernel
+// parameters and the FFT twiddles are computed on the device, so nothing is
+// copied from host memory.
 
 #define JERK_STATIC_SCRATCH_BYTES (192 * 1024)
 static __device__ __align__(256) unsigned char g_static_scratch[JERK_STATIC_SCRATCH_BYTES];
@@ -1126,15 +1129,74 @@ static_assert(kOffRinds + 2 * (size_t)kStaticMaxUselen <= JERK_STATIC_SCRATCH_BY
 
 std::mutex g_static_mu;
 unsigned char *g_static_addr[64];
-float2 g_static_tw[81920 / sizeof(float2)];  // host staging of one twiddle table
 
-int static_fail(const char *msg)
+int static_fail(int code, const char *msg)
 {
-    fprintf(stderr, "jerk_volume_static: %s\n", msg);
-    return JERK_EINVAL;
+    char buf[256];
+    snprintf(buf, sizeof buf, "jerk_volume_static: %s", msg);
+    return set_error(code, buf);
+}
+
+// Radices of one FFT plan, passed by value to the set-up kernel.
+struct StaticRadices {
+    int n;
+    int r[kMaxStages];
+};
+
+template <int N>
+StaticRadices static_radices()
+{
+    StaticRadices R{};
+    R.n = FftPlan<N>::nstages;
+    for (int i = 0; i < R.n; i++)
+        R.r[i] = FftPlan<N>::radices[i];
+    return R;
+}
+
+StaticRadices static_radices_of(int N)
+{
+    switch (N) {
+#define JERK_SR(NN) case NN: return static_radices<NN>();
+    JERK_SR(128) JERK_SR(192) JERK_SR(256) JERK_SR(384) JERK_SR(512) JERK_SR(768)
+    JERK_SR(1024) JERK_SR(1280) JERK_SR(2048) JERK_SR(4096) JERK_SR(5120) JERK_SR(7680)
+#undef JERK_SR
+    default: return StaticRadices{};
+    }
 }
 
 }  // namespace
+
+// Writes the call's descriptors and the plan's per-stage twiddle tables (the
+// layout fft_stage_twiddles writes on the host: stage s >= 1 holds
+// W_{Ns R}^(r k) at [r Ns + k]) into the static array.  Twiddles are taken in
+// double, as on the host, and rounded to float.
+__global__ void static_setup_kernel(SubDev sd, StepDev sp, StaticRadices R, int tws,
+                                    SubDev *dsub, StepDev *dstep, float2 *dtw)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        *dsub = sd;
+        *dstep = sp;
+    }
+    if (i >= tws)
+        return;
+    int off = 0, ns = R.r[0];
+    for (int s = 1; s < R.n; s++) {
+        const int size = ns * R.r[s];
+        if (i < off + size) {
+            const int idx = i - off, r = idx / ns, k = idx % ns;
+            const double a = -2.0 * 3.14159265358979323846264338327950288 * (double)(r * k) /
+                             (double)size;
+            double sa, ca;
+            sincos(a, &sa, &ca);
+            dtw[i] = make_float2((float)ca, (float)sa);
+            return;
+        }
+        off += size;
+        ns *= R.r[s];
+    }
+}
+
 }  // namespace jerk
 
 extern "C" int jerk_volume_static(const void *spectrum, long long numbins, long long lobin,
@@ -1144,15 +1206,15 @@ extern "C" int jerk_volume_static(const void *spectrum, long long numbins, long 
 {
     using namespace jerk;
     if (!spectrum || !sub || !kernels || !volume || numbins < 1)
-        return static_fail("null argument");
+        return static_fail(JERK_EINVAL, "null argument");
     const int N = sub->fftlen;
     const int tws = fft_twiddle_size(N);
     if (N > kStaticMaxFft || tws < 0 || (size_t)tws * sizeof(float2) > kOffData - kOffTw)
-        return static_fail("fftlen beyond the static scratch (at most 7680, and supported)");
+        return static_fail(JERK_EINVAL, "fftlen beyond the static scratch (at most 7680, and supported)");
     if (corr_uselen <= 0 || corr_uselen % 2 || corr_uselen > kStaticMaxUselen)
-        return static_fail("corr_uselen beyond the static scratch (even, at most 16384)");
+        return static_fail(JERK_EINVAL, "corr_uselen beyond the static scratch (even, at most 16384)");
     if (sub->numharm < 1 || sub->harmnum < 1 || sub->numz < 1 || sub->numw < 1)
-        return static_fail("bad subharmonic");
+        return static_fail(JERK_EINVAL, "bad subharmonic");
 
     // rstep geometry, as jerk_plan_create computes it (src/accel_utils.c:1107-1141)
     const double hf = (double)sub->harmnum / (double)sub->numharm;
@@ -1165,24 +1227,29 @@ extern "C" int jerk_volume_static(const void *spectrum, long long numbins, long 
     else if (numrs % 2)
         numrs = (numrs / 2 + 1) * 2;
     if (numrs + 2 * sub->halfwidth > N)
-        return static_fail("fftlen too short for the good bins");
+        return static_fail(JERK_EINVAL, "fftlen too short for the good bins");
 
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-        return JERK_ECUDA;
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[dev]) {
-        void *addr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
-        if (e != cudaSuccess || !addr) {
-            fprintf(stderr, "jerk_volume_static: cudaGetSymbolAddress: %s\n",
-                    cudaGetErrorString(e));
-            return JERK_ECUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return static_fail(JERK_ECUDA, "cudaGetDevice failed");
+    if (dev < 0 || dev >= 64)
+        return static_fail(JERK_EUNSUPPORTED, "device ordinal above 63");
+    unsigned char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (!g_static_addr[dev]) {
+            void *addr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
+            if (e != cudaSuccess || !addr) {
+                char msg[160];
+                snprintf(msg, sizeof msg, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+                return static_fail(JERK_ECUDA, msg);
+            }
+            g_static_addr[dev] = (unsigned char *)addr;
         }
-        g_static_addr[dev] = (unsigned char *)addr;
+        base = g_static_addr[dev];
     }
-    unsigned char *base = g_static_addr[dev];
 
     SubDev sd{};
     sd.numharm = sub->numharm;
@@ -1203,14 +1270,13 @@ extern "C" int jerk_volume_static(const void *spectrum, long long numbins, long 
     sp.rlo = (long long)floor(drlo);
     sp.fullrlo = fullrlo;
     sp.numrs = numrs;
-    fft_twiddle_table(N, g_static_tw);
 
-    cudaError_t e = cudaMemcpyAsync(base + kOffSub, &sd, sizeof(sd), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(base + kOffStep, &sp, sizeof(sp), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(base + kOffTw, g_static_tw, sizeof(float2) * tws,
-                            cudaMemcpyHostToDevice, st);
+    // descriptors and twiddles into the array, by a kernel on the call's
+    // stream: no copy from host memory
+    static_setup_kernel<<<(tws + 255) / 256 > 0 ? (tws + 255) / 256 : 1, 256, 0, st>>>(
+        sd, sp, static_radices_of(N), tws, (SubDev *)(base + kOffSub),
+        (StepDev *)(base + kOffStep), (float2 *)(base + kOffTw));
+    cudaError_t e = cudaGetLastError();
 
     SearchDev P{};
     P.spec = (const float2 *)spectrum;
@@ -1242,10 +1308,8 @@ extern "C" int jerk_volume_static(const void *spectrum, long long numbins, long 
         G.rowstart[1] = sub->numw * sub->numz;
         e = launch_corr(P, N, G, G.rowstart[1], st);
     }
-    if (e != cudaSuccess) {
-        fprintf(stderr, "jerk_volume_static: %s\n", cudaGetErrorString(e));
-        return JERK_ECUDA;
-    }
+    if (e != cudaSuccess)
+        return static_fail(JERK_ECUDA, cudaGetErrorString(e));
     if (numrs_out)
         *numrs_out = numrs;
     if (rlo_out)
