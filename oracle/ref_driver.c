@@ -57,6 +57,32 @@ extern Cmdline *parseCmdline(int argc, char **argv);
 static Cmdline *g_cmd_static;
 static Cmdline g_cmd_defaults;
 
+extern int get_birdies(char *zapfilenm, double T, double avg_vel, double **lobins,
+                       double **hibins);
+extern void zapbirds(double lobin, double hibin, FILE *fftfile, fcomplex *fft);
+
+/* The step the reference's main takes between create_accelobs and the
+ * kernels (src/accelsearch.c:85-107): with -zaplist and a spectrum held in
+ * memory (a .dat input), the listed birdies are zapped in sorted order, the
+ * list stopping at N/2 and a last birdie clamped below it. */
+static void ref_zap_listed(refctx *c)
+{
+    if (!(c->cmd->zaplistP && !c->obs.mmap_file && c->obs.fft))
+        return;
+    double *lo, *hi;
+    const int n = get_birdies(c->cmd->zaplist, c->obs.T, c->cmd->baryv, &lo, &hi);
+    const double top = c->obs.N / 2;
+    for (int ii = 0; ii < n; ii++) {
+        if (lo[ii] >= top)
+            break;
+        if (hi[ii] >= top)
+            hi[ii] = top - 1;
+        zapbirds(lo[ii], hi[ii], NULL, c->obs.fft);
+    }
+    vect_free(lo);
+    vect_free(hi);
+}
+
 refctx *ref_open(int argc, char **argv)
 {
     refctx *c = (refctx *)calloc(1, sizeof(refctx));
@@ -70,6 +96,7 @@ refctx *ref_open(int argc, char **argv)
     c->own_cmd = *parseCmdline(argc, argv);
     c->cmd = &c->own_cmd;
     create_accelobs(&c->obs, &c->idata, c->cmd, 1);
+    ref_zap_listed(c);
     return c;
 }
 

@@ -130,6 +130,45 @@ def small_spectrum(seed: int = 20241203):
     return presto_fft(ts), N, dt
 
 
+def red_noise_timeseries(N: int, dt: float, seed: int, pulsars: Sequence[Pulsar] = (),
+                         birdies: Sequence[float] = (), birdie_power: float = 400.0,
+                         fknee: float = 2.0, slope: float = 1.5, red_level: float = 10.0
+                         ) -> np.ndarray:
+    """Float32 series for the memory-heavy workload: a white N(0, 1) floor,
+    seeded red noise whose power falls as f**-slope below fknee Hz
+    (``red_level * ((f / fknee)**-slope - 1)`` times the white level, so it
+    meets the floor at the knee), single-bin sinusoids ("birdies") at the
+    given frequencies (each rounded to the nearest Fourier bin, normalised
+    power ``birdie_power``), and the given pulsars."""
+    rng = np.random.default_rng(seed + 1)
+    T = N * dt
+    nb = N // 2 + 1
+    f = np.arange(nb) / T
+    shape = np.zeros(nb)
+    red = (f > 0) & (f < fknee)
+    shape[red] = red_level * ((f[red] / fknee) ** (-slope) - 1.0)
+    # E|X_k|^2 = N for unit white noise: the red part has shape * N there
+    amp = np.sqrt(shape * N / 2.0)
+    X = amp * (rng.standard_normal(nb) + 1j * rng.standard_normal(nb))
+    X[0] = 0.0
+    X[-1] = 0.0
+    # a cosine of amplitude a at integer bin k has X[k] = a N / 2
+    a = np.sqrt(4.0 * birdie_power / N)
+    for fb in birdies:
+        X[int(round(fb * T))] += a * N / 2.0
+    x = np.fft.irfft(X, n=N)
+    x += timeseries(N, dt, pulsars, seed).astype(np.float64)
+    return x.astype(np.float32)
+
+
+def memory_heavy_birdies() -> List[float]:
+    """20 fixed birdie frequencies (Hz): three inside the first rsteps of a
+    -flo 1 search at zmax 300 (1.0 - 3.6 Hz), the 50 Hz mains and six of its
+    harmonics, and ten scattered ones."""
+    return [1.37, 2.11, 3.05, 50.0, 100.0, 150.0, 200.0, 250.0, 300.0, 350.0,
+            12.5, 33.3, 61.8, 87.1, 123.0, 177.7, 211.9, 266.6, 404.0, 512.0]
+
+
 def paper_pulsars(seed: int = 2025) -> List[Pulsar]:
     """Four pulsars: f~U(5,500) Hz, 1-8 harmonics, z~U(-180,180),
     w~U(-280,280), SNR~U(6,20)."""

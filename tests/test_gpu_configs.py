@@ -13,9 +13,10 @@ For each configuration:
     rows to 1e-5 relative to max(power, 1) -- whole volumes, or, where the
     kernels of one subharmonic exceed 256 MB, 9 sampled (w, z) rows, each row
     being its own correlation; the worst error is printed per configuration;
-  * (except the memory-heavy one, whose reference bank takes minutes on one
-    CPU core) the candidate list over the first rsteps equals the reference
-    CPU search's, except entries within 1e-4 of a stage cutoff.
+  * the candidate list over the first rsteps equals the reference CPU
+    search's, except entries within 1e-4 of a stage cutoff (the memory-heavy
+    configuration in its own test below, from a red-noise .dat with birdies
+    and a zaplist, as that configuration is defined).
 Spectra: seeded Gaussian noise plus injected pulsars (prestozl_b200.synth).
 """
 
@@ -143,3 +144,97 @@ def test_configuration_matches_reference(name, tmp_path):
     plan.close()
     bank.close()
     ref.close()
+
+
+def test_memory_heavy_red_noise_and_birdies_match_reference(tmp_path):
+    """The memory-heavy configuration end to end, as the reference runs it on
+    a .dat input with -zaplist: a 2^25-sample series (dt 54.6 us) of red noise
+    (power falling as f^-1.5 below 2 Hz over a white floor), 20 single-bin
+    birdies and one pulsar, searched at -zmax 300 -wmax 600 -numharm 32
+    -sigma 4.0.
+
+    The reference's CPU accelsearch reads the .dat, FFTs it, removes the red
+    noise (src/accel_utils.c:1557-1634), zaps the zaplist's birdies
+    (src/accelsearch_lib.c:393-418, src/zapping.c:29-81) and searches.  Here
+    the GPU does every step: jerk_spectrum_from_timeseries, jerk_zap_birdies,
+    the kernel bank (jerk_bank_generate) and the search.
+      * The GPU's dereddened and zapped spectrum equals, bitwise, the
+        reference's own deredden and zapbirds applied to the GPU's real FFT,
+        and differs from the spectrum the reference prepared itself only by
+        the real FFT's rounding (rms difference at most 1e-5 of the rms; the
+        GPU's FP32 real FFT is held to a single-precision library in
+        test_gpu_input).
+      * The candidate lists of the first two rsteps (1.0 - 2.7 Hz: the
+        whitened red-noise band, two zapped birdies and the pulsar's
+        fundamental) are equal except entries within 1e-4 of a cutoff;
+        powers and sigmas agree to 1e-5.
+    The reference searches on one thread (its threaded search calls
+    dcdflib's cdfchi concurrently, which aborts at 32 harmonics)."""
+    torch = pytest.importorskip("torch")
+    build.build()
+    H.ensure_oracle()
+    if not H.have_ref():
+        pytest.skip("the reference build (oracle/_ref) is needed")
+    N, nsteps = 1 << 25, 2
+    T = N * DT
+    birdies = synth.memory_heavy_birdies()
+    psr = synth.Pulsar(f=1.9, z=120.0, w=-200.0, snr=30.0, nharm=4, phase=0.3)
+    x = synth.red_noise_timeseries(N, DT, 505, pulsars=[psr], birdies=birdies)
+    root = str(tmp_path / "series")
+    x.tofile(root + ".dat")
+    synth.write_inf(root, N, DT)
+    width = 0.003  # Hz: about 5.5 bins
+    with open(root + ".zaplist", "w") as f:
+        f.write("# freq width (Hz)\n")
+        for fb in birdies:
+            f.write(f"{fb!r} {width!r}\n")
+    # get_birdies (src/birdzap.c:6-80) at zero velocity, sorted by lobin
+    lob = sorted((fb - 0.5 * width) * T for fb in birdies)
+    hib = sorted((fb + 0.5 * width) * T for fb in birdies)
+
+    args = ["-zmax", "300", "-wmax", "600", "-numharm", "32", "-sigma", "4.0",
+            "-zaplist", root + ".zaplist"]
+    ob.set_threads(1)
+    ref = ob.RefSearch(root + ".dat", args)
+    ro = ref.obs
+    obs, fftlen, _ = jerk.obs_from_params(N // 2, N, DT, 300, 600, 32, 4.0)
+    assert (obs.numz, obs.numw, obs.numharmstages, fftlen) == (ro.numz, ro.numw, 6, ro.fftlen)
+
+    # the spectrum, on the GPU, and its pin against the reference's own steps
+    d = torch.from_numpy(x).cuda()
+    raw = jerk.realfft(d).cpu().numpy()
+    spec = jerk.spectrum_from_timeseries(d)
+    jerk.zap_birdies(spec, N, lob, hib)
+    got_spec = spec.cpu().numpy()
+    want_spec = ob.deredden(raw, reference=True)
+    want_spec[0] = 1.0 + 1.0j
+    for lo, hi in zip(lob, hib):
+        want_spec = ob.zapbirds(want_spec, lo, min(hi, N // 2 - 1), reference=True)
+    assert np.array_equal(got_spec.view(np.uint32), want_spec.view(np.uint32))
+    # the spectrum the reference prepared itself (its real FFT, deredden and
+    # zapping) differs from the GPU's only by the real FFT's rounding
+    rs = ref.spectrum()
+    diff = np.abs(rs.astype(np.complex128) - got_spec)
+    rms = float(np.sqrt(np.mean(np.abs(rs.astype(np.complex128)) ** 2)))
+    assert float(np.sqrt(np.mean(diff ** 2))) <= 1e-5 * rms
+
+    subs = jerk.subharm_sizes(obs, fftlen)
+    bank = jerk.DeviceBank(subs)
+    plan = jerk.JerkPlan(obs, subs, batch=2, device_bank=bank.ptr.value)
+    got = plan.search(spec, 0, nsteps)
+    torch.cuda.synchronize()
+    plan.close()
+    bank.close()
+    del spec, d
+
+    ref.make_bank()
+    want, done = ref.search(max_steps=nsteps)
+    ref.close()
+    assert done == nsteps and len(want) > 0
+    probs = H.compare_cands(got, want, list(ro.powcut))
+    assert not probs, probs[:10]
+    # the pulsar is found near its fundamental; no birdie survives the zapping
+    assert np.any(np.abs(got["r"] - 1.9 * T) < 2.0)
+    for fb in birdies[:2]:
+        assert not np.any(np.abs(got["r"] - fb * T) < 1.0), fb
+    print(f"memory-heavy red noise + birdies: {len(got)} candidates (reference {len(want)})")
