@@ -350,6 +350,15 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
             tws[i] = P.twiddles[sd.twoff + i];
     }
 
+    if (P.wait_probe && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+        // a wait that must run out: phase 0 of s_probe never completes
+        __shared__ uint64_t s_probe;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_probe)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (!bar_wait(&s_probe, 0) && P.status)
+            atomicOr(P.status, kStatusCopy);
+    }
+
     // the kernel row, in the order this thread's first-stage butterfly reads it
     // (kBig: read from global memory at every rstep instead)
     float2 kreg[R0];

@@ -736,6 +736,7 @@ struct jerk_plan {
     float *d_hit_pows = nullptr;
     unsigned int *d_hit_count = nullptr;
     unsigned int *d_status = nullptr;
+    int wait_probe = 0;                // jerk_debug_wait_probe
     long long max_hits = 0;
     long long plane_floats = 0, prepped_f2 = 0;
     // a search pass being enqueued batch by batch
@@ -1320,6 +1321,7 @@ static SearchDev make_args(const jerk_plan *p, const float2 *spec)
     a.hit_count = p->d_hit_count;
     a.max_hits = p->max_hits;
     a.status = p->d_status;
+    a.wait_probe = p->wait_probe;
     return a;
 }
 
@@ -1391,6 +1393,8 @@ static int pass_begin(jerk_plan *p, const float2 *spec, long long first, long lo
     ps.count = count;
     ps.next = first;
     JERK_CUDA(cudaMemsetAsync(p->d_hit_count, 0, sizeof(unsigned int), p->stream));
+    // a pass that reported a failed wait or index leaves no trace in the next
+    JERK_CUDA(cudaMemsetAsync(p->d_status, 0, sizeof(unsigned int), p->stream));
     return JERK_OK;
 }
 
@@ -1759,6 +1763,17 @@ extern "C" long long jerk_plan_device_bytes(const jerk_plan *p)
                        sizeof(StepDev) * p->hsteps.size() + sizeof(float2) * p->spec_cap +
                        (p->own_bank ? sizeof(float2) * jerk_bank_elements(p->subs.data(), p->nsubs)
                                     : 0));
+}
+
+extern "C" int jerk_debug_wait_probe(jerk_plan *p, int on)
+{
+    if (!p)
+        return fail(JERK_EINVAL, "jerk_debug_wait_probe: null plan");
+    if (p->in_flight)
+        return fail(JERK_EINVAL, "jerk_debug_wait_probe: a search is in flight");
+    p->wait_probe = on != 0;
+    drop_graph(p);  // a captured pass holds the old launch arguments
+    return JERK_OK;
 }
 
 extern "C" int jerk_debug_volume(jerk_plan *p, const void *spectrum, int spectrum_on_device,

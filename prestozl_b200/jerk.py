@@ -116,7 +116,7 @@ EXPORTS = [
     "jerk_polish_rzw", "jerk_zap_birdies", "jerk_local_power", "jerk_derivs",
     "jerk_optimize_cand", "jerk_downsample_subbands", "jerk_dedisperser_create",
     "jerk_dedisperser_destroy", "jerk_dedisperser_shape", "jerk_dedisperser_matches",
-    "jerk_dedisp_subbands", "jerk_dedisp_plan",
+    "jerk_dedisp_subbands", "jerk_dedisp_plan", "jerk_debug_wait_probe",
 ]
 
 
@@ -145,6 +145,7 @@ def lib() -> C.CDLL:
     L.jerk_num_rsteps.restype = C.c_longlong
     L.jerk_debug_volume.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int,
                                     C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+    L.jerk_debug_wait_probe.argtypes = [C.c_void_p, C.c_int]
     L.jerk_candidate_sigma.restype = C.c_double
     L.jerk_candidate_sigma.argtypes = [C.c_double, C.c_int, C.c_double]
     L.jerk_power_for_sigma.restype = C.c_double
@@ -661,6 +662,11 @@ class JerkPlan:
         h, d = C.c_longlong(0), C.c_longlong(0)
         lib().jerk_plan_transfer_stats(self._p, C.byref(h), C.byref(d))
         return h.value, d.value
+
+    def set_wait_probe(self, on: bool) -> None:
+        """Test hook: later passes also run one bounded wait that must give
+        up, and fail with JERK_ECUDA (jerk_debug_wait_probe)."""
+        _check(lib().jerk_debug_wait_probe(self._p, int(bool(on))))
 
     def volume(self, spectrum, rstep: int, sub: int):
         """ffdot volume [numw][numz][numrs] of one (rstep, subharmonic)."""

@@ -326,3 +326,23 @@ def test_frequency_band_matches_reference(tmp_path):
     probs = H.compare_cands(got, want, list(prob.obs.powcut))
     assert not probs, probs[:10]
     assert got["r"].min() >= prob.obs.rlo and got["r"].max() <= prob.obs.highestbin
+
+
+def test_bounded_wait_gives_up_without_fault(small, plan):
+    """Every device wait here is bounded.  A pass whose correlation kernel runs
+    one wait that must give up (an mbarrier nothing completes, with no copy in
+    flight) fails with JERK_ECUDA and the wait's message instead of hanging;
+    the context and the same plan stay usable, and the next pass gives the
+    results of a pass that never failed."""
+    want = plan.search(small.spec, 100, 8, want_hits=True)
+    plan.set_wait_probe(True)
+    try:
+        with pytest.raises(jerk.JerkError) as ei:
+            plan.search(small.spec, 100, 8)
+        assert ei.value.code == jerk.JERK_ECUDA
+        assert "timed out" in str(ei.value)
+    finally:
+        plan.set_wait_probe(False)
+    got = plan.search(small.spec, 100, 8, want_hits=True)
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
