@@ -455,6 +455,20 @@ void jerk_server_destroy(jerk_server *server);
 double jerk_candidate_sigma(double power, int numsum, double numtrials);
 double jerk_power_for_sigma(double sigma, int numsum, double numtrials);
 
+/* The host merge of one spectrum searched in pieces (disjoint rstep ranges
+ * on several GPUs, or several calls): the raw hits of all pieces (jerk_hits
+ * keys and powers, in any order) are sorted by key -- the reference's
+ * insertion order -- decoded with the spectrum's geometry (obs and its
+ * fundamental, jerk_subharm_sizes entry 0), given their sigma and inserted
+ * with the reference's rule.  The list equals the one a single search of the
+ * union of the ranges returns.  Host only (no GPU).  Replaces the order-
+ * sensitive merge of the reference's GPU path: sort_search_results and
+ * insert_to_cands (src/accel_kernels.cu:997-1010, src/accel_utils_cu.c:857-929,
+ * src/accelsearch_lib.c:831-878).  *cands is freed with jerk_free. */
+int jerk_merge_hits(const jerk_obs *obs, const jerk_subharm *fundamental,
+                    const unsigned long long *keys, const float *powers, long long nhits,
+                    jerk_cand **cands, long long *ncands);
+
 /* Candidate insertion with the reference's 15-bin rule over a decoded hit
  * sequence; used by jerk_search, exported for tests. */
 long long jerk_insert_hits(const jerk_cand *hits, long long nhits, jerk_cand **cands);

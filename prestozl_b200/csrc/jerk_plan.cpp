@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -1633,6 +1634,72 @@ extern "C" int jerk_search_ready(jerk_plan *p)
     return cuda_fail(e, "jerk_search_ready");
 }
 
+// What decoding a hit key needs: the fundamental's geometry and, per rstep,
+// the fundamental's first r (hsteps[rs][0].rlo).
+struct HitGeom {
+    int S = 1;
+    long long numrs0 = 0, numz0 = 0, numw0 = 0;
+    int zlo0 = 0, wlo0 = 0;
+    const long long *numindep = nullptr;
+    std::function<long long(long long)> rlo_of;
+};
+
+// Hits in key order -- the reference's insertion order (rstep, stage, w, z,
+// r; src/accel_utils_cu.c:857-929) -- decoded into candidates with their
+// sigma and inserted with the reference's rule.  order receives the sorted
+// permutation of the input.
+static void hits_to_list(const HitGeom &g, const unsigned long long *keys, const float *pows,
+                         uint32_t nh, std::vector<uint32_t> &order, CandList &L)
+{
+    order.resize(nh);
+    for (uint32_t i = 0; i < nh; i++)
+        order[i] = i;
+    std::sort(order.begin(), order.end(),
+              [&](uint32_t x, uint32_t y) { return keys[x] < keys[y]; });
+    // decode + sigma per hit (independent, so spread over host threads when
+    // there are many), then the insertions in key order (sequential: each
+    // depends on the list the earlier ones left)
+    std::vector<jerk_cand> cv(nh);
+    auto decode = [&](uint32_t lo, uint32_t hi) {
+        for (uint32_t i = lo; i < hi; i++) {
+            unsigned long long key = keys[order[i]];
+            const int kk = (int)(key % g.numrs0);
+            key /= g.numrs0;
+            const int jj = (int)(key % g.numz0);
+            key /= g.numz0;
+            const int ii = (int)(key % g.numw0);
+            key /= g.numw0;
+            const int stage = (int)(key % g.S);
+            const long long rs = (long long)(key / g.S);
+            const int nhm = 1 << stage;
+            jerk_cand &c = cv[i];
+            c.power = pows[order[i]];
+            c.sigma = (float)jerk_candidate_sigma(c.power, nhm, (double)g.numindep[stage]);
+            c.numharm = nhm;
+            c.r = ((double)g.rlo_of(rs) + kk * kDR) / (double)nhm;
+            c.z = (g.zlo0 + jj * (double)kDZ) / (double)nhm;
+            c.w = (g.wlo0 + ii * (double)kDW) / (double)nhm;
+        }
+    };
+    const uint32_t nthr =
+        nh < 8192 ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (nthr == 1) {
+        decode(0, nh);
+    } else {
+        std::vector<std::thread> pool;
+        const uint32_t per = (nh + nthr - 1) / nthr;
+        for (uint32_t t = 0; t < nthr; t++) {
+            const uint32_t lo = t * per, hi = std::min(nh, lo + per);
+            if (lo < hi)
+                pool.emplace_back(decode, lo, hi);
+        }
+        for (auto &th : pool)
+            th.join();
+    }
+    for (uint32_t i = 0; i < nh; i++)
+        insert_cand(L, cv[i]);
+}
+
 extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *ncands,
                                    jerk_hits *hits)
 {
@@ -1673,58 +1740,18 @@ extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *n
                              cudaMemcpyDeviceToHost));
         p->d2h_bytes += (long long)nh * (sizeof(unsigned long long) + sizeof(float));
     }
-    std::vector<uint32_t> order(nh);
-    for (uint32_t i = 0; i < nh; i++)
-        order[i] = i;
-    std::sort(order.begin(), order.end(),
-              [&](uint32_t x, uint32_t y) { return keys[x] < keys[y]; });
-
-    const int S = p->obs.numharmstages;
-    const long long numrs0 = p->obs.corr_uselen, numz0 = p->subs[0].numz,
-                    numw0 = p->subs[0].numw;
-    // decode + sigma per hit (independent, so spread over host threads when
-    // there are many), then the insertions in key order (sequential: each
-    // depends on the list the earlier ones left)
-    std::vector<jerk_cand> cv(nh);
-    auto decode = [&](uint32_t lo, uint32_t hi) {
-        for (uint32_t i = lo; i < hi; i++) {
-            unsigned long long key = keys[order[i]];
-            const int kk = (int)(key % numrs0);
-            key /= numrs0;
-            const int jj = (int)(key % numz0);
-            key /= numz0;
-            const int ii = (int)(key % numw0);
-            key /= numw0;
-            const int stage = (int)(key % S);
-            const long long rs = (long long)(key / S);
-            const int nhm = 1 << stage;
-            jerk_cand &c = cv[i];
-            c.power = pows[order[i]];
-            c.sigma = (float)jerk_candidate_sigma(c.power, nhm, (double)p->obs.numindep[stage]);
-            c.numharm = nhm;
-            c.r = ((double)p->hsteps[(size_t)rs * p->nsubs].rlo + kk * kDR) / (double)nhm;
-            c.z = (p->zlo0 + jj * (double)kDZ) / (double)nhm;
-            c.w = (p->wlo0 + ii * (double)kDW) / (double)nhm;
-        }
-    };
-    const uint32_t nthr =
-        nh < 8192 ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    if (nthr == 1) {
-        decode(0, nh);
-    } else {
-        std::vector<std::thread> pool;
-        const uint32_t per = (nh + nthr - 1) / nthr;
-        for (uint32_t t = 0; t < nthr; t++) {
-            const uint32_t lo = t * per, hi = std::min(nh, lo + per);
-            if (lo < hi)
-                pool.emplace_back(decode, lo, hi);
-        }
-        for (auto &th : pool)
-            th.join();
-    }
+    HitGeom g;
+    g.S = p->obs.numharmstages;
+    g.numrs0 = p->obs.corr_uselen;
+    g.numz0 = p->subs[0].numz;
+    g.numw0 = p->subs[0].numw;
+    g.zlo0 = p->zlo0;
+    g.wlo0 = p->wlo0;
+    g.numindep = p->obs.numindep;
+    g.rlo_of = [p](long long rs) { return p->hsteps[(size_t)rs * p->nsubs].rlo; };
     CandList L;
-    for (uint32_t i = 0; i < nh; i++)
-        insert_cand(L, cv[i]);
+    std::vector<uint32_t> order;
+    hits_to_list(g, keys.data(), pows.data(), nh, order, L);
     if (hits) {
         hits->count = nh;
         hits->keys = (unsigned long long *)malloc(sizeof(unsigned long long) * (nh ? nh : 1));
@@ -1734,6 +1761,49 @@ extern "C" int jerk_search_collect(jerk_plan *p, jerk_cand **cands, long long *n
             hits->powers[i] = pows[order[i]];
         }
     }
+    const long long n = export_list(L, cands);
+    if (n < 0)
+        return fail(JERK_ENOMEM, "candidate list allocation");
+    if (ncands)
+        *ncands = n;
+    return JERK_OK;
+}
+
+extern "C" int jerk_merge_hits(const jerk_obs *obs, const jerk_subharm *fundamental,
+                               const unsigned long long *keys, const float *powers,
+                               long long nhits, jerk_cand **cands, long long *ncands)
+{
+    if (!obs || !fundamental || !cands || nhits < 0 || (nhits && (!keys || !powers)))
+        return fail(JERK_EINVAL, "jerk_merge_hits: bad argument");
+    if (nhits > 0xffffffffll)
+        return fail(JERK_EUNSUPPORTED, "jerk_merge_hits: more than 2^32 hits");
+    if (fundamental->numharm != 1 || fundamental->harmnum != 1 || fundamental->numz != obs->numz ||
+        fundamental->numw < 1 || obs->corr_uselen < 2 || obs->numharmstages < 1 ||
+        obs->numharmstages > JERK_MAX_STAGES)
+        return fail(JERK_EINVAL, "jerk_merge_hits: fundamental and obs do not match");
+    const long long nrsteps = count_rsteps(*obs);
+    const long long per_rstep = (long long)obs->numharmstages * fundamental->numw *
+                                fundamental->numz * obs->corr_uselen;
+    for (long long i = 0; i < nhits; i++)
+        if (keys[i] / (unsigned long long)per_rstep >= (unsigned long long)nrsteps)
+            return fail(JERK_EINVAL, "jerk_merge_hits: a key lies beyond the last rstep");
+    HitGeom g;
+    g.S = obs->numharmstages;
+    g.numrs0 = obs->corr_uselen;
+    g.numz0 = fundamental->numz;
+    g.numw0 = fundamental->numw;
+    g.zlo0 = calc_required_z(1.0, obs->zlo);
+    g.wlo0 = calc_required_w(1.0, obs->wlo);
+    g.numindep = obs->numindep;
+    const int rstep = (int)(obs->corr_uselen * kDR);
+    const double rlo = obs->rlo;
+    // as the plan's step table: floor(calc_required_r(1, startr))
+    g.rlo_of = [rstep, rlo](long long rs) {
+        return (long long)floor(calc_required_r(1.0, rlo + (double)rs * rstep));
+    };
+    CandList L;
+    std::vector<uint32_t> order;
+    hits_to_list(g, keys, powers, (uint32_t)nhits, order, L);
     const long long n = export_list(L, cands);
     if (n < 0)
         return fail(JERK_ENOMEM, "candidate list allocation");

@@ -116,7 +116,7 @@ EXPORTS = [
     "jerk_polish_rzw", "jerk_zap_birdies", "jerk_local_power", "jerk_derivs",
     "jerk_optimize_cand", "jerk_downsample_subbands", "jerk_dedisperser_create",
     "jerk_dedisperser_destroy", "jerk_dedisperser_shape", "jerk_dedisperser_matches",
-    "jerk_dedisp_subbands", "jerk_dedisp_plan", "jerk_debug_wait_probe",
+    "jerk_dedisp_subbands", "jerk_dedisp_plan", "jerk_debug_wait_probe", "jerk_merge_hits",
 ]
 
 
@@ -146,6 +146,9 @@ def lib() -> C.CDLL:
     L.jerk_debug_volume.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int,
                                     C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
     L.jerk_debug_wait_probe.argtypes = [C.c_void_p, C.c_int]
+    L.jerk_merge_hits.argtypes = [C.POINTER(Obs), C.POINTER(Subharm), C.c_void_p, C.c_void_p,
+                                  C.c_longlong, C.POINTER(C.POINTER(Cand)),
+                                  C.POINTER(C.c_longlong)]
     L.jerk_candidate_sigma.restype = C.c_double
     L.jerk_candidate_sigma.argtypes = [C.c_double, C.c_int, C.c_double]
     L.jerk_power_for_sigma.restype = C.c_double
@@ -265,6 +268,26 @@ def insert_hits(hits: np.ndarray) -> np.ndarray:
     res = np.frombuffer(arr.tobytes(), dtype=CAND_DTYPE).copy()
     lib().jerk_free(out)
     return res
+
+
+def merge_hits(obs: Obs, fundamental: dict, keys, powers) -> np.ndarray:
+    """Candidates of one spectrum from the raw hits of searches of disjoint
+    rstep ranges (any order): jerk_merge_hits.  Host only."""
+    k = np.ascontiguousarray(keys, dtype=np.uint64)
+    pw = np.ascontiguousarray(powers, dtype=np.float32)
+    if len(k) != len(pw):
+        raise JerkError(JERK_EINVAL, "merge_hits: keys and powers differ in length")
+    f = (Subharm * 1)(fundamental) if isinstance(fundamental, Subharm) else \
+        _subharm_array([fundamental])
+    out = C.POINTER(Cand)()
+    n = C.c_longlong(0)
+    _check(lib().jerk_merge_hits(C.byref(obs), f, k.ctypes.data, pw.ctypes.data, len(k),
+                                 C.byref(out), C.byref(n)))
+    nb = n.value * CAND_DTYPE.itemsize
+    cands = np.frombuffer(C.string_at(out, nb), dtype=CAND_DTYPE).copy() if nb else \
+        np.zeros(0, dtype=CAND_DTYPE)
+    lib().jerk_free(out)
+    return cands
 
 
 def _subharm_array(subs: Sequence[dict]):
