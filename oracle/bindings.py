@@ -29,7 +29,11 @@ REFGPU_CLI = os.path.join(REF_DIR, "accelsearch_refgpu")
 REF_DEDISP_GPU_LIB = os.path.join(REF_DIR, "libprestodedisp_gpu.so")
 PREPSUBBAND_DROPIN_LIB = os.path.join(REF_DIR, "libprepsubband_dropin.so")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
-REFERENCE_SOURCES = "/root/reference"
+# Where the reference's sources lie: $PRESTOZL_REFERENCE, by default the
+# checkout this build recipe was written against.  Only the build (and CPU
+# tests that read the reference's Python) look there; the built oracle/_ref
+# travels without it.
+REFERENCE_SOURCES = os.environ.get("PRESTOZL_REFERENCE", "/root/reference")
 
 
 def build(reference: Optional[bool] = None) -> None:
@@ -38,7 +42,8 @@ def build(reference: Optional[bool] = None) -> None:
     if reference is None:
         reference = os.path.isdir(os.path.join(REFERENCE_SOURCES, "src"))
     targets = ["oracle"] + (["ref", "dropin", "refgpu", "dedispgpu"] if reference else [])
-    subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", f"REF={REFERENCE_SOURCES}", *targets],
+                   check=True)
 
 
 def have_reference() -> bool:

@@ -14,6 +14,8 @@ drives them on seeded synthetic inputs and stores small results:
 * ``kernels_small.npz``  a few response-kernel FFTs of the small search's bank.
 * ``small_ACCEL.txt``    the reference CLI's ACCEL output for the small search
                          (after its sort / harmonic removal / optimisation).
+* ``small_ACCEL.cand``   the same run's binary .cand file: one fourierprops
+                         record per candidate (src/accelsearch_lib.c:958-961).
 * ``dedisp_small.npz``   two seeded blocks of 96 samples x 12 subbands, an
                          offsets table of 7 DMs (0 and 96 included) and the
                          reference's float_dedisp (src/dispersion.c:208-231)
@@ -23,6 +25,7 @@ Run from the repository root after ``make -C oracle``:
 
     python tests/golden/make_golden.py            # every fixture
     python tests/golden/make_golden.py dedisp     # only dedisp_small.npz
+    python tests/golden/make_golden.py accel      # only small_ACCEL.txt / .cand
 """
 
 from __future__ import annotations
@@ -108,6 +111,8 @@ def accel_small(tmp: str) -> None:
     subprocess.run([ob.REF_CLI, *SMALL_ARGS, "small.fft"], cwd=tmp, env=env, check=True,
                    stdout=subprocess.DEVNULL)
     shutil.copy(os.path.join(tmp, "small_ACCEL_20_JERK_60"), os.path.join(HERE, "small_ACCEL.txt"))
+    shutil.copy(os.path.join(tmp, "small_ACCEL_20_JERK_60.cand"),
+                os.path.join(HERE, "small_ACCEL.cand"))
 
 
 def sizing(tmp: str) -> list:
@@ -162,6 +167,10 @@ def main() -> None:
     ob.build()
     if sys.argv[1:] == ["dedisp"]:
         dedisp_small()
+        return
+    if sys.argv[1:] == ["accel"]:
+        with tempfile.TemporaryDirectory() as tmp:
+            accel_small(tmp)
         return
     with tempfile.TemporaryDirectory() as tmp:
         with open(os.path.join(HERE, "small_cands.json"), "w") as f:

@@ -7,11 +7,18 @@ and flags (tests/golden/small_ACCEL.txt).
 Every field of both ACCEL tables must match as printed, except the search's
 summed power and its sigma (columns 2 and 3 of the first table), which come
 from FP32 powers and may differ in the last printed digit (tolerance 0.011).
+The binary .cand file (one fourierprops record per candidate,
+src/accelsearch_lib.c:958-961) must equal the reference's field for field
+(tests/golden/small_ACCEL.cand).  Both files are written by the reference's
+own CPU2, so downstream tools read them as they read the reference's
+(tests/test_sifting.py runs the reference's sifting parser on the ACCEL
+file).
 """
 
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 from oracle import bindings as ob
@@ -19,6 +26,21 @@ from prestozl_b200 import build, synth
 from tests import helpers as H
 
 pytestmark = pytest.mark.gpu
+
+
+# fourierprops (include/presto.h:171-189) as the reference writes it (x86-64
+# alignment: the doubles on 8-byte boundaries)
+FOURIERPROPS = np.dtype([("r", "f8"), ("rerr", "f4"), ("z", "f8"), ("zerr", "f4"), ("w", "f8"),
+                         ("werr", "f4"), ("pow", "f4"), ("powerr", "f4"), ("sig", "f4"),
+                         ("rawpow", "f4"), ("phs", "f4"), ("phserr", "f4"), ("cen", "f4"),
+                         ("cenerr", "f4"), ("pur", "f4"), ("purerr", "f4"), ("locpow", "f4")],
+                        align=True)
+
+
+def read_cand(path: str) -> np.ndarray:
+    raw = open(path, "rb").read()
+    assert len(raw) % FOURIERPROPS.itemsize == 0, len(raw)
+    return np.frombuffer(raw, dtype=FOURIERPROPS)
 
 
 def accel_rows(text: str):
@@ -57,6 +79,12 @@ def test_dropin_accel_matches_reference(tmp_path):
             assert abs(float(a) - float(b)) <= 0.011, (g, w)
         if len(g) > 12 and g[1].isdigit():
             fund = False  # second table rows start "cand harm"
+    # the .cand records, field by field (padding bytes are not data)
+    gc = read_cand(str(tmp_path / "small_ACCEL_20_JERK_60.cand"))
+    wc = read_cand(os.path.join(H.GOLDEN, "small_ACCEL.cand"))
+    assert len(gc) == len(wc) > 0
+    for f in FOURIERPROPS.names:
+        assert np.array_equal(gc[f], wc[f]), (f, gc[f], wc[f])
 
 
 def test_dropin_many_spectra_in_one_process(tmp_path):
