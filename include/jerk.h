@@ -167,6 +167,33 @@ int jerk_search_advance(jerk_plan *plan, int ahead);
 int jerk_search_ready(jerk_plan *plan);
 int jerk_search_collect(jerk_plan *plan, jerk_cand **cands, long long *ncands, jerk_hits *hits);
 
+/* The batched form across plans: several searches (spectra of any length,
+ * plans of any geometry) advanced in waves of merged launches.  One wave
+ * takes the next batch of every listed plan with work left (up to 12 per
+ * wave) and runs one prep launch, one correlation launch per FFT length and
+ * one harmonic-sum launch per stage count over all of them, so small
+ * searches share the GPU instead of each underfilling it.  Each plan's
+ * results are bitwise those of jerk_search.  Replaces, for this purpose, the
+ * reference's process pool (bin/accelsearch_pipeline_cu.py:296-407), whose
+ * processes each run their own batches (src/accelsearch_lib.c:660-830).
+ *   jerk_search_begin    stages the spectrum and starts a pass without
+ *                        enqueueing anything (no graph replay);
+ *   jerk_group_advance   enqueues waves while the listed plans have fewer
+ *                        than `ahead` batches queued or running (ahead <= 0:
+ *                        everything); the plans whose passes are in flight
+ *                        must share one stream and device.  Returns 1 while
+ *                        batches remain, 0 once all are enqueued, < 0 on error;
+ *   then jerk_search_ready / jerk_search_collect per plan as above;
+ *   jerk_search_group    all of it for whole spectra: begin, advance
+ *                        everything, collect; cands[i] / ncands[i] receive
+ *                        plan i's list (free each with jerk_free). */
+int jerk_search_begin(jerk_plan *plan, const void *spectrum, int spectrum_on_device,
+                      long long first_rstep, long long num_rsteps);
+int jerk_group_advance(jerk_plan *const *plans, int nplans, int ahead);
+int jerk_search_group(jerk_plan *const *plans, const void *const *spectra,
+                      const int *spectrum_on_device, int nplans, jerk_cand **cands,
+                      long long *ncands);
+
 /* Device memory the plan holds (volumes, tables, hit buffer, its own bank). */
 long long jerk_plan_device_bytes(const jerk_plan *plan);
 

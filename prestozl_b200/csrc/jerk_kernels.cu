@@ -208,10 +208,9 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
     }
 }
 
-__global__ void __launch_bounds__(1024) prep_kernel(const SearchDev P)
+__device__ __forceinline__ void prep_dispatch(const SearchDev &P, int b, int s)
 {
     extern __shared__ float smem[];
-    const int b = blockIdx.x, s = blockIdx.y;
     switch (P.subs[s].fftlen) {
 #define JERK_PREP_CASE(NN)                   \
     case NN:                                 \
@@ -235,6 +234,28 @@ __global__ void __launch_bounds__(1024) prep_kernel(const SearchDev P)
     default:
         break;
     }
+}
+
+__global__ void __launch_bounds__(1024) prep_kernel(const __grid_constant__ SearchDev P)
+{
+    prep_dispatch(P, blockIdx.x, blockIdx.y);
+}
+
+// plan i of the wave: index of the plan that owns flat CTA x
+__device__ __forceinline__ int group_plan(const GroupLaunch &M, int x)
+{
+    int i = 0;
+    while (i + 1 < M.n && x >= M.cta0[i + 1])
+        i++;
+    return i;
+}
+
+__global__ void __launch_bounds__(1024) prep_group_kernel(const __grid_constant__ GroupLaunch M)
+{
+    const int i = group_plan(M, blockIdx.x);
+    const int local = blockIdx.x - M.cta0[i];
+    const int nsubs = M.P[i].nsubs;
+    prep_dispatch(M.P[i], local / nsubs, local % nsubs);
 }
 
 // ---------------------------------------------------------------------------
@@ -306,9 +327,11 @@ __device__ __forceinline__ bool bar_wait(uint64_t *bar, unsigned parity)
 constexpr unsigned kStatusRind = 1u;     // harmsum: a subharmonic r index left its row
 constexpr unsigned kStatusCopy = 2u;     // corr: a data-row copy did not complete
 
+// One CTA: kernel row `row` of the fftlen-N group G, rsteps [b0, b1) of the
+// batch.  probe: this is the plan's first CTA (the wait probe runs there).
 template <int N>
-__global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
-    corr_kernel(const SearchDev P, const RowGroup G)
+__device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G, const int row,
+                                          const int b0, const int b1, const bool probe)
 {
     constexpr int R0 = FftPlan<N>::R0;
     constexpr int T = FftPlan<N>::T;
@@ -321,7 +344,6 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     float2 *tws = sm2 + fft_buf_len<N>();
     float2 *dsm = sm2 + CorrSmem<N>::kBase;  // staged data row (kStage)
     const int tid = threadIdx.x;
-    const int row = blockIdx.x;
     int gi = 0;
     while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
         gi++;
@@ -329,10 +351,6 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     const int lrow = row - G.rowstart[gi];
     const SubDev sd = P.subs[s];
     const float2 *D0 = P.prepped + sd.data_off;
-    // this CTA's rsteps: all of the batch, or a share of them when a small
-    // group's rows alone would leave SMs idle (gridDim.y > 1)
-    const int bchunk = (P.nb + (int)gridDim.y - 1) / (int)gridDim.y;
-    const int b0 = min(P.nb, (int)blockIdx.y * bchunk), b1 = min(P.nb, b0 + bchunk);
 
     if constexpr (kStage) {
         if (tid == 0) {
@@ -350,7 +368,7 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
             tws[i] = P.twiddles[sd.twoff + i];
     }
 
-    if (P.wait_probe && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+    if (P.wait_probe && probe && tid == 0) {
         // a wait that must run out: phase 0 of s_probe never completes
         __shared__ uint64_t s_probe;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_probe)) : "memory");
@@ -410,6 +428,36 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
         }
         __syncthreads();
     }
+}
+
+// this CTA's rsteps: all of the batch, or a share of them when a small
+// group's rows alone would leave SMs idle (ny > 1 chunks)
+__device__ __forceinline__ void rstep_chunk(int nb, int ny, int y, int *b0, int *b1)
+{
+    const int bchunk = (nb + ny - 1) / ny;
+    *b0 = min(nb, y * bchunk);
+    *b1 = min(nb, *b0 + bchunk);
+}
+
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
+    corr_kernel(const __grid_constant__ SearchDev P, const __grid_constant__ RowGroup G)
+{
+    int b0, b1;
+    rstep_chunk(P.nb, (int)gridDim.y, (int)blockIdx.y, &b0, &b1);
+    corr_body<N>(P, G, blockIdx.x, b0, b1, blockIdx.x == 0 && blockIdx.y == 0);
+}
+
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
+    corr_group_kernel(const __grid_constant__ GroupLaunch M)
+{
+    const int i = group_plan(M, blockIdx.x);
+    const int local = blockIdx.x - M.cta0[i];
+    const int ny = M.ny[i];
+    int b0, b1;
+    rstep_chunk(M.P[i].nb, ny, local % ny, &b0, &b1);
+    corr_body<N>(M.P[i], M.G[i], local / ny, b0, b1, local == 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -515,9 +563,11 @@ __device__ __noinline__ void harmsum_rare_hits(const SearchDev &P, const int *hs
     }
 }
 
+// One CTA: r block bx of fundamental w row ii of rstep b.  T (the tensor maps)
+// is read only with PF.
 template <int S, int ZU, bool PF>
-__global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
-    harmsum_kernel(const SearchDev P, const __grid_constant__ HarmTma T)
+__device__ __forceinline__ void harmsum_body(const SearchDev &P, const HarmTma *T, const int bx,
+                                             const int ii, const int b)
 {
     constexpr int kHarmZ = ZU;
     static_assert(ZU == 4 || ZU == 8, "whole int4s of z offsets");
@@ -530,10 +580,8 @@ __global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
     __shared__ int s_numrs[NS];
     const int numz0 = P.numz0;
     const int pitch = zrow_pitch(numz0);
-    const int b = blockIdx.z;
-    const int ii = blockIdx.y;
     const int tid = threadIdx.x;
-    const int kk = blockIdx.x * kHarmThreads + tid;
+    const int kk = bx * kHarmThreads + tid;
     const bool valid = kk < P.corr_uselen;
     const long long rstep = P.first_rstep + b;
 
@@ -545,7 +593,7 @@ __global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
                                      (long long)wind * sd.numz * sd.stride);
         s_numrs[tid] = P.steps[rstep * NS + tid].numrs;
         if constexpr (PF) {
-            const int k0 = blockIdx.x * kHarmThreads;
+            const int k0 = bx * kHarmThreads;
             s_pwind[tid] = wind;
             s_prstart[tid] = tid == 0 ? k0
                                       : (int)(P.rinds[((long long)b * NS + tid) * P.corr_uselen + k0] &
@@ -586,8 +634,8 @@ __global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
     constexpr int NA = NS > 1 ? NS / 2 : 1;
     if constexpr (PF) {
         if (tid == 0) {
-            prefetch_tile<NS>(P, T, 0, s_prstart, s_pwind, b);
-            prefetch_tile<NS>(P, T, kPrefetchRows, s_prstart, s_pwind, b);
+            prefetch_tile<NS>(P, *T, 0, s_prstart, s_pwind, b);
+            prefetch_tile<NS>(P, *T, kPrefetchRows, s_prstart, s_pwind, b);
         }
     }
     for (int jj0 = 0; jj0 < numz0; jj0 += kHarmZ) {
@@ -595,7 +643,7 @@ __global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
         if constexpr (PF) {
             // one tile ahead of the rows being gathered
             if (tid == 0 && jj0 > 0 && jj0 % kPrefetchRows == 0)
-                prefetch_tile<NS>(P, T, jj0 + kPrefetchRows, s_prstart, s_pwind, b);
+                prefetch_tile<NS>(P, *T, jj0 + kPrefetchRows, s_prstart, s_pwind, b);
         }
         float v[kHarmZ];
         unsigned int hm = 0;  // bit stage * ZU + u: row u crossed that stage's cutoff
@@ -671,6 +719,24 @@ __global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
         if (hm)
             harmsum_rare_hits<S>(P, hsm, pitch, s_base, b, ii, kk, jj0, hm, kHarmZ);
     }
+}
+
+template <int S, int ZU, bool PF>
+__global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, ZU>::value)
+    harmsum_kernel(const __grid_constant__ SearchDev P, const __grid_constant__ HarmTma T)
+{
+    harmsum_body<S, ZU, PF>(P, &T, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// The gather form over a wave of plans with S stages each (no prefetch).
+template <int S>
+__global__ void __launch_bounds__(kHarmThreads, HarmOcc<S, 4>::value)
+    harmsum_group_kernel(const __grid_constant__ GroupLaunch M)
+{
+    const int i = group_plan(M, blockIdx.x);
+    const int local = blockIdx.x - M.cta0[i];
+    const int nx = M.ny[i], nw = M.P[i].numw0;
+    harmsum_body<S, 4, false>(M.P[i], nullptr, local % nx, (local / nx) % nw, local / (nx * nw));
 }
 
 // ---------------------------------------------------------------------------
@@ -1041,6 +1107,117 @@ static cudaError_t launch_harmsum_p(const SearchDev &P, const HarmTma &T, cudaSt
 cudaError_t launch_harmsum(const SearchDev &P, const HarmTma &T, bool prefetch, cudaStream_t st)
 {
     return prefetch ? launch_harmsum_p<true>(P, T, st) : launch_harmsum_p<false>(P, T, st);
+}
+
+// ---------------------------------------------------------------------------
+// Waves: one launch per kernel kind over the current batches of several
+// plans.  The caller fills M.n, M.P and (corr) M.G; the launchers fill the
+// CTA ranges.
+
+cudaError_t launch_prep_group(GroupLaunch M, int maxfft, cudaStream_t st)
+{
+    if (M.n < 1 || M.n > kMaxGroupPlans)
+        return cudaErrorInvalidValue;
+    int x = 0;
+    for (int i = 0; i < M.n; i++) {
+        M.cta0[i] = x;
+        M.ny[i] = 1;
+        x += M.P[i].nb * M.P[i].nsubs;
+    }
+    M.cta0[M.n] = x;
+    const size_t smem = prep_smem_bytes(maxfft);
+    cudaError_t e = cudaFuncSetAttribute(prep_group_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    prep_group_kernel<<<x, prep_threads(maxfft), smem, st>>>(M);
+    return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t launch_corr_group_n(GroupLaunch &M, cudaStream_t st)
+{
+    const size_t smem = sizeof(float2) * CorrSmem<N>::value;
+    cudaError_t e = cudaFuncSetAttribute(corr_group_kernel<N>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(corr_group_kernel<N>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess)
+        return e;
+    // the single-plan rule, applied to the wave's rows together: fewer rows
+    // than two waves of CTAs also split their rsteps
+    const int wave = sm_count() * CorrOcc<N>::value;
+    long long total = 0;
+    for (int i = 0; i < M.n; i++)
+        total += M.G[i].rowstart[M.G[i].n];
+    long long x = 0;
+    for (int i = 0; i < M.n; i++) {
+        const int rows = M.G[i].rowstart[M.G[i].n];
+        const int split = total >= 2 * wave ? 1
+                          : std::max(1, std::min(M.P[i].nb, (int)((2 * wave + total - 1) / total)));
+        M.cta0[i] = (int)x;
+        M.ny[i] = split;
+        x += (long long)rows * split;
+    }
+    if (x >= (1ll << 31))
+        return cudaErrorInvalidValue;
+    M.cta0[M.n] = (int)x;
+    corr_group_kernel<N><<<(unsigned)x, FftPlan<N>::T, smem, st>>>(M);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corr_group(GroupLaunch M, int fftlen, cudaStream_t st)
+{
+    if (M.n < 1 || M.n > kMaxGroupPlans)
+        return cudaErrorInvalidValue;
+    switch (fftlen) {
+#define JERK_CG(NN) case NN: return launch_corr_group_n<NN>(M, st);
+    JERK_CG(128) JERK_CG(192) JERK_CG(256) JERK_CG(384) JERK_CG(512) JERK_CG(768)
+    JERK_CG(1024) JERK_CG(1280) JERK_CG(2048) JERK_CG(4096) JERK_CG(5120) JERK_CG(7680)
+    JERK_CG(10240) JERK_CG(15360)
+#undef JERK_CG
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int S>
+static cudaError_t launch_harmsum_group_s(GroupLaunch &M, cudaStream_t st)
+{
+    size_t smem = 0;
+    long long x = 0;
+    for (int i = 0; i < M.n; i++) {
+        const SearchDev &P = M.P[i];
+        smem = std::max(smem, harmsum_smem_bytes(P.nsubs, P.numz0));
+        M.cta0[i] = (int)x;
+        M.ny[i] = (P.corr_uselen + kHarmThreads - 1) / kHarmThreads;
+        x += (long long)M.ny[i] * P.numw0 * P.nb;
+    }
+    if (x >= (1ll << 31))
+        return cudaErrorInvalidValue;
+    M.cta0[M.n] = (int)x;
+    cudaError_t e = cudaFuncSetAttribute(harmsum_group_kernel<S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    harmsum_group_kernel<S><<<(unsigned)x, kHarmThreads, smem, st>>>(M);
+    return cudaGetLastError();
+}
+
+// Every plan of M must have nstages stages.
+cudaError_t launch_harmsum_group(GroupLaunch M, int nstages, cudaStream_t st)
+{
+    if (M.n < 1 || M.n > kMaxGroupPlans)
+        return cudaErrorInvalidValue;
+    switch (nstages) {
+    case 1: return launch_harmsum_group_s<1>(M, st);
+    case 2: return launch_harmsum_group_s<2>(M, st);
+    case 3: return launch_harmsum_group_s<3>(M, st);
+    case 4: return launch_harmsum_group_s<4>(M, st);
+    case 5: return launch_harmsum_group_s<5>(M, st);
+    case 6: return launch_harmsum_group_s<6>(M, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 size_t harmsum_tma_smem_bytes(const HarmTma &T, int nsubs, int numz0)

@@ -108,6 +108,22 @@ struct RowGroup {
     int rowstart[kMaxSubs + 1];  // prefix sums of numw * numz
 };
 
+// One merged launch over the current batches of several plans (a "wave"):
+// flat CTA index x belongs to plan i for cta0[i] <= x < cta0[i + 1], and
+// that plan's part runs exactly the CTAs its own launch would run, with its
+// own arguments, so every plan's results are bitwise those of its own
+// launches.  ny[i]: corr -- rstep chunks per kernel row; harmsum -- r blocks
+// per w row.  Passed by value as a __grid_constant__ parameter.
+constexpr int kMaxGroupPlans = 12;
+struct GroupLaunch {
+    int n;
+    int cta0[kMaxGroupPlans + 1];
+    int ny[kMaxGroupPlans];
+    SearchDev P[kMaxGroupPlans];
+    RowGroup G[kMaxGroupPlans];
+};
+static_assert(sizeof(GroupLaunch) <= 30000, "kernel parameter space");
+
 // Records msg as the text jerk_last_error returns and passes code back.
 int set_error(int code, const char *msg);
 // w_resp_halfwidth(z, w, LOWACC) (src/responses.c:49-84).

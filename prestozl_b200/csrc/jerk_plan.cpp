@@ -35,6 +35,9 @@ cudaError_t launch_harmsum(const SearchDev &P, const HarmTma &T, bool prefetch, 
 cudaError_t launch_harmsum_tma(const SearchDev &P, const HarmTma &T, int zt, cudaStream_t st);
 size_t harmsum_tma_smem_bytes(const HarmTma &T, int nsubs, int numz0);
 bool fftlen_supported(int n);
+cudaError_t launch_prep_group(GroupLaunch M, int maxfft, cudaStream_t st);
+cudaError_t launch_corr_group(GroupLaunch M, int fftlen, cudaStream_t st);
+cudaError_t launch_harmsum_group(GroupLaunch M, int nstages, cudaStream_t st);
 int fft_twiddle_size(int N);
 void fft_twiddle_table(int N, float2 *out);
 cudaError_t launch_bank_response(const BankRow *rows, int nrows, int max_pts, float2 *bank,
@@ -1332,6 +1335,22 @@ static inline double fft_flops(int n)
     return 5.0 * n * log2((double)n);
 }
 
+// The rows of the subharmonics subs (one fftlen), numbered consecutively.
+static RowGroup row_group(const jerk_plan *p, const std::vector<int> &subs)
+{
+    RowGroup G{};
+    G.n = (int)subs.size();
+    int rows = 0;
+    for (int i = 0; i < G.n; i++) {
+        const int s = subs[i];
+        G.sub[i] = s;
+        G.rowstart[i] = rows;
+        rows += p->subs[s].numw * p->subs[s].numz;
+    }
+    G.rowstart[G.n] = rows;
+    return G;
+}
+
 static int run_volumes(jerk_plan *p, SearchDev &a)
 {
     {
@@ -1349,16 +1368,8 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
     }
     cudaError_t e = cudaSuccess;
     for (auto &kv : p->groups) {
-        RowGroup G{};
-        G.n = (int)kv.second.size();
-        int rows = 0;
-        for (int i = 0; i < G.n; i++) {
-            const int s = kv.second[i];
-            G.sub[i] = s;
-            G.rowstart[i] = rows;
-            rows += p->subs[s].numw * p->subs[s].numz;
-        }
-        G.rowstart[G.n] = rows;
+        const RowGroup G = row_group(p, kv.second);
+        const int rows = G.rowstart[G.n];
         // algorithmic traffic: each kernel row read once per batch, each
         // prepared chunk read once, every good power written once
         const int N = kv.first;
@@ -1409,6 +1420,30 @@ static long long pass_done_batches(jerk_plan *p)
     return ps.ndone;
 }
 
+// The plan's own harmonic-sum launch for batch arguments a.
+static cudaError_t launch_harmsum_of(const jerk_plan *p, const SearchDev &a, cudaStream_t st)
+{
+    static const HarmTma no_maps{};
+    return p->harm_mode >= 3 ? launch_harmsum_tma(a, *p->tma, p->harm_tile, st)
+           : p->harm_mode == 2 ? launch_harmsum(a, *p->tma, true, st)
+                               : launch_harmsum(a, no_maps, false, st);
+}
+
+// algorithmic traffic of one batch's harmonic sum: every volume read once
+static void harmsum_work(const jerk_plan *p, const SearchDev &a, double *bytes, double *flops)
+{
+    double b = 0;
+    const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
+    for (int s = 0; s < p->nsubs; s++) {
+        double numrs = 0;
+        for (int k = 0; k < a.nb; k++)
+            numrs += p->hsteps[(size_t)(a.first_rstep + k) * p->nsubs + s].numrs;
+        b += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
+    }
+    *bytes += b;
+    *flops += npts * p->nsubs;
+}
+
 static int pass_enqueue_one(jerk_plan *p)
 {
     jerk_plan::Pass &ps = p->pass;
@@ -1421,21 +1456,10 @@ static int pass_enqueue_one(jerk_plan *p)
     int rc = run_volumes(p, a);
     if (rc != JERK_OK)
         return rc;
-    // algorithmic traffic: every volume of the batch read once
     double bytes = 0, flops = 0;
-    const double npts = (double)a.nb * p->subs[0].numw * p->subs[0].numz * p->obs.corr_uselen;
-    for (int s = 0; s < p->nsubs; s++) {
-        double numrs = 0;
-        for (int b = 0; b < a.nb; b++)
-            numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
-        bytes += (double)p->subs[s].numw * p->subs[s].numz * numrs * 4.0;
-    }
-    flops = npts * p->nsubs;
+    harmsum_work(p, a, &bytes, &flops);
     const int tok = launch_begin(p, kclass(p, "harmsum"), bytes, flops);
-    static const HarmTma no_maps{};
-    cudaError_t e = p->harm_mode >= 3 ? launch_harmsum_tma(a, *p->tma, p->harm_tile, p->stream)
-                    : p->harm_mode == 2 ? launch_harmsum(a, *p->tma, true, p->stream)
-                                        : launch_harmsum(a, no_maps, false, p->stream);
+    cudaError_t e = launch_harmsum_of(p, a, p->stream);
     launch_end(p, tok);
     if (e != cudaSuccess)
         return cuda_fail(e, "harmsum_kernel");
@@ -1632,6 +1656,233 @@ extern "C" int jerk_search_ready(jerk_plan *p)
     if (e == cudaErrorNotReady)
         return 0;
     return cuda_fail(e, "jerk_search_ready");
+}
+
+// ---------------------------------------------------------------------------
+// Waves: the current batches of several plans' passes in merged launches --
+// one prep launch, one correlation launch per FFT length and one harmonic
+// sum per stage count, each covering every plan of the wave (up to
+// kMaxGroupPlans) -- so spectra of uneven length and geometry share launches
+// and small ones fill the GPU together.  Every plan's CTAs run as in its own
+// launches, so its results are bitwise the same.
+
+extern "C" int jerk_search_begin(jerk_plan *p, const void *spectrum, int spectrum_on_device,
+                                 long long first_rstep, long long num_rsteps)
+{
+    if (!p || !spectrum)
+        return fail(JERK_EINVAL, "jerk_search_begin: null argument");
+    if (p->in_flight)
+        return fail(JERK_EINVAL, "jerk_search_begin: a search is already in flight on this plan");
+    long long count = 0;
+    int rc = check_range(p, first_rstep, num_rsteps, &count);
+    if (rc != JERK_OK)
+        return rc;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != p->device)
+        JERK_CUDA(cudaSetDevice(p->device));
+    const float2 *spec = nullptr;
+    rc = stage_spectrum(p, spectrum, spectrum_on_device, &spec);
+    if (rc == JERK_OK)
+        rc = pass_begin(p, spec, first_rstep, count);
+    if (rc != JERK_OK)
+        return rc;
+    p->in_flight = true;
+    p->inflight_spec = spec;
+    p->inflight_first = first_rstep;
+    p->inflight_count = count;
+    return JERK_OK;
+}
+
+// One wave over W (same stream): every plan's next batch.
+static int enqueue_wave(const std::vector<jerk_plan *> &W)
+{
+    jerk_plan *p0 = W[0];
+    cudaStream_t st = p0->stream;
+    const int n = (int)W.size();
+    int maxfft = 0;
+    double pbytes = 0, pflops = 0;
+    for (jerk_plan *p : W) {
+        jerk_plan::Pass &ps = p->pass;
+        SearchDev &a = ps.a;
+        a.first_rstep = ps.next;
+        a.nb = (int)std::min<long long>(p->batch, ps.first + ps.count - ps.next);
+        a.planes = p->d_planes;
+        a.rinds = p->d_rinds;
+        maxfft = std::max(maxfft, p->maxfft);
+        for (int s = 0; s < p->nsubs; s++) {
+            const int N = p->subs[s].fftlen;
+            pbytes += (double)a.nb * (N / 2 * 8.0 + N * 8.0);
+            pflops += (double)a.nb * fft_flops(N);
+        }
+    }
+    auto fail_all = [&](cudaError_t e, const char *what) {
+        const int rc = cuda_fail(e, what);
+        for (jerk_plan *p : W)
+            p->pass.error = rc;
+        return rc;
+    };
+    GroupLaunch M{};
+    M.n = n;
+    for (int i = 0; i < n; i++)
+        M.P[i] = W[i]->pass.a;
+    int tok = launch_begin(p0, kclass(p0, "wave_prep"), pbytes, pflops);
+    cudaError_t e = launch_prep_group(M, maxfft, st);
+    launch_end(p0, tok);
+    if (e != cudaSuccess)
+        return fail_all(e, "prep_group_kernel");
+
+    // correlation: one launch per FFT length over every plan that has it
+    std::map<int, std::vector<int>> byN;
+    for (int i = 0; i < n; i++)
+        for (auto &kv : W[i]->groups)
+            byN[kv.first].push_back(i);
+    for (auto &kv : byN) {
+        const int N = kv.first;
+        GroupLaunch C{};
+        C.n = (int)kv.second.size();
+        double bytes = 0, flops = 0;
+        for (int j = 0; j < C.n; j++) {
+            jerk_plan *p = W[kv.second[j]];
+            const SearchDev &a = p->pass.a;
+            C.P[j] = a;
+            C.G[j] = row_group(p, p->groups.at(N));
+            for (int g = 0; g < C.G[j].n; g++) {
+                const int s = C.G[j].sub[g];
+                const double nrow = (double)p->subs[s].numw * p->subs[s].numz;
+                double numrs = 0;
+                for (int b = 0; b < a.nb; b++)
+                    numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
+                bytes += nrow * N * 8.0 + a.nb * N * 8.0 + nrow * numrs * 4.0;
+                flops += nrow * a.nb * (fft_flops(N) + 6.0 * N) + nrow * numrs * 3.0;
+            }
+        }
+        tok = launch_begin(p0, kclass(p0, "wave_corr_" + std::to_string(N)), bytes, flops);
+        e = launch_corr_group(C, N, st);
+        launch_end(p0, tok);
+        if (e != cudaSuccess)
+            return fail_all(e, "corr_group_kernel");
+    }
+
+    // harmonic sums: the gather form merged per stage count; plans tuned to
+    // another form launch their own
+    std::map<int, std::vector<int>> byS;
+    for (int i = 0; i < n; i++) {
+        jerk_plan *p = W[i];
+        if (p->harm_mode <= 1) {
+            byS[p->obs.numharmstages].push_back(i);
+            continue;
+        }
+        double bytes = 0, flops = 0;
+        harmsum_work(p, p->pass.a, &bytes, &flops);
+        tok = launch_begin(p0, kclass(p0, "wave_harmsum"), bytes, flops);
+        e = launch_harmsum_of(p, p->pass.a, st);
+        launch_end(p0, tok);
+        if (e != cudaSuccess)
+            return fail_all(e, "harmsum_kernel");
+    }
+    for (auto &kv : byS) {
+        GroupLaunch H{};
+        H.n = (int)kv.second.size();
+        double bytes = 0, flops = 0;
+        for (int j = 0; j < H.n; j++) {
+            jerk_plan *p = W[kv.second[j]];
+            H.P[j] = p->pass.a;
+            harmsum_work(p, p->pass.a, &bytes, &flops);
+        }
+        tok = launch_begin(p0, kclass(p0, "wave_harmsum"), bytes, flops);
+        e = launch_harmsum_group(H, kv.first, st);
+        launch_end(p0, tok);
+        if (e != cudaSuccess)
+            return fail_all(e, "harmsum_group_kernel");
+    }
+
+    for (jerk_plan *p : W) {
+        jerk_plan::Pass &ps = p->pass;
+        JERK_CUDA(cudaEventRecord(p->ev_batch[ps.nbatch % jerk_plan::kRing], st));
+        ps.next += ps.a.nb;
+        ps.nbatch++;
+        if (ps.next >= ps.first + ps.count) {
+            const int rc = pass_finish_enqueue(p);
+            if (rc != JERK_OK)
+                return ps.error = rc;
+        }
+    }
+    return JERK_OK;
+}
+
+extern "C" int jerk_group_advance(jerk_plan *const *plans, int nplans, int ahead)
+{
+    if (!plans || nplans < 0)
+        return fail(JERK_EINVAL, "jerk_group_advance: bad argument");
+    jerk_plan *first = nullptr;
+    for (int i = 0; i < nplans; i++) {
+        jerk_plan *p = plans[i];
+        if (!p)
+            return fail(JERK_EINVAL, "jerk_group_advance: null plan");
+        if (!p->in_flight || p->pass.all_enqueued || p->pass.error)
+            continue;
+        if (!first)
+            first = p;
+        else if (p->stream != first->stream || p->device != first->device)
+            return fail(JERK_EINVAL, "jerk_group_advance: plans on different streams or devices");
+    }
+    if (!first)
+        return 0;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != first->device)
+        JERK_CUDA(cudaSetDevice(first->device));
+    const int limit = ahead <= 0 ? 1 << 30 : std::min(ahead, jerk_plan::kRing - 2);
+    for (;;) {
+        std::vector<jerk_plan *> sel;
+        bool left = false;
+        for (int i = 0; i < nplans; i++) {
+            jerk_plan *p = plans[i];
+            jerk_plan::Pass &ps = p->pass;
+            if (!p->in_flight || ps.all_enqueued || ps.error)
+                continue;
+            left = true;
+            if (ps.nbatch - pass_done_batches(p) < limit)
+                sel.push_back(p);
+        }
+        if (sel.empty())
+            return left ? 1 : 0;
+        for (size_t i = 0; i < sel.size(); i += kMaxGroupPlans) {
+            std::vector<jerk_plan *> W(sel.begin() + i,
+                                       sel.begin() + std::min(sel.size(), i + kMaxGroupPlans));
+            const int rc = enqueue_wave(W);
+            if (rc != JERK_OK)
+                return rc;
+        }
+    }
+}
+
+extern "C" int jerk_search_group(jerk_plan *const *plans, const void *const *spectra,
+                                 const int *spectrum_on_device, int nplans, jerk_cand **cands,
+                                 long long *ncands)
+{
+    if (!plans || !spectra || !spectrum_on_device || !cands || !ncands || nplans < 1)
+        return fail(JERK_EINVAL, "jerk_search_group: bad argument");
+    for (int i = 0; i < nplans; i++) {
+        cands[i] = nullptr;
+        ncands[i] = 0;
+    }
+    int rc = JERK_OK, began = 0;
+    for (; began < nplans && rc == JERK_OK; began++)
+        rc = jerk_search_begin(plans[began], spectra[began], spectrum_on_device[began], 0, 0);
+    if (rc != JERK_OK)
+        began--;  // the failed one holds no pass
+    if (rc == JERK_OK)
+        rc = jerk_group_advance(plans, nplans, 0);
+    // every begun pass is collected (ends its in-flight state), even after a
+    // failure; the first error is returned
+    for (int i = 0; i < began; i++) {
+        const int r = jerk_search_collect(plans[i], &cands[i], &ncands[i], nullptr);
+        if (rc == JERK_OK)
+            rc = r;
+    }
+    return rc;
 }
 
 // What decoding a hit key needs: the fundamental's geometry and, per rstep,

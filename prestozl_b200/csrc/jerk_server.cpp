@@ -10,10 +10,13 @@
 // (zmax, wmax, numharm, geometry) and shared by every request that matches;
 // idle plans with identical geometry are reused instead of reallocated.
 //
-// The active searches share one stream: the worker enqueues their batches
-// round-robin, a few ahead of the device each, so the GPU runs one kernel at
-// a time, back to back (kernels of different searches sharing SMs measured
-// slower than the same kernels in sequence), while every request advances.
+// The active searches share one stream, and their work overlaps on the
+// device: the worker enqueues waves (jerk_group_advance), each one merged
+// launch per kernel kind over the next batch of every active search, a few
+// waves ahead of the device.  A request admitted while others run joins the
+// next wave.  (Kernels of different searches on separate streams sharing SMs
+// measured slower than the same kernels in sequence; merged launches give
+// the overlap without that contention.)
 //
 // It is built only on the public C ABI of jerk.h, so its results are exactly
 // jerk_search's for the same spectrum and parameters, alone or in a mix.
@@ -360,9 +363,9 @@ static bool admit(jerk_server *s, const Pending &pd)
     if (pd.req.timeseries) {
         rc = prepare_series(s, sl);
         if (rc == JERK_OK)
-            rc = jerk_search_async(sl.plan, sl.series, 1, 0, 0);
+            rc = jerk_search_begin(sl.plan, sl.series, 1, 0, 0);
     } else {
-        rc = jerk_search_async(sl.plan, pd.req.spectrum, pd.req.on_device, 0, 0);
+        rc = jerk_search_begin(sl.plan, pd.req.spectrum, pd.req.on_device, 0, 0);
     }
     if (rc != JERK_OK) {
         if (sl.series)
@@ -421,11 +424,17 @@ static void worker_main(jerk_server *s)
             for (auto &pd : expired)
                 finish(s, pd.req, pd.t_submit, now_s(), JERK_TIMEOUT, nullptr, 0);
         }
-        // keep every active search a few batches ahead of the device, round
-        // robin, so every admitted request advances
+        // keep every active search a few batches ahead of the device, in
+        // waves of merged launches over all of them
         bool progressed = false;
-        for (auto &sl : s->active)
-            jerk_search_advance(sl.plan, s->cfg.batches_ahead);  // errors: jerk_search_ready
+        {
+            std::vector<jerk_plan *> plans;
+            for (auto &sl : s->active)
+                plans.push_back(sl.plan);
+            if (!plans.empty())
+                jerk_group_advance(plans.data(), (int)plans.size(),
+                                   s->cfg.batches_ahead);  // errors: jerk_search_ready
+        }
 
         // completions
         for (size_t i = 0; i < s->active.size();) {

@@ -117,6 +117,7 @@ EXPORTS = [
     "jerk_optimize_cand", "jerk_downsample_subbands", "jerk_dedisperser_create",
     "jerk_dedisperser_destroy", "jerk_dedisperser_shape", "jerk_dedisperser_matches",
     "jerk_dedisp_subbands", "jerk_dedisp_plan", "jerk_debug_wait_probe", "jerk_merge_hits",
+    "jerk_search_begin", "jerk_group_advance", "jerk_search_group",
 ]
 
 
@@ -146,6 +147,11 @@ def lib() -> C.CDLL:
     L.jerk_debug_volume.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int,
                                     C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
     L.jerk_debug_wait_probe.argtypes = [C.c_void_p, C.c_int]
+    L.jerk_search_begin.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_longlong]
+    L.jerk_group_advance.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int]
+    L.jerk_search_group.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                    C.POINTER(C.c_int), C.c_int,
+                                    C.POINTER(C.POINTER(Cand)), C.POINTER(C.c_longlong)]
     L.jerk_merge_hits.argtypes = [C.POINTER(Obs), C.POINTER(Subharm), C.c_void_p, C.c_void_p,
                                   C.c_longlong, C.POINTER(C.POINTER(Cand)),
                                   C.POINTER(C.c_longlong)]
@@ -668,6 +674,36 @@ class JerkPlan:
         lib().jerk_free(C.cast(hits.powers, C.c_void_p))
         return cands, k, p
 
+    def begin(self, spectrum, first_rstep: int = 0, num_rsteps: int = 0) -> None:
+        """Start a pass whose batches come from group_advance (jerk_search_begin).
+        The spectrum must stay alive until collect()."""
+        ptr, dev, keep = _spectrum_arg(spectrum)
+        _check(lib().jerk_search_begin(self._p, ptr, dev, first_rstep, num_rsteps))
+        self._inflight_keep = keep
+
+    def collect(self, want_hits: bool = False):
+        """Finish the pass in flight (jerk_search_collect): candidates, and
+        optionally the raw hits, as search() returns them."""
+        out = C.POINTER(Cand)()
+        n = C.c_longlong(0)
+        hits = Hits()
+        try:
+            _check(lib().jerk_search_collect(self._p, C.byref(out), C.byref(n),
+                                             C.byref(hits) if want_hits else None))
+        finally:
+            self._inflight_keep = None
+        nb = n.value * CAND_DTYPE.itemsize
+        cands = np.frombuffer(C.string_at(out, nb), dtype=CAND_DTYPE).copy() if nb else \
+            np.zeros(0, dtype=CAND_DTYPE)
+        lib().jerk_free(out)
+        if not want_hits:
+            return cands
+        k = np.ctypeslib.as_array(hits.keys, shape=(max(hits.count, 1),))[: hits.count].copy()
+        p = np.ctypeslib.as_array(hits.powers, shape=(max(hits.count, 1),))[: hits.count].copy()
+        lib().jerk_free(C.cast(hits.keys, C.c_void_p))
+        lib().jerk_free(C.cast(hits.powers, C.c_void_p))
+        return cands, k, p
+
     def set_profiling(self, on: bool) -> None:
         _check(lib().jerk_plan_set_profiling(self._p, int(on)))
 
@@ -713,6 +749,42 @@ class JerkPlan:
         ii = k % numw; k //= numw
         st = k % S; rs = k // S
         return rs, st, ii, jj, kk
+
+
+def group_advance(plans: Sequence["JerkPlan"], ahead: int = 0) -> int:
+    """Enqueue waves of merged launches over the plans' passes in flight
+    (jerk_group_advance): 1 while batches remain, 0 once all are enqueued."""
+    n = len(plans)
+    parr = (C.c_void_p * max(n, 1))(*[p._p.value for p in plans])
+    rc = lib().jerk_group_advance(parr, n, ahead)
+    if rc < 0:
+        _check(rc)
+    return rc
+
+
+def search_group(plans: Sequence["JerkPlan"], spectra) -> List[np.ndarray]:
+    """Whole-spectrum searches of several plans (any geometries, one shared
+    stream) in waves of merged launches (jerk_search_group); returns each
+    plan's candidate list, bitwise what plan.search(spectrum) returns."""
+    n = len(plans)
+    if n != len(spectra) or n < 1:
+        raise JerkError(JERK_EINVAL, "search_group: one spectrum per plan")
+    args = [_spectrum_arg(s) for s in spectra]
+    parr = (C.c_void_p * n)(*[p._p.value for p in plans])
+    sarr = (C.c_void_p * n)(*[a[0].value for a in args])
+    darr = (C.c_int * n)(*[a[1] for a in args])
+    outs = (C.POINTER(Cand) * n)()
+    counts = (C.c_longlong * n)()
+    rc = lib().jerk_search_group(parr, sarr, darr, n, outs, counts)
+    res = []
+    for i in range(n):
+        nb = counts[i] * CAND_DTYPE.itemsize
+        res.append(np.frombuffer(C.string_at(outs[i], nb), dtype=CAND_DTYPE).copy() if nb
+                   else np.zeros(0, dtype=CAND_DTYPE))
+        if outs[i]:
+            lib().jerk_free(outs[i])
+    _check(rc)
+    return res
 
 
 def _cands_array(ptr, n: int) -> np.ndarray:
