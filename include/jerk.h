@@ -421,8 +421,10 @@ int jerk_dedisp_subbands(jerk_dedisperser *dedisperser, const float *cur, const 
  * Submitted spectra wait in a queue; a worker thread that owns the device
  * admits them while fewer than max_active searches run and their device
  * footprint fits hbm_budget_bytes, keeps the admitted searches in flight
- * together on their own streams, and queues each finished candidate list for
- * jerk_server_poll.  Kernel banks are generated once per search geometry and
+ * together -- their batches run in waves of merged launches on the server's
+ * stream (jerk_group_advance), so a request admitted while others run shares
+ * their launches from its next wave on -- and queues each finished
+ * candidate list for jerk_server_poll.  Kernel banks are generated once per search geometry and
  * shared; idle plans of the same geometry are reused.  A result equals
  * jerk_search's for the same spectrum and parameters.  (The reference's
  * counterpart is the process pool of bin/accelsearch_pipeline_cu.py.) */
@@ -433,7 +435,7 @@ typedef struct jerk_server_config {
     int max_active;              /* searches in flight at once; 0 = 3 */
     int batch_rsteps;            /* rsteps per batch of each plan; 0 = 16 */
     int device;                  /* CUDA device the worker owns */
-    int batches_ahead;           /* batches each search keeps queued; 0 = 3 */
+    int batches_ahead;           /* waves each search keeps queued; 0 = 3 */
     double queue_timeout_s;      /* a request not admitted within this fails
                                     with JERK_TIMEOUT; 0 = never */
     int harm_mode;               /* jerk_config.harm_mode of every plan */
