@@ -477,6 +477,9 @@ int jerk_server_submit(jerk_server *server, const jerk_request *req);
 int jerk_server_poll(jerk_server *server, jerk_result *out, int timeout_ms);
 /* out[6]: submitted, finished, failed, queued, peak device bytes, budget. */
 void jerk_server_stats(jerk_server *server, long long *out);
+/* Bytes copied host->device (host spectra and series) and device->host
+ * (hit counts and hit lists) for the requests finished so far. */
+void jerk_server_transfer_stats(jerk_server *server, long long *h2d, long long *d2h);
 /* Finishes every submitted request, then stops; unpolled results are freed. */
 void jerk_server_destroy(jerk_server *server);
 

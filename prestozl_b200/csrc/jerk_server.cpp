@@ -114,6 +114,7 @@ struct jerk_server {
     // counters (under mu)
     long long submitted = 0, finished = 0, failed = 0;
     long long peak_bytes = 0;
+    long long h2d_bytes = 0, d2h_bytes = 0;  // host<->device traffic of finished requests
 };
 
 static int geometry_of(const jerk_request &r, Geometry *g)
@@ -207,6 +208,10 @@ static int prepare_series(jerk_server *s, Slot &sl)
     }
     const long long sbytes = 4 * sl.req.N;
     const long long off = (sbytes + 255) & ~255LL;
+    if (!sl.req.on_device) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->h2d_bytes += sbytes;
+    }
     if (cudaMemcpyAsync(sl.series, sl.req.spectrum, (size_t)sbytes,
                         sl.req.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                         s->stream) != cudaSuccess)
@@ -447,6 +452,15 @@ static void worker_main(jerk_server *s)
             jerk_cand *c = nullptr;
             long long n = 0;
             const int rc = ready < 0 ? ready : jerk_search_collect(sl.plan, &c, &n, nullptr);
+            {
+                // the plan's own copies: a host spectrum in, hit lists out
+                long long h = 0, d = 0;
+                jerk_plan_transfer_stats(sl.plan, &h, &d);
+                jerk_plan_reset_stats(sl.plan);
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->h2d_bytes += h;
+                s->d2h_bytes += d;
+            }
             release_bank(s, sl.key);
             if (sl.series) {
                 if (rc < 0)
@@ -566,6 +580,20 @@ extern "C" void jerk_server_stats(jerk_server *s, long long *out)
     out[3] = (long long)s->pending.size();
     out[4] = s->peak_bytes;
     out[5] = s->cfg.hbm_budget_bytes;
+}
+
+extern "C" void jerk_server_transfer_stats(jerk_server *s, long long *h2d, long long *d2h)
+{
+    long long h = 0, d = 0;
+    if (s) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        h = s->h2d_bytes;
+        d = s->d2h_bytes;
+    }
+    if (h2d)
+        *h2d = h;
+    if (d2h)
+        *d2h = d;
 }
 
 extern "C" void jerk_server_destroy(jerk_server *s)

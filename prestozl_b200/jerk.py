@@ -117,7 +117,7 @@ EXPORTS = [
     "jerk_optimize_cand", "jerk_downsample_subbands", "jerk_dedisperser_create",
     "jerk_dedisperser_destroy", "jerk_dedisperser_shape", "jerk_dedisperser_matches",
     "jerk_dedisp_subbands", "jerk_dedisp_plan", "jerk_debug_wait_probe", "jerk_merge_hits",
-    "jerk_search_begin", "jerk_group_advance", "jerk_search_group",
+    "jerk_search_begin", "jerk_group_advance", "jerk_search_group", "jerk_server_transfer_stats",
 ]
 
 
@@ -189,6 +189,9 @@ def lib() -> C.CDLL:
     L.jerk_server_poll.argtypes = [C.c_void_p, C.POINTER(Result), C.c_int]
     L.jerk_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
     L.jerk_server_stats.restype = None
+    L.jerk_server_transfer_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong),
+                                             C.POINTER(C.c_longlong)]
+    L.jerk_server_transfer_stats.restype = None
     L.jerk_server_destroy.argtypes = [C.c_void_p]
     L.jerk_server_destroy.restype = None
     L.jerk_volume_static.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.POINTER(Subharm),
@@ -861,8 +864,12 @@ class JerkServer:
     def stats(self) -> dict:
         a = (C.c_longlong * 6)()
         lib().jerk_server_stats(self._s, a)
-        return dict(zip(["submitted", "finished", "failed", "queued", "peak_bytes", "budget"],
-                        list(a)))
+        out = dict(zip(["submitted", "finished", "failed", "queued", "peak_bytes", "budget"],
+                       list(a)))
+        h, d = C.c_longlong(0), C.c_longlong(0)
+        lib().jerk_server_transfer_stats(self._s, C.byref(h), C.byref(d))
+        out["h2d_bytes"], out["d2h_bytes"] = h.value, d.value
+        return out
 
     def close(self) -> None:
         if self._s:
