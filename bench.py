@@ -540,6 +540,246 @@ def _count_rsteps(obs) -> int:
 
 
 # --------------------------------------------------------------------------
+# The batched workload: 48 spectra of uneven length and geometry.
+
+MIX_LENGTHS = (1 << 22, 1 << 24, 1 << 25)
+MIX_GEOMS = ((50, 160), (200, 300), (100, 0))
+MIX_SIGMA = 3.0
+
+
+def mix_workload(n: int = 48):
+    """(N, zmax, wmax, numharm, seed) per spectrum: lengths 2^22 / 2^24 /
+    2^25 in turn, the three (zmax, wmax) pairs and numharm 8 / 16 spread over
+    them (16 spectra of each length; every combination occurs)."""
+    return [(MIX_LENGTHS[i % 3], *MIX_GEOMS[(i // 3) % 3], (8, 16)[(i // 9) % 2], 7000 + i)
+            for i in range(n)]
+
+
+def mix_spectrum(N: int, zmax: int, wmax: int, seed: int, device):
+    """Seeded Gaussian noise with 0-2 pulsars (up to 5 harmonics, SNR 8-20)
+    inside the geometry's f-dot / f-dot-dot range."""
+    from prestozl_b200 import synth
+
+    rng = np.random.default_rng(seed)
+    ps = synth.random_pulsars(rng, int(rng.integers(0, 3)), zmax=0.9 * zmax,
+                              wmax=0.9 * wmax if wmax else 0.0, snr=(8.0, 20.0), maxharm=5)
+    return synth.presto_fft_torch(synth.timeseries_torch(N, DT, ps, seed, device=device))
+
+
+def mix_leg(args, local: int):
+    """The batched workload three ways, on resident kernel banks:
+    plain drop-in -- what accelsearch_GPU does per spectrum: a plan at
+    -batchsize 8, the host spectrum copied in, the search, the plan freed;
+    sequential -- one search at a time at args.mix_batch rsteps per batch,
+    spectra and plans resident; batched -- the request loop, every spectrum
+    submitted at once, args.mix_active searches in flight advanced in waves
+    of merged launches.  Each mode's lists must equal the plain drop-in's."""
+    import torch
+
+    from prestozl_b200 import jerk
+
+    work = mix_workload(args.mix_spectra)
+    specs = [mix_spectrum(N, z, w, seed, "cuda") for N, z, w, nh, seed in work]
+    torch.cuda.synchronize()
+    geo, banks = [], {}
+    for (N, z, w, nh, seed), sp in zip(work, specs):
+        obs, fftlen, _ = jerk.obs_from_params(N // 2, N, DT, z, w, nh, MIX_SIGMA)
+        subs = jerk.subharm_sizes(obs, fftlen)
+        key = (z, w, nh)
+        if key not in banks:
+            banks[key] = jerk.DeviceBank(subs)
+        geo.append((obs, subs, key))
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1000.0, out
+
+    host = [sp.cpu().numpy() for sp in specs]
+
+    def plain_dropin():
+        res = []
+        for (obs, subs, key), hs in zip(geo, host):
+            p = jerk.JerkPlan(obs, subs, batch=8, device_bank=banks[key].ptr.value)
+            res.append(p.search(hs))
+            p.close()
+        return res
+
+    def sequential():
+        plans, res = {}, []
+        for (obs, subs, key), sp in zip(geo, specs):
+            k = (key, obs.numbins)
+            if k not in plans:
+                plans[k] = jerk.JerkPlan(obs, subs, batch=args.mix_batch,
+                                         device_bank=banks[key].ptr.value)
+            res.append(plans[k].search(sp))
+        for p in plans.values():
+            p.close()
+        return res
+
+    srv = jerk.JerkServer(max_active=args.mix_active, batch=args.mix_batch, device=local)
+    # warm: one request per geometry builds the server's resident banks
+    seen = {}
+    for i, (N, z, w, nh, seed) in enumerate(work):
+        seen.setdefault((z, w, nh), i)
+    for i in seen.values():
+        N, z, w, nh, _ = work[i]
+        srv.submit(specs[i], N, DT, z, w, nh, MIX_SIGMA, tag=10 ** 6 + i)
+    for _ in seen:
+        srv.poll(600000)
+
+    def batched():
+        for i, ((N, z, w, nh, seed), sp) in enumerate(zip(work, specs)):
+            srv.submit(sp, N, DT, z, w, nh, MIX_SIGMA, tag=i)
+        res = [None] * len(work)
+        for _ in work:
+            r = srv.poll(600000)
+            if r is None:
+                raise RuntimeError("batched workload stalled")
+            res[r[0]] = r[1]
+        return res
+
+    t_drop, r_drop = timed(plain_dropin)
+    t_seq, r_seq = timed(sequential)
+    t_bat, r_bat = timed(batched)
+    srv.close()
+    for b in banks.values():
+        b.close()
+
+    def same(a, b):
+        return len(a) == len(b) and all(np.array_equal(a[f], b[f]) for f in a.dtype.names)
+
+    equal = all(same(a, b) and same(a, c) for a, b, c in zip(r_drop, r_seq, r_bat))
+    n = len(work)
+    return {"workload": f"{n} spectra: 16 each of 2^22 / 2^24 / 2^25 samples (dt 54.6 us), "
+                        "(zmax, wmax) in (50, 160), (200, 300), (100, 0), numharm 8 / 16, "
+                        f"sigma {MIX_SIGMA}",
+            "plain_dropin": {"value": n / t_drop * 3600.0, "s": t_drop, "batch_rsteps": 8},
+            "sequential": {"value": n / t_seq * 3600.0, "s": t_seq,
+                           "batch_rsteps": args.mix_batch},
+            "batched": {"value": n / t_bat * 3600.0, "s": t_bat, "batch_rsteps": args.mix_batch,
+                        "in_flight": args.mix_active,
+                        "form": "request loop, all spectra submitted at once, waves of merged "
+                                "launches"},
+            "speedup_vs_plain_dropin": t_drop / t_bat,
+            "speedup_vs_sequential": t_seq / t_bat,
+            "candidates": int(sum(len(r) for r in r_drop)),
+            "equal_results": bool(equal),
+            "timing": "CUDA events around each whole mode"}
+
+
+# --------------------------------------------------------------------------
+# The served stream: dedispersion trials arriving at 40 per second, with a
+# memory-heavy spectrum mixed in.
+
+HEAVY_TAG = 999999
+
+
+def stream_leg(args, local: int):
+    """A bounded sample of the served stream: args.stream_trials consecutive
+    dedispersion trials (2^24 samples each, zmax 200, wmax 300, numharm 16)
+    around the DM index where a pulsar peaks (it is in 6 of them, SNR
+    falling as a Gaussian of sigma 3 trials), arriving as a Poisson process
+    at 40 per second, plus one memory-heavy request (a 2^25-sample red-noise
+    time series with 20 birdies, prepared, zapped and searched at zmax 300,
+    wmax 600, numharm 32, sigma 4) arriving mid-stream, under a 150 GB
+    device budget.  Latencies are from submission to result (queue and
+    service) and from admission to result (service)."""
+    import torch
+
+    from prestozl_b200 import jerk, synth
+
+    Nt, peak, sig_trials = 1 << 24, 288, 3.0
+    first = peak - args.stream_trials // 2
+    trials = list(range(first, first + args.stream_trials))
+    rng = np.random.default_rng(4040)
+    base = synth.random_pulsars(np.random.default_rng(88), 1, zmax=150.0, wmax=250.0,
+                                snr=(20.0, 20.0), maxharm=4)[0]
+    specs = []
+    for t in trials:
+        ps = []
+        if abs(t - peak) <= 2 or t == peak + 3:  # the 6 trials that carry it
+            snr = 20.0 * float(np.exp(-0.5 * ((t - peak) / sig_trials) ** 2))
+            ps = [synth.Pulsar(base.f, base.z, base.w, snr, base.nharm, base.phase)]
+        specs.append(synth.presto_fft_torch(synth.timeseries_torch(Nt, DT, ps, 9000 + t,
+                                                                   device="cuda")))
+    Nh = 1 << 25
+    birds = synth.memory_heavy_birdies()
+    heavy = torch.from_numpy(synth.red_noise_timeseries(Nh, DT, 505, birdies=birds)).cuda()
+    Th = Nh * DT
+    lob = sorted((f - 0.0015) * Th for f in birds)
+    hib = sorted((f + 0.0015) * Th for f in birds)
+    small_heavy = torch.from_numpy(synth.red_noise_timeseries(1 << 20, DT, 506)).cuda()
+    torch.cuda.synchronize()
+
+    srv = jerk.JerkServer(hbm_budget_bytes=150 * 10 ** 9, max_active=args.stream_active,
+                          batch=16, device=local)
+    # warm: the two geometries' banks (a short series of the heavy one)
+    srv.submit(specs[0], Nt, DT, 200, 300, 16, 3.0, tag=10 ** 6)
+    srv.submit(small_heavy, 1 << 20, DT, 300, 600, 32, 4.0, tag=10 ** 6 + 1, timeseries=True)
+    for _ in range(2):
+        srv.poll(600000)
+    s0 = srv.stats()
+
+    arrivals = np.cumsum(rng.exponential(1.0 / 40.0, len(trials) + 1))
+    heavy_at = len(trials) // 2
+    order = list(range(len(trials)))
+    order.insert(heavy_at, -1)
+    t0 = time.perf_counter()
+    submitted, results, best = 0, {}, {}
+    t_sub = {}
+    while len(results) < len(order):
+        now = time.perf_counter() - t0
+        while submitted < len(order) and arrivals[submitted] <= now:
+            k = order[submitted]
+            if k < 0:
+                srv.submit(heavy, Nh, DT, 300, 600, 32, 4.0, tag=HEAVY_TAG, timeseries=True,
+                           birdies=(lob, hib))
+            else:
+                srv.submit(specs[k], Nt, DT, 200, 300, 16, 3.0, tag=k)
+            submitted += 1
+        wait_ms = 1 if submitted < len(order) else 1000
+        r = srv.poll(wait_ms)
+        if r is not None:
+            tag, cands, t = r
+            results[tag] = t
+            if tag < len(trials):
+                best[trials[tag]] = float(cands["sigma"].max()) if len(cands) else 0.0
+    t_end = time.perf_counter() - t0
+    s1 = srv.stats()
+    srv.close()
+    tl = [results[k] for k in range(len(trials))]
+    total = [(t["done"] - t["submit"]) * 1000.0 for t in tl]
+    service = [(t["done"] - t["start"]) * 1000.0 for t in tl]
+    h = results[HEAVY_TAG]
+    n = len(order)
+    return {"workload": f"{len(trials)} dedispersion trials (2^24 samples, zmax 200 wmax 300 "
+                        "numharm 16 sigma 3) around the DM of a pulsar that is in 6 of them, "
+                        "Poisson arrivals at 40/s, plus one memory-heavy time series "
+                        "(2^25 samples, red noise + 20 birdies zapped, zmax 300 wmax 600 "
+                        "numharm 32 sigma 4) arriving mid-stream; 150 GB device budget",
+            "value": n / t_end * 3600.0, "unit": UNIT, "wall_s": t_end,
+            "arrival_span_s": float(arrivals[len(order) - 1]),
+            "latency_ms": {"p50": float(np.percentile(total, 50)),
+                           "p99": float(np.percentile(total, 99)),
+                           "service_p50": float(np.percentile(service, 50)),
+                           "service_p99": float(np.percentile(service, 99)),
+                           "heavy": (h["done"] - h["submit"]) * 1000.0},
+            "peak_device_bytes": s1["peak_bytes"], "budget_bytes": s1["budget"],
+            "in_flight": args.stream_active,
+            "h2d_bytes": s1["h2d_bytes"] - s0["h2d_bytes"],
+            "d2h_bytes": s1["d2h_bytes"] - s0["d2h_bytes"],
+            "best_sigma_by_trial": best,
+            "timing": "host wall clock from the first arrival to the last result; latencies "
+                      "from the server's own submit / start / done times"}
+
+
+# --------------------------------------------------------------------------
 
 def run_served(srv, spectra, dev: bool, device_events: bool = True):
     """Submit every spectrum at once to the server and wait for all results.
@@ -593,6 +833,16 @@ def main():
     ap.add_argument("--extras-reps", type=int, default=5,
                     help="--extras-only: timed input preparations")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-mix", action="store_true",
+                    help="skip the batched workload of uneven spectra")
+    ap.add_argument("--mix-only", action="store_true",
+                    help="only the batched workload and the served stream")
+    ap.add_argument("--mix-spectra", type=int, default=48)
+    ap.add_argument("--mix-batch", type=int, default=32)
+    ap.add_argument("--mix-active", type=int, default=12)
+    ap.add_argument("--no-stream", action="store_true", help="skip the served stream")
+    ap.add_argument("--stream-trials", type=int, default=16)
+    ap.add_argument("--stream-active", type=int, default=12)
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference's own GPU search on this GPU")
     ap.add_argument("--e2e-steps", type=int, default=0)
@@ -616,6 +866,20 @@ def main():
         return
     if args.extras_only:
         run_extras(args)
+        return
+    if args.mix_only:
+        import torch
+
+        from prestozl_b200 import build
+
+        build.build()
+        torch.cuda.set_device(0)
+        out = {"impl": "ours", "mode": "mix-only"}
+        if not args.no_mix:
+            out["batched_mix"] = mix_leg(args, 0)
+        if not args.no_stream:
+            out["served_stream"] = stream_leg(args, 0)
+        print(json.dumps(out))
         return
 
     import torch
@@ -697,7 +961,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         g_ms = []
-        for i in range(args.steps):
+        for i in range(min(args.steps, 4)):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             gplan.search(specs[i % nspec], 0, nsearch)
@@ -706,7 +970,7 @@ def main():
             g_ms.append(e0.elapsed_time(e1))
         gplan.close()
         g_s = replicas.max_over_ranks(sum(g_ms) / 1000.0, dist, "cuda")
-        graph_info = {"value": world * args.steps / g_s * 3600.0,
+        graph_info = {"value": world * len(g_ms) / g_s * 3600.0,
                       "ms_per_spectrum": statistics.mean(g_ms)}
 
     # ---- plain drop-in: what accelsearch_GPU does per spectrum -- allocate a
@@ -755,10 +1019,13 @@ def main():
         srv = jerk.JerkServer(max_active=args.max_active, batch=args.batch, device=local,
                               harm_mode=harm_mode)
         run_served(srv, hnp[:1], False)
+        st0 = srv.stats()
         e2e_s, _, _, _ = run_served(srv, hnp, False)
+        st1 = srv.stats()
         srv.close()
-        h2d = len(hnp) * hnp[0].nbytes
-        d2h = None
+        # the served path's own copies: host spectra in, hit counts and lists out
+        h2d = st1["h2d_bytes"] - st0["h2d_bytes"]
+        d2h = st1["d2h_bytes"] - st0["d2h_bytes"]
     else:
         plan.reset_stats()
         torch.cuda.synchronize()
@@ -780,9 +1047,6 @@ def main():
     torch.cuda.synchronize()
     plan.set_profiling(False)
     kstats = plan.kernel_stats()
-    _, prof_d2h = plan.transfer_stats()
-    if d2h is None:
-        d2h = prof_d2h * e2e_steps
     dom = max(kstats.items(), key=lambda kv: kv[1]["ms"])
     dname, d = dom
     launches = max(d["launches"], 1)
@@ -812,6 +1076,16 @@ def main():
             extras["dedisp"] = {"error": f"{type(e).__name__}: {e}"}
         spec0_np = specs[0].cpu().numpy()
         extras["polish"] = polish_leg(spec0_np, cands0)
+    if not nsearch and world == 1:
+        # the other workloads of the batched and served forms (1 GPU)
+        for name, skip, fn in (("batched_mix", args.no_mix, mix_leg),
+                               ("served_stream", args.no_stream, stream_leg)):
+            if skip:
+                continue
+            try:
+                extras[name] = fn(args, local)
+            except Exception as e:  # a side leg: report it, keep the headline line
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
     timed_spectra = args.steps * (2 if served else 1)
 
     value = served_info["value"] if served else plain_value
