@@ -28,21 +28,39 @@ def _stale(target: str, deps) -> bool:
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile every source to an object in parallel, then link libjerk.so."""
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
     target = os.path.join(LIBDIR, "libjerk.so")
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps.append(os.path.join(ROOT, "include", "jerk.h"))
-    deps.append(os.path.abspath(__file__))
-    if not force and not _stale(target, deps):
-        return target
-    cmd = [NVCC, "-O3", "-std=c++17", "--expt-relaxed-constexpr", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
-           "-I" + os.path.join(ROOT, "include"), "-o", target]
+    common = [os.path.join(CSRC, f) for f in HEADERS]
+    common += [os.path.join(ROOT, "include", "jerk.h"), os.path.abspath(__file__)]
+    flags = ["-O3", "-std=c++17", "--expt-relaxed-constexpr", *ARCH, "-lineinfo",
+             "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
+    srcs = [os.path.join(CSRC, f) for f in SOURCES]
+    if not force and not _stale(target, srcs + common):
+        return target  # objects need not be present (a copy of the tree with the library)
+    jobs = []
+    objs = []
     for f in SOURCES:
-        p = os.path.join(CSRC, f)
-        cmd += (["-x", "cu", p] if f.endswith(".cpp") else [p])
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(objdir, os.path.splitext(f)[0] + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + common):
+            cmd = [NVCC, *flags, "-c"] + (["-x", "cu", src] if f.endswith(".cpp") else [src])
+            jobs.append(cmd + ["-o", obj])
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1) or 1) as ex:
+        for f in [ex.submit(run, c) for c in jobs]:
+            f.result()
+    run([NVCC, *ARCH, "-shared", "-o", target, *objs])
     return target
 
 

@@ -181,6 +181,8 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
     // power-of-two fftlen the chunk is scaled by 1/fftlen here, exactly (a
     // power of two), so the correlation's |y|^2 already carries the
     // reference's 1/fftlen^2 and needs no multiply; other lengths keep it.
+    // The transform of the spread chunk repeats with period N/2; only the
+    // first half is stored (the correlation reads it twice).
     float2 *outp = P.prepped + sd.data_off + (long long)b * N;
     auto in = [&](int r) -> float2 {
         const int m = tid + r * (N / R0);
@@ -192,7 +194,8 @@ __device__ void prep_impl(const SearchDev &P, int b, int s, float *smem)
             y.x = __fmul_rn(y.x, inv);
             y.y = __fmul_rn(y.y, inv);
         }
-        outp[m] = y;
+        if (m < N / 2)
+            outp[m] = y;
     };
     fft_block<N, -1>(buf, tw, tid, in, out);
 
@@ -286,8 +289,9 @@ template <int N>
 struct CorrSmem {
     static constexpr int kBase =
         (fft_buf_len<N>() + (CorrBig<N>::value ? 0 : FftPlan<N>::twsize()) + 1) & ~1;
-    static constexpr bool kStage = (size_t)(kBase + N) * 8 * CorrOcc<N>::value <= 220 * 1024;
-    static constexpr int value = kBase + (kStage ? N : 0);
+    // the staged row is the prepared chunk's first half (see corr_body)
+    static constexpr bool kStage = (size_t)(kBase + N / 2) * 8 * CorrOcc<N>::value <= 220 * 1024;
+    static constexpr int value = kBase + (kStage ? N / 2 : 0);
 };
 
 // Bulk (TMA engine) copy of one data row into shared memory, completed on an
@@ -327,6 +331,17 @@ __device__ __forceinline__ bool bar_wait(uint64_t *bar, unsigned parity)
 constexpr unsigned kStatusRind = 1u;     // harmsum: a subharmonic r index left its row
 constexpr unsigned kStatusCopy = 2u;     // corr: a data-row copy did not complete
 
+// A wait that must run out: phase 0 of s_probe never completes (no copy is
+// involved).  Out of line, so the correlation's registers do not pay for it.
+__device__ __noinline__ void run_wait_probe(unsigned int *status)
+{
+    __shared__ uint64_t s_probe;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_probe)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (!bar_wait(&s_probe, 0) && status)
+        atomicOr(status, kStatusCopy);
+}
+
 // One CTA: kernel row `row` of the fftlen-N group G, rsteps [b0, b1) of the
 // batch.  probe: this is the plan's first CTA (the wait probe runs there).
 template <int N>
@@ -352,6 +367,13 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
     const SubDev sd = P.subs[s];
     const float2 *D0 = P.prepped + sd.data_off;
 
+    // The prepared chunk is the FFT of data spread to even interbins, which
+    // repeats with period N/2 (X[k + N/2] = X[k]); prep_kernel stores its
+    // first half only, and element m of the product reads X[m mod N/2].  In
+    // the first-stage butterfly of thread tid, input r is element
+    // tid + r N/R0, so inputs r and r + R0/2 read the same value.
+    static_assert(R0 % 2 == 0 && (N / R0) * (R0 / 2) == N / 2, "half-row reads");
+    constexpr unsigned kRowBytes = N / 2 * sizeof(float2);
     if constexpr (kStage) {
         if (tid == 0) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
@@ -359,7 +381,7 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
         }
         __syncthreads();
         if (tid == 0 && b0 < b1)
-            bulk_row_load(dsm, D0 + (long long)b0 * N, N * sizeof(float2), &s_bar);
+            bulk_row_load(dsm, D0 + (long long)b0 * N, kRowBytes, &s_bar);
     }
 
     const float2 *tw = kBig ? P.twiddles + sd.twoff : tws;
@@ -368,14 +390,8 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
             tws[i] = P.twiddles[sd.twoff + i];
     }
 
-    if (P.wait_probe && probe && tid == 0) {
-        // a wait that must run out: phase 0 of s_probe never completes
-        __shared__ uint64_t s_probe;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_probe)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        if (!bar_wait(&s_probe, 0) && P.status)
-            atomicOr(P.status, kStatusCopy);
-    }
+    if (P.wait_probe && probe && tid == 0)
+        run_wait_probe(P.status);
 
     // the kernel row, in the order this thread's first-stage butterfly reads it
     // (kBig: read from global memory at every rstep instead)
@@ -400,8 +416,8 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
         // the chunk.
         auto out = [&](int m, float2 y) {
             const int kk = m - offset;
-            const float pw = __fadd_rn(__fmul_rn(y.x, y.x), __fmul_rn(y.y, y.y));
-            const float o = IsPow2<N>::value ? pw : __fmul_rn(pw, norm);
+            const float pw = fmaf(y.x, y.x, y.y * y.y);
+            const float o = IsPow2<N>::value ? pw : pw * norm;
             if ((unsigned)kk < (unsigned)numrs)
                 outp[kk] = o;
         };
@@ -410,11 +426,13 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
             // has read it, thread 0 starts the copy of rstep b + 1's row
             if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
                 atomicOr(P.status, kStatusCopy);
-            auto in = [&](int r) -> float2 { return cmulconj(dsm[tid + r * (N / R0)], kreg[r]); };
+            auto in = [&](int r) -> float2 {
+                return cmulconj(dsm[tid + (r % (R0 / 2)) * (N / R0)], kreg[r]);
+            };
             auto mid = [&] {
                 if (tid == 0 && b + 1 < b1) {
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    bulk_row_load(dsm, D0 + (long long)(b + 1) * N, N * sizeof(float2), &s_bar);
+                    bulk_row_load(dsm, D0 + (long long)(b + 1) * N, kRowBytes, &s_bar);
                 }
             };
             fft_block<N, +1>(buf, tw, tid, in, out, mid);
@@ -422,7 +440,7 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
             const float2 *D = D0 + (long long)b * N;
             auto in = [&](int r) -> float2 {
                 const int m = tid + r * (N / R0);
-                return cmulconj(D[m], kBig ? K[m] : kreg[r]);
+                return cmulconj(D[tid + (r % (R0 / 2)) * (N / R0)], kBig ? K[m] : kreg[r]);
             };
             fft_block<N, +1>(buf, tw, tid, in, out);
         }

@@ -1357,7 +1357,7 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
         double bytes = 0, flops = 0;
         for (int s = 0; s < p->nsubs; s++) {
             const int N = p->subs[s].fftlen;
-            bytes += (double)a.nb * (N / 2 * 8.0 + N * 8.0);
+            bytes += (double)a.nb * (N / 2 * 8.0 + N / 2 * 8.0);
             flops += (double)a.nb * fft_flops(N);
         }
         const int tok = launch_begin(p, kclass(p, "prep"), bytes, flops);
@@ -1380,7 +1380,7 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
             double numrs = 0;
             for (int b = 0; b < a.nb; b++)
                 numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
-            bytes += nrow * N * 8.0 + a.nb * N * 8.0 + nrow * numrs * 4.0;
+            bytes += nrow * N * 8.0 + a.nb * N / 2 * 8.0 + nrow * numrs * 4.0;
             flops += nrow * a.nb * (fft_flops(N) + 6.0 * N) + nrow * numrs * 3.0;
         }
         const int tok = launch_begin(p, kclass(p, "corr_" + std::to_string(N)), bytes, flops);
@@ -1712,7 +1712,7 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
         maxfft = std::max(maxfft, p->maxfft);
         for (int s = 0; s < p->nsubs; s++) {
             const int N = p->subs[s].fftlen;
-            pbytes += (double)a.nb * (N / 2 * 8.0 + N * 8.0);
+            pbytes += (double)a.nb * (N / 2 * 8.0 + N / 2 * 8.0);
             pflops += (double)a.nb * fft_flops(N);
         }
     }
@@ -1753,7 +1753,7 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
                 double numrs = 0;
                 for (int b = 0; b < a.nb; b++)
                     numrs += p->hsteps[(size_t)(a.first_rstep + b) * p->nsubs + s].numrs;
-                bytes += nrow * N * 8.0 + a.nb * N * 8.0 + nrow * numrs * 4.0;
+                bytes += nrow * N * 8.0 + a.nb * N / 2 * 8.0 + nrow * numrs * 4.0;
                 flops += nrow * a.nb * (fft_flops(N) + 6.0 * N) + nrow * numrs * 3.0;
             }
         }
