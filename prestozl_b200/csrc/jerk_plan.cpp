@@ -153,29 +153,35 @@ static int fftlen_from_kernwidth(int kw)
 }
 
 // ---------------------------------------------------------------------------
-// Statistics: restatement of src/characteristics.c:400-705 for the integer
-// numsum the search uses.
+// Statistics: candidate_sigma / power_for_sigma (src/characteristics.c:400-705)
+// for the integer numsum the search uses, written from the published
+// formulas the reference's code evaluates.
 
-static double log_asymtotic_incomplete_gamma(double a, double z)
+// ln Gamma(a, z), the upper incomplete gamma function, for large z by its
+// asymptotic series (Abramowitz & Stegun 6.5.32):
+//   Gamma(a, z) ~ z^(a-1) e^(-z) sum_k (a-1)(a-2)...(a-k) / z^k,
+// summed until a term drops below 1e-15.
+static double log_upper_gamma_large_z(double a, double z)
 {
-    double x = 1.0, newxpart = 1.0, term = 1.0;
-    int ii = 1;
-    while (fabs(newxpart) > 1e-15) {
-        term *= (a - ii);
-        newxpart = term / pow(z, ii);
-        x += newxpart;
-        ii += 1;
+    double sum = 1.0, coef = 1.0, term = 1.0;
+    for (int k = 1; fabs(term) > 1e-15; k++) {
+        coef *= (a - k);
+        term = coef / pow(z, k);
+        sum += term;
     }
-    return (a - 1.0) * log(z) - z + log(x);
+    return (a - 1.0) * log(z) - z + log(sum);
 }
 
-static double log_asymtotic_gamma(double z)
+// ln Gamma(z) by Stirling's series (Abramowitz & Stegun 6.1.41), to the
+// z^-7 term: (z - 1/2) ln z - z + ln(2 pi)/2 + 1/(12 z) - 1/(360 z^3)
+// + 1/(1260 z^5) - 1/(1680 z^7).
+static double log_gamma_stirling(double z)
 {
-    double x = (z - 0.5) * log(z) - z + 0.91893853320467267;
-    const double y = 1.0 / (z * z);
-    x += (((-5.9523809523809529e-4 * y + 7.9365079365079365079365e-4) * y -
-           2.7777777777777777777778e-3) * y + 8.3333333333333333333333e-2) / z;
-    return x;
+    const double half_log_2pi = 0.91893853320467274178;
+    const double u = 1.0 / (z * z);
+    const double series =
+        (((-1.0 / 1680.0) * u + 1.0 / 1260.0) * u - 1.0 / 360.0) * u + 1.0 / 12.0;
+    return (z - 0.5) * log(z) - z + half_log_2pi + series / z;
 }
 
 // Q(a, x) for integer a: exp(-x) sum_{n<a} x^n / n!
@@ -196,8 +202,8 @@ static double chi2_logp(double chi2, double dof)
     if (chi2 <= 0.0)
         return -INFINITY;
     if (chi2 / dof > 15.0 || (dof > 150 && chi2 / dof > 6.0))
-        return log_asymtotic_incomplete_gamma(0.5 * dof, 0.5 * chi2) -
-               log_asymtotic_gamma(0.5 * dof);
+        return log_upper_gamma_large_z(0.5 * dof, 0.5 * chi2) -
+               log_gamma_stirling(0.5 * dof);
     return log(q_gamma_int((int)(0.5 * dof + 0.5), 0.5 * chi2));
 }
 
@@ -227,7 +233,8 @@ static double equivalent_gaussian_sigma(double logp)
 {
     double x;
     if (logp < -600.0) {
-        // A&S 26.2.23 on log p
+        // the rational approximation of the normal quantile, Abramowitz &
+        // Stegun 26.2.23, on log p (|error| < 4.5e-4)
         const double t = sqrt(-2.0 * logp);
         const double num = 2.515517 + t * (0.802853 + t * 0.010328);
         const double den = 1.0 + t * (1.432788 + t * (0.189269 + t * 0.001308));
