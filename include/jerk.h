@@ -206,10 +206,10 @@ int jerk_debug_volume(jerk_plan *plan, const void *spectrum, int spectrum_on_dev
                       long long rstep, int sub, float *out, int *numrs, long long *rlo);
 
 /* Debug/test: with on != 0, every later pass of the plan also runs one
- * bounded wait that must give up (thread 0 of the first correlation CTA waits
- * on an mbarrier that nothing completes; no copy is involved).  The pass then
- * fails with JERK_ECUDA, as a data-row copy that never completes would, and
- * the plan stays usable.  The reference has no bounded waits: its CUDA errors
+ * bounded wait that must give up (the correlation's bounded mbarrier wait, in
+ * a one-thread kernel on the plan's stream, on an mbarrier that nothing
+ * completes; no copy is involved).  The pass then fails with JERK_ECUDA, as a
+ * data-row copy that never completes would, and the plan stays usable.  The reference has no bounded waits: its CUDA errors
  * exit the process (include/cuda_helper.h:2-16). */
 int jerk_debug_wait_probe(jerk_plan *plan, int on);
 

@@ -331,9 +331,12 @@ __device__ __forceinline__ bool bar_wait(uint64_t *bar, unsigned parity)
 constexpr unsigned kStatusRind = 1u;     // harmsum: a subharmonic r index left its row
 constexpr unsigned kStatusCopy = 2u;     // corr: a data-row copy did not complete
 
-// A wait that must run out: phase 0 of s_probe never completes (no copy is
-// involved).  Out of line, so the correlation's registers do not pay for it.
-__device__ __noinline__ void run_wait_probe(unsigned int *status)
+// A wait that must run out: the correlation's bounded wait (bar_wait) on an
+// mbarrier whose phase 0 nothing completes (no copy is involved, so nothing
+// is left in flight).  It gives up after its poll limit and reports as a
+// data-row copy that never completed would.  Launched by plans whose wait
+// probe is on (jerk_debug_wait_probe), one thread.
+__global__ void wait_probe_kernel(unsigned int *status)
 {
     __shared__ uint64_t s_probe;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_probe)) : "memory");
@@ -342,11 +345,20 @@ __device__ __noinline__ void run_wait_probe(unsigned int *status)
         atomicOr(status, kStatusCopy);
 }
 
-// One CTA: kernel row `row` of the fftlen-N group G, rsteps [b0, b1) of the
-// batch.  probe: this is the plan's first CTA (the wait probe runs there).
+cudaError_t launch_wait_probe(unsigned int *status, cudaStream_t st)
+{
+    wait_probe_kernel<<<1, 1, 0, st>>>(status);
+    return cudaGetLastError();
+}
+
+// One CTA of a wave: kernel row `row` of the fftlen-N group G, rsteps
+// [b0, b1) of the batch.  (A plan's own launch, corr_kernel below, is the
+// same code reading its arguments straight from the kernel parameters: the
+// body, which reaches them through references, measured 6 % slower at
+// fftlen 2048 and spills at 1280, where CTAs of 80 threads run 8 per SM.)
 template <int N>
 __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G, const int row,
-                                          const int b0, const int b1, const bool probe)
+                                          const int b0, const int b1)
 {
     constexpr int R0 = FftPlan<N>::R0;
     constexpr int T = FftPlan<N>::T;
@@ -390,8 +402,6 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
             tws[i] = P.twiddles[sd.twoff + i];
     }
 
-    if (P.wait_probe && probe && tid == 0)
-        run_wait_probe(P.status);
 
     // the kernel row, in the order this thread's first-stage butterfly reads it
     // (kBig: read from global memory at every rstep instead)
@@ -457,17 +467,125 @@ __device__ __forceinline__ void rstep_chunk(int nb, int ny, int y, int *b0, int 
     *b1 = min(nb, *b0 + bchunk);
 }
 
+// A plan's own launch: one CTA per kernel row (blockIdx.x) of the group,
+// rsteps of chunk blockIdx.y of gridDim.y.
 template <int N>
 __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     corr_kernel(const __grid_constant__ SearchDev P, const __grid_constant__ RowGroup G)
 {
-    int b0, b1;
-    rstep_chunk(P.nb, (int)gridDim.y, (int)blockIdx.y, &b0, &b1);
-    corr_body<N>(P, G, blockIdx.x, b0, b1, blockIdx.x == 0 && blockIdx.y == 0);
+    constexpr int R0 = FftPlan<N>::R0;
+    constexpr int T = FftPlan<N>::T;
+    constexpr int TWN = FftPlan<N>::twsize();
+    constexpr bool kStage = CorrSmem<N>::kStage;
+    constexpr bool kBig = CorrBig<N>::value;
+    extern __shared__ __align__(16) float2 sm2[];
+    __shared__ uint64_t s_bar;
+    float2 *buf = sm2;
+    float2 *tws = sm2 + fft_buf_len<N>();
+    float2 *dsm = sm2 + CorrSmem<N>::kBase;  // staged data row (kStage)
+    const int tid = threadIdx.x;
+    const int row = blockIdx.x;
+    int gi = 0;
+    while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
+        gi++;
+    const int s = G.sub[gi];
+    const int lrow = row - G.rowstart[gi];
+    const SubDev sd = P.subs[s];
+    const float2 *D0 = P.prepped + sd.data_off;
+    // this CTA's rsteps: all of the batch, or a share of them when a small
+    // group's rows alone would leave SMs idle (gridDim.y > 1)
+    const int bchunk = (P.nb + (int)gridDim.y - 1) / (int)gridDim.y;
+    const int b0 = min(P.nb, (int)blockIdx.y * bchunk), b1 = min(P.nb, b0 + bchunk);
+
+    // The prepared chunk is the FFT of data spread to even interbins, which
+    // repeats with period N/2 (X[k + N/2] = X[k]); prep_kernel stores its
+    // first half only, and element m of the product reads X[m mod N/2].  In
+    // the first-stage butterfly of thread tid, input r is element
+    // tid + r N/R0, so inputs r and r + R0/2 read the same value.
+    static_assert(R0 % 2 == 0 && (N / R0) * (R0 / 2) == N / 2, "half-row reads");
+    constexpr unsigned kRowBytes = N / 2 * sizeof(float2);
+    if constexpr (kStage) {
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (tid == 0 && b0 < b1)
+            bulk_row_load(dsm, D0 + (long long)b0 * N, kRowBytes, &s_bar);
+    }
+
+    const float2 *tw = kBig ? P.twiddles + sd.twoff : tws;
+    if constexpr (!kBig) {
+        for (int i = tid; i < TWN; i += T)
+            tws[i] = P.twiddles[sd.twoff + i];
+    }
+
+
+    // the kernel row, in the order this thread's first-stage butterfly reads it
+    // (kBig: read from global memory at every rstep instead)
+    float2 kreg[R0];
+    const float2 *K = P.bank + sd.kern_off + (long long)lrow * N;
+    if constexpr (!kBig) {
+#pragma unroll
+        for (int r = 0; r < R0; r++)
+            kreg[r] = K[tid + r * (N / R0)];
+    }
+    __syncthreads();
+
+    const int offset = sd.halfwidth * 2;  // binoffset * ACCEL_NUMBETWEEN
+    const float norm = sd.pownorm;
+    for (int b = b0; b < b1; b++) {
+        const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
+        float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
+                      (long long)lrow * sd.stride;
+        // the power is formed for every output and the store predicated on
+        // the good-bin range (one unsigned compare): measured faster than a
+        // branch around both.  Power-of-two fftlen: 1/fftlen^2 is already in
+        // the chunk.
+        auto out = [&](int m, float2 y) {
+            const int kk = m - offset;
+            const float pw = fmaf(y.x, y.x, y.y * y.y);
+            const float o = IsPow2<N>::value ? pw : pw * norm;
+            if ((unsigned)kk < (unsigned)numrs)
+                outp[kk] = o;
+        };
+        if constexpr (kStage) {
+            // rstep b's row is (or will shortly be) in dsm; once every thread
+            // has read it, thread 0 starts the copy of rstep b + 1's row
+            if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
+                atomicOr(P.status, kStatusCopy);
+            auto in = [&](int r) -> float2 {
+                return cmulconj(dsm[tid + (r % (R0 / 2)) * (N / R0)], kreg[r]);
+            };
+            auto mid = [&] {
+                if (tid == 0 && b + 1 < b1) {
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    bulk_row_load(dsm, D0 + (long long)(b + 1) * N, kRowBytes, &s_bar);
+                }
+            };
+            fft_block<N, +1>(buf, tw, tid, in, out, mid);
+        } else {
+            const float2 *D = D0 + (long long)b * N;
+            auto in = [&](int r) -> float2 {
+                const int m = tid + r * (N / R0);
+                return cmulconj(D[tid + (r % (R0 / 2)) * (N / R0)], kBig ? K[m] : kreg[r]);
+            };
+            fft_block<N, +1>(buf, tw, tid, in, out);
+        }
+        __syncthreads();
+    }
 }
 
+// A wave's CTAs reach their plan's arguments by index, which costs registers:
+// at fftlen 1280 (80-thread CTAs, 8 per SM, 80 registers) the body spills,
+// so those run 5 per SM.
 template <int N>
-__global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
+struct CorrGroupOcc {
+    static constexpr int value = N == 1280 ? 5 : CorrOcc<N>::value;
+};
+
+template <int N>
+__global__ void __launch_bounds__(FftPlan<N>::T, CorrGroupOcc<N>::value)
     corr_group_kernel(const __grid_constant__ GroupLaunch M)
 {
     const int i = group_plan(M, blockIdx.x);
@@ -475,7 +593,7 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
     const int ny = M.ny[i];
     int b0, b1;
     rstep_chunk(M.P[i].nb, ny, local % ny, &b0, &b1);
-    corr_body<N>(M.P[i], M.G[i], local / ny, b0, b1, local == 0);
+    corr_body<N>(M.P[i], M.G[i], local / ny, b0, b1);
 }
 
 // ---------------------------------------------------------------------------
@@ -1165,7 +1283,7 @@ static cudaError_t launch_corr_group_n(GroupLaunch &M, cudaStream_t st)
         return e;
     // the single-plan rule, applied to the wave's rows together: fewer rows
     // than two waves of CTAs also split their rsteps
-    const int wave = sm_count() * CorrOcc<N>::value;
+    const int wave = sm_count() * CorrGroupOcc<N>::value;
     long long total = 0;
     for (int i = 0; i < M.n; i++)
         total += M.G[i].rowstart[M.G[i].n];

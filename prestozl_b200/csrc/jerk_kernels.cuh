@@ -72,10 +72,6 @@ struct SearchDev {
     unsigned int *status;     // bit 0: a subharmonic r index fell outside its row
                               // (or its TMA box); bit 1: a bounded wait on a bulk
                               // or tensor copy gave up
-    int wait_probe;           // nonzero: thread 0 of the first correlation CTA
-                              // also waits, bounded, on an mbarrier that nothing
-                              // completes (tests the give-up path; no copy is
-                              // involved, so nothing is left in flight)
 };
 
 // Tensor maps of the harmonic sum's TMA path: subharmonic s's batch volumes

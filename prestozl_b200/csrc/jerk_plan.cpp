@@ -38,6 +38,7 @@ bool fftlen_supported(int n);
 cudaError_t launch_prep_group(GroupLaunch M, int maxfft, cudaStream_t st);
 cudaError_t launch_corr_group(GroupLaunch M, int fftlen, cudaStream_t st);
 cudaError_t launch_harmsum_group(GroupLaunch M, int nstages, cudaStream_t st);
+cudaError_t launch_wait_probe(unsigned int *status, cudaStream_t st);
 int fft_twiddle_size(int N);
 void fft_twiddle_table(int N, float2 *out);
 cudaError_t launch_bank_response(const BankRow *rows, int nrows, int max_pts, float2 *bank,
@@ -1332,7 +1333,6 @@ static SearchDev make_args(const jerk_plan *p, const float2 *spec)
     a.hit_count = p->d_hit_count;
     a.max_hits = p->max_hits;
     a.status = p->d_status;
-    a.wait_probe = p->wait_probe;
     return a;
 }
 
@@ -1414,6 +1414,8 @@ static int pass_begin(jerk_plan *p, const float2 *spec, long long first, long lo
     JERK_CUDA(cudaMemsetAsync(p->d_hit_count, 0, sizeof(unsigned int), p->stream));
     // a pass that reported a failed wait or index leaves no trace in the next
     JERK_CUDA(cudaMemsetAsync(p->d_status, 0, sizeof(unsigned int), p->stream));
+    if (p->wait_probe)
+        JERK_CUDA(launch_wait_probe(p->d_status, p->stream));
     return JERK_OK;
 }
 

@@ -329,9 +329,10 @@ def test_frequency_band_matches_reference(tmp_path):
 
 
 def test_bounded_wait_gives_up_without_fault(small, plan):
-    """Every device wait here is bounded.  A pass whose correlation kernel runs
-    one wait that must give up (an mbarrier nothing completes, with no copy in
-    flight) fails with JERK_ECUDA and the wait's message instead of hanging;
+    """Every device wait here is bounded.  A pass that runs the correlation's
+    bounded wait on an mbarrier nothing completes (a one-thread probe kernel on
+    the plan's stream, with no copy in flight) fails with JERK_ECUDA and the
+    wait's message instead of hanging;
     the context and the same plan stay usable, and the next pass gives the
     results of a pass that never failed."""
     want = plan.search(small.spec, 100, 8, want_hits=True)
