@@ -1303,6 +1303,24 @@ static cudaError_t launch_corr_group_n(GroupLaunch &M, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// CTAs of one full wave of the single-plan correlation / harmonic sum
+int corr_wave_ctas(int fftlen)
+{
+    switch (fftlen) {
+#define JERK_CW(NN) case NN: return sm_count() * CorrOcc<NN>::value;
+    JERK_CW(128) JERK_CW(192) JERK_CW(256) JERK_CW(384) JERK_CW(512) JERK_CW(768)
+    JERK_CW(1024) JERK_CW(1280) JERK_CW(2048) JERK_CW(4096) JERK_CW(5120) JERK_CW(7680)
+    JERK_CW(10240) JERK_CW(15360)
+#undef JERK_CW
+    default: return sm_count();
+    }
+}
+
+int harmsum_wave_ctas(int nstages)
+{
+    return sm_count() * (nstages <= 5 ? HarmOcc<5, 4>::value : HarmOcc<6, 4>::value);
+}
+
 cudaError_t launch_corr_group(GroupLaunch M, int fftlen, cudaStream_t st)
 {
     if (M.n < 1 || M.n > kMaxGroupPlans)

@@ -39,6 +39,8 @@ cudaError_t launch_prep_group(GroupLaunch M, int maxfft, cudaStream_t st);
 cudaError_t launch_corr_group(GroupLaunch M, int fftlen, cudaStream_t st);
 cudaError_t launch_harmsum_group(GroupLaunch M, int nstages, cudaStream_t st);
 cudaError_t launch_wait_probe(unsigned int *status, cudaStream_t st);
+int corr_wave_ctas(int fftlen);
+int harmsum_wave_ctas(int nstages);
 int fft_twiddle_size(int N);
 void fft_twiddle_table(int N, float2 *out);
 cudaError_t launch_bank_response(const BankRow *rows, int nrows, int max_pts, float2 *bank,
@@ -1741,11 +1743,25 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
     if (e != cudaSuccess)
         return fail_all(e, "prep_group_kernel");
 
-    // correlation: one launch per FFT length over every plan that has it
+    // correlation: one launch per FFT length over every plan that has it; a
+    // plan whose rows of that length fill the GPU twice over by themselves
+    // gains nothing from merging and takes its own (faster) launch
     std::map<int, std::vector<int>> byN;
-    for (int i = 0; i < n; i++)
-        for (auto &kv : W[i]->groups)
-            byN[kv.first].push_back(i);
+    for (int i = 0; i < n; i++) {
+        jerk_plan *p = W[i];
+        for (auto &kv : p->groups) {
+            const RowGroup G = row_group(p, kv.second);
+            if (G.rowstart[G.n] < 2 * corr_wave_ctas(kv.first)) {
+                byN[kv.first].push_back(i);
+                continue;
+            }
+            tok = launch_begin(p0, kclass(p0, "wave_corr_" + std::to_string(kv.first)), 0.0, 0.0);
+            e = launch_corr(p->pass.a, kv.first, G, G.rowstart[G.n], st);
+            launch_end(p0, tok);
+            if (e != cudaSuccess)
+                return fail_all(e, "corr_kernel");
+        }
+    }
     for (auto &kv : byN) {
         const int N = kv.first;
         GroupLaunch C{};
@@ -1778,7 +1794,9 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
     std::map<int, std::vector<int>> byS;
     for (int i = 0; i < n; i++) {
         jerk_plan *p = W[i];
-        if (p->harm_mode <= 1) {
+        const SearchDev &a = p->pass.a;
+        const long long ctas = (long long)((a.corr_uselen + 127) / 128) * a.numw0 * a.nb;
+        if (p->harm_mode <= 1 && ctas < 2 * harmsum_wave_ctas(a.nstages)) {
             byS[p->obs.numharmstages].push_back(i);
             continue;
         }
