@@ -718,7 +718,7 @@ def stream_leg(args, local: int):
     torch.cuda.synchronize()
 
     srv = jerk.JerkServer(hbm_budget_bytes=150 * 10 ** 9, max_active=args.stream_active,
-                          batch=16, device=local)
+                          batch=args.stream_batch, device=local)
     # warm: the two geometries' banks (a short series of the heavy one)
     srv.submit(specs[0], Nt, DT, 200, 300, 16, 3.0, tag=10 ** 6)
     srv.submit(small_heavy, 1 << 20, DT, 300, 600, 32, 4.0, tag=10 ** 6 + 1, timeseries=True)
@@ -771,7 +771,7 @@ def stream_leg(args, local: int):
                            "service_p99": float(np.percentile(service, 99)),
                            "heavy": (h["done"] - h["submit"]) * 1000.0},
             "peak_device_bytes": s1["peak_bytes"], "budget_bytes": s1["budget"],
-            "in_flight": args.stream_active,
+            "max_in_flight": args.stream_active, "batch_rsteps": args.stream_batch,
             "h2d_bytes": s1["h2d_bytes"] - s0["h2d_bytes"],
             "d2h_bytes": s1["d2h_bytes"] - s0["d2h_bytes"],
             "best_sigma_by_trial": best,
@@ -842,7 +842,10 @@ def main():
     ap.add_argument("--mix-active", type=int, default=12)
     ap.add_argument("--no-stream", action="store_true", help="skip the served stream")
     ap.add_argument("--stream-trials", type=int, default=16)
-    ap.add_argument("--stream-active", type=int, default=12)
+    ap.add_argument("--stream-active", type=int, default=16,
+                    help="served stream: searches in flight at most (the 150 GB budget "
+                         "binds first at the default batch)")
+    ap.add_argument("--stream-batch", type=int, default=64)
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip timing the reference's own GPU search on this GPU")
     ap.add_argument("--e2e-steps", type=int, default=0)
