@@ -437,7 +437,9 @@ __device__ __forceinline__ void corr_body(const SearchDev &P, const RowGroup &G,
             if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
                 atomicOr(P.status, kStatusCopy);
             auto in = [&](int r) -> float2 {
-                return cmulconj(dsm[tid + (r % (R0 / 2)) * (N / R0)], kreg[r]);
+                // kBig: the kernel row is read from global memory here too
+                return cmulconj(dsm[tid + (r % (R0 / 2)) * (N / R0)],
+                                kBig ? K[tid + r * (N / R0)] : kreg[r]);
             };
             auto mid = [&] {
                 if (tid == 0 && b + 1 < b1) {
@@ -555,7 +557,9 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrOcc<N>::value)
             if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
                 atomicOr(P.status, kStatusCopy);
             auto in = [&](int r) -> float2 {
-                return cmulconj(dsm[tid + (r % (R0 / 2)) * (N / R0)], kreg[r]);
+                // kBig: the kernel row is read from global memory here too
+                return cmulconj(dsm[tid + (r % (R0 / 2)) * (N / R0)],
+                                kBig ? K[tid + r * (N / R0)] : kreg[r]);
             };
             auto mid = [&] {
                 if (tid == 0 && b + 1 < b1) {
