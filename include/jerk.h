@@ -110,7 +110,9 @@ typedef struct jerk_config {
                                  capped to what 32-bit volume offsets allow */
     long long max_hits;       /* initial hit-buffer capacity; 0 = auto */
     void *stream;             /* cudaStream_t to run on; NULL = a private stream */
-    const void *device_bank;  /* optional resident bank (jerk_bank_generate) */
+    const void *device_bank;  /* optional resident bank (jerk_bank_generate); it
+                                 must be complete when the plan is created (the
+                                 plan folds its fftlen-2048 rows from it then) */
     int harm_mode;            /* harmonic-sum kernel (a tuning knob; results do
                                  not depend on it): 1 = gather (global loads),
                                  2 = gather + TMA prefetch of the next tile into

@@ -601,6 +601,371 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrGroupOcc<N>::value)
 }
 
 // ---------------------------------------------------------------------------
+// 2b. Correlation at fftlen 2048 on folded kernel rows.
+//
+// The prepared chunk D repeats with period N/2 (it is the transform of data
+// spread to even interbins), so the inverse transform of D conj(K) splits
+// into two half-length transforms, one per output parity:
+//   y[2m]     = IFFT_{N/2}(D A)[m],  A[k] = conj K[k] + conj K[k + N/2]
+//   y[2m + 1] = IFFT_{N/2}(D B)[m],  B[k] = (conj K[k] - conj K[k + N/2]) e^{+2 pi i k/N}
+// for k < N/2.  A and B depend only on the kernel row, so a plan folds its
+// rows of length 2048 once (fold_rows_kernel, in double, each value rounded
+// once) and the correlation runs two 1024-point transforms that read each
+// data value once for both: the first radix-2 layer of the 2048-point
+// transform (its butterflies and twiddles) is gone, the last stage shares
+// its twiddles between the two transforms, and each thread stores the two
+// powers of an output pair with one 8-byte store.
+//
+// The 1024-point plan is [8, 16, 8] for 128 threads: stage 0 (radix 8, 128
+// butterflies) -- thread j does butterfly j of both transforms from the same
+// 8 data values; stage 1 (radix 16, 64 butterflies each) -- threads 0-63 the
+// even transform, 64-127 the odd one; stage 2 (radix 8, 128 butterflies) --
+// thread j butterfly j of both, with shared twiddles.
+
+static int sm_count();
+
+constexpr int kFoldN = 2048;
+constexpr int kFoldH = kFoldN / 2;
+constexpr int kFoldTw1 = 8 * 16;     // stage 1: W_128^(r k) at [r 8 + k]
+constexpr int kFoldTw2 = 128 * 8;    // stage 2: W_1024^(r k) at [r 128 + k]
+
+int fold_twiddle_size() { return kFoldTw1 + kFoldTw2; }
+
+// Host: the two tables, forward sign, in double rounded to float.
+void fold_twiddle_table(float2 *out)
+{
+    const double tau = 2.0 * 3.14159265358979323846264338327950288;
+    for (int r = 0; r < 16; r++)
+        for (int k = 0; k < 8; k++) {
+            const double a = -tau * (double)(r * k) / 128.0;
+            out[r * 8 + k] = make_float2((float)cos(a), (float)sin(a));
+        }
+    for (int r = 0; r < 8; r++)
+        for (int k = 0; k < 128; k++) {
+            const double a = -tau * (double)(r * k) / 1024.0;
+            out[kFoldTw1 + r * 128 + k] = make_float2((float)cos(a), (float)sin(a));
+        }
+}
+
+// Folded rows: row i of the launch's groups (consecutive over its
+// subharmonics) from bank row src[i]; out[i] = A (first half), B (second).
+__global__ void fold_rows_kernel(const float2 *__restrict__ bank, const long long *src,
+                                 float2 *__restrict__ out, int nrows)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long row = t / kFoldH;
+    const int k = (int)(t % kFoldH);
+    if (row >= nrows)
+        return;
+    const float2 *K = bank + src[row];
+    const float2 k0 = K[k], k1 = K[k + kFoldH];
+    // conj K[k] +/- conj K[k + N/2], in double
+    const double ar = (double)k0.x + (double)k1.x, ai = -(double)k0.y - (double)k1.y;
+    const double dr = (double)k0.x - (double)k1.x, di = -(double)k0.y + (double)k1.y;
+    double sn, cs;
+    sincospi((double)k / (double)kFoldH, &sn, &cs);  // e^{+2 pi i k / N}
+    float2 *o = out + row * kFoldN;
+    o[k] = make_float2((float)ar, (float)ai);
+    o[k + kFoldH] = make_float2((float)(dr * cs - di * sn), (float)(dr * sn + di * cs));
+}
+
+cudaError_t launch_fold_rows(const float2 *bank, const long long *src, float2 *out, int nrows,
+                             cudaStream_t st)
+{
+    const long long n = (long long)nrows * kFoldH;
+    fold_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(bank, src, out, nrows);
+    return cudaGetLastError();
+}
+
+// shared memory of corr_fold_kernel, in float2: two transform buffers, the
+// two twiddle tables, the staged half data row
+constexpr int kFoldBufs = 2 * fft_buf_len<kFoldH>();
+constexpr int kFoldSmem = kFoldBufs + kFoldTw1 + kFoldTw2 + kFoldH;
+static_assert((kFoldBufs + kFoldTw1 + kFoldTw2) % 2 == 0, "16-byte aligned staging row");
+
+// A plan's own launch at fftlen 2048: one CTA per kernel row (blockIdx.x)
+// of the group, rsteps of chunk blockIdx.y of gridDim.y; F: the group's
+// folded rows in launch order; ftw: the two twiddle tables.
+__global__ void __launch_bounds__(128, 4)
+    corr_fold_kernel(const __grid_constant__ SearchDev P, const __grid_constant__ RowGroup G,
+                     const float2 *__restrict__ F, const float2 *__restrict__ ftw)
+{
+    constexpr int H = kFoldH;
+    extern __shared__ __align__(16) float2 sm2[];
+    __shared__ uint64_t s_bar;
+    float2 *bufE = sm2;
+    float2 *bufO = sm2 + fft_buf_len<H>();
+    float2 *tws = sm2 + kFoldBufs;
+    float2 *dsm = tws + kFoldTw1 + kFoldTw2;
+    const int tid = threadIdx.x;
+    const int row = blockIdx.x;
+    int gi = 0;
+    while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
+        gi++;
+    const int s = G.sub[gi];
+    const int lrow = row - G.rowstart[gi];
+    const SubDev sd = P.subs[s];
+    const float2 *D0 = P.prepped + sd.data_off;
+    const int bchunk = (P.nb + (int)gridDim.y - 1) / (int)gridDim.y;
+    const int b0 = min(P.nb, (int)blockIdx.y * bchunk), b1 = min(P.nb, b0 + bchunk);
+    constexpr unsigned kRowBytes = H * sizeof(float2);
+
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0 && b0 < b1)
+        bulk_row_load(dsm, D0 + (long long)b0 * kFoldN, kRowBytes, &s_bar);
+    for (int i = tid; i < kFoldTw1 + kFoldTw2; i += 128)
+        tws[i] = ftw[i];
+    // this thread's folded kernel values: A and B at k = tid + 128 r
+    float2 ka[8], kb[8];
+    const float2 *Fr = F + (long long)row * kFoldN;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        ka[r] = Fr[tid + 128 * r];
+        kb[r] = Fr[H + tid + 128 * r];
+    }
+    __syncthreads();
+
+    const int offset = sd.halfwidth * 2;
+    const bool odd_half = tid >= 64;  // stage 1: warps 2-3 take the odd transform
+    for (int b = b0; b < b1; b++) {
+        const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
+        float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
+                      (long long)lrow * sd.stride;
+        if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
+            atomicOr(P.status, kStatusCopy);
+        // stage 0: radix 8 of both transforms from the same data values
+        {
+            float2 ve[8], vo[8];
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const float2 d = dsm[tid + 128 * r];
+                ve[r] = cmul(d, ka[r]);
+                vo[r] = cmul(d, kb[r]);
+            }
+            Dft<8, +1>::run(ve);
+            Dft<8, +1>::run(vo);
+            const int pd = pad(tid * 8);
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                bufE[pad_add(pd, r)] = ve[r];
+                bufO[pad_add(pd, r)] = vo[r];
+            }
+        }
+        __syncthreads();
+        // every thread has read the staged row: start the next rstep's copy
+        if (tid == 0 && b + 1 < b1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_row_load(dsm, D0 + (long long)(b + 1) * kFoldN, kRowBytes, &s_bar);
+        }
+        // stage 1: radix 16 (Ns = 8), 64 butterflies per transform
+        fft_stage_inplace<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, tws, tid & 63, true);
+        // stage 2: radix 8 (Ns = 128), butterfly tid of both, shared twiddles
+        {
+            float2 we[8], wo[8];
+            const int pj = pad(tid);
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                we[r] = bufE[pad_add(pj, r * 128)];
+                wo[r] = bufO[pad_add(pj, r * 128)];
+            }
+#pragma unroll
+            for (int r = 1; r < 8; r++) {
+                const float2 w = twiddle<+1>(tws + kFoldTw1, r * 128 + tid);
+                we[r] = cmul(we[r], w);
+                wo[r] = cmul(wo[r], w);
+            }
+            Dft<8, +1>::run(we);
+            Dft<8, +1>::run(wo);
+            // outputs 2 m and 2 m + 1, m = tid + 128 r: one pair of powers per
+            // 8-byte store (offset and numrs are even)
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const int kk = 2 * (tid + 128 * r) - offset;
+                const float pe = fmaf(we[r].x, we[r].x, we[r].y * we[r].y);
+                const float po = fmaf(wo[r].x, wo[r].x, wo[r].y * wo[r].y);
+                if ((unsigned)kk < (unsigned)numrs)
+                    *reinterpret_cast<float2 *>(outp + kk) = make_float2(pe, po);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One CTA of a wave at fftlen 2048 (the folded form): the same loop as
+// corr_fold_kernel, reaching its plan's arguments by reference.
+__device__ __forceinline__ void corr_fold_body(const SearchDev &P, const RowGroup &G,
+                                               const float2 *__restrict__ F,
+                                               const float2 *__restrict__ ftw, const int row,
+                                               const int b0, const int b1)
+{
+    constexpr int H = kFoldH;
+    extern __shared__ __align__(16) float2 sm2[];
+    __shared__ uint64_t s_bar;
+    float2 *bufE = sm2;
+    float2 *bufO = sm2 + fft_buf_len<H>();
+    float2 *tws = sm2 + kFoldBufs;
+    float2 *dsm = tws + kFoldTw1 + kFoldTw2;
+    const int tid = threadIdx.x;
+    int gi = 0;
+    while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
+        gi++;
+    const int s = G.sub[gi];
+    const int lrow = row - G.rowstart[gi];
+    const SubDev sd = P.subs[s];
+    const float2 *D0 = P.prepped + sd.data_off;
+    constexpr unsigned kRowBytes = H * sizeof(float2);
+
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0 && b0 < b1)
+        bulk_row_load(dsm, D0 + (long long)b0 * kFoldN, kRowBytes, &s_bar);
+    for (int i = tid; i < kFoldTw1 + kFoldTw2; i += 128)
+        tws[i] = ftw[i];
+    // this thread's folded kernel values: A and B at k = tid + 128 r
+    float2 ka[8], kb[8];
+    const float2 *Fr = F + (long long)row * kFoldN;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        ka[r] = Fr[tid + 128 * r];
+        kb[r] = Fr[H + tid + 128 * r];
+    }
+    __syncthreads();
+
+    const int offset = sd.halfwidth * 2;
+    const bool odd_half = tid >= 64;  // stage 1: warps 2-3 take the odd transform
+    for (int b = b0; b < b1; b++) {
+        const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
+        float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
+                      (long long)lrow * sd.stride;
+        if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
+            atomicOr(P.status, kStatusCopy);
+        // stage 0: radix 8 of both transforms from the same data values
+        {
+            float2 ve[8], vo[8];
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const float2 d = dsm[tid + 128 * r];
+                ve[r] = cmul(d, ka[r]);
+                vo[r] = cmul(d, kb[r]);
+            }
+            Dft<8, +1>::run(ve);
+            Dft<8, +1>::run(vo);
+            const int pd = pad(tid * 8);
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                bufE[pad_add(pd, r)] = ve[r];
+                bufO[pad_add(pd, r)] = vo[r];
+            }
+        }
+        __syncthreads();
+        // every thread has read the staged row: start the next rstep's copy
+        if (tid == 0 && b + 1 < b1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_row_load(dsm, D0 + (long long)(b + 1) * kFoldN, kRowBytes, &s_bar);
+        }
+        // stage 1: radix 16 (Ns = 8), 64 butterflies per transform
+        fft_stage_inplace<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, tws, tid & 63, true);
+        // stage 2: radix 8 (Ns = 128), butterfly tid of both, shared twiddles
+        {
+            float2 we[8], wo[8];
+            const int pj = pad(tid);
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                we[r] = bufE[pad_add(pj, r * 128)];
+                wo[r] = bufO[pad_add(pj, r * 128)];
+            }
+#pragma unroll
+            for (int r = 1; r < 8; r++) {
+                const float2 w = twiddle<+1>(tws + kFoldTw1, r * 128 + tid);
+                we[r] = cmul(we[r], w);
+                wo[r] = cmul(wo[r], w);
+            }
+            Dft<8, +1>::run(we);
+            Dft<8, +1>::run(wo);
+            // outputs 2 m and 2 m + 1, m = tid + 128 r: one pair of powers per
+            // 8-byte store (offset and numrs are even)
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const int kk = 2 * (tid + 128 * r) - offset;
+                const float pe = fmaf(we[r].x, we[r].x, we[r].y * we[r].y);
+                const float po = fmaf(wo[r].x, wo[r].x, wo[r].y * wo[r].y);
+                if ((unsigned)kk < (unsigned)numrs)
+                    *reinterpret_cast<float2 *>(outp + kk) = make_float2(pe, po);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(128, 4) corr_fold_group_kernel(const __grid_constant__ GroupLaunch M)
+{
+    const int i = group_plan(M, blockIdx.x);
+    const int local = blockIdx.x - M.cta0[i];
+    const int ny = M.ny[i];
+    int b0, b1;
+    rstep_chunk(M.P[i].nb, ny, local % ny, &b0, &b1);
+    corr_fold_body(M.P[i], M.G[i], M.fold[i], M.fold_tw[i], local / ny, b0, b1);
+}
+
+// A wave's plans at fftlen 2048, in the folded form (M.fold, M.fold_tw set).
+cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st)
+{
+    if (M.n < 1 || M.n > kMaxGroupPlans)
+        return cudaErrorInvalidValue;
+    const size_t smem = sizeof(float2) * kFoldSmem;
+    cudaError_t e = cudaFuncSetAttribute(corr_fold_group_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(corr_fold_group_kernel,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess)
+        return e;
+    const int wave = sm_count() * 4;
+    long long total = 0;
+    for (int i = 0; i < M.n; i++)
+        total += M.G[i].rowstart[M.G[i].n];
+    long long x = 0;
+    for (int i = 0; i < M.n; i++) {
+        const int rows = M.G[i].rowstart[M.G[i].n];
+        const int split = total >= 2 * wave ? 1
+                          : std::max(1, std::min(M.P[i].nb, (int)((2 * wave + total - 1) / total)));
+        M.cta0[i] = (int)x;
+        M.ny[i] = split;
+        x += (long long)rows * split;
+    }
+    if (x >= (1ll << 31))
+        return cudaErrorInvalidValue;
+    M.cta0[M.n] = (int)x;
+    corr_fold_group_kernel<<<(unsigned)x, 128, smem, st>>>(M);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corr_fold(const SearchDev &P, const RowGroup &G, int rows, const float2 *F,
+                             const float2 *ftw, cudaStream_t st)
+{
+    const size_t smem = sizeof(float2) * kFoldSmem;
+    cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(corr_fold_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess)
+        return e;
+    const int wave = sm_count() * 4;
+    const int split = rows >= 2 * wave ? 1 : std::max(1, std::min(P.nb, (2 * wave + rows - 1) / rows));
+    corr_fold_kernel<<<dim3(rows, split), 128, smem, st>>>(P, G, F, ftw);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // 3. Harmonic summing + threshold + compaction.
 
 constexpr int kHarmThreads = 128;

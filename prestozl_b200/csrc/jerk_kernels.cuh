@@ -117,6 +117,8 @@ struct GroupLaunch {
     int ny[kMaxGroupPlans];
     SearchDev P[kMaxGroupPlans];
     RowGroup G[kMaxGroupPlans];
+    const float2 *fold[kMaxGroupPlans];     // corr at fftlen 2048: folded kernel rows
+    const float2 *fold_tw[kMaxGroupPlans];  // and their twiddle tables
 };
 static_assert(sizeof(GroupLaunch) <= 30000, "kernel parameter space");
 

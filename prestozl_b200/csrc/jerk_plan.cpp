@@ -40,6 +40,13 @@ cudaError_t launch_corr_group(GroupLaunch M, int fftlen, cudaStream_t st);
 cudaError_t launch_harmsum_group(GroupLaunch M, int nstages, cudaStream_t st);
 cudaError_t launch_wait_probe(unsigned int *status, cudaStream_t st);
 int corr_wave_ctas(int fftlen);
+int fold_twiddle_size();
+void fold_twiddle_table(float2 *out);
+cudaError_t launch_fold_rows(const float2 *bank, const long long *src, float2 *out, int nrows,
+                             cudaStream_t st);
+cudaError_t launch_corr_fold(const SearchDev &P, const RowGroup &G, int rows, const float2 *F,
+                             const float2 *ftw, cudaStream_t st);
+cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st);
 int harmsum_wave_ctas(int nstages);
 int fft_twiddle_size(int N);
 void fft_twiddle_table(int N, float2 *out);
@@ -737,6 +744,11 @@ struct jerk_plan {
     float2 *d_bank = nullptr;
     bool own_bank = false;
     float2 *d_tw = nullptr;
+    // fftlen 2048: the rows folded for the half-length correlation, and the
+    // offset of its twiddle tables in d_tw
+    float2 *d_fold = nullptr;
+    long long fold_floats2 = 0;
+    int fold_twoff = -1;
     SubDev *d_subs = nullptr;
     StepDev *d_steps = nullptr;
     uint16_t *d_zinds = nullptr;
@@ -895,6 +907,7 @@ static void plan_free_device(jerk_plan *p)
     if (p->own_bank)
         cudaFree(p->d_bank);
     cudaFree(p->d_tw);
+    cudaFree(p->d_fold);
     cudaFree(p->d_subs);
     cudaFree(p->d_steps);
     cudaFree(p->d_zinds);
@@ -1211,6 +1224,12 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
         for (auto &o : byoff)
             append_twiddles(o.second, tw);
     }
+    if (p->groups.count(2048)) {
+        p->fold_twoff = twtotal;
+        tw.resize(twtotal + fold_twiddle_size());
+        fold_twiddle_table(tw.data() + twtotal);
+        twtotal += fold_twiddle_size();
+    }
 
 #define JERK_CUDA_B(call)                                \
     do {                                                 \
@@ -1237,6 +1256,25 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     JERK_CUDA_B(cudaMalloc(&p->d_tw, sizeof(float2) * twtotal));
     JERK_CUDA_B(cudaMemcpyAsync(p->d_tw, tw.data(), sizeof(float2) * twtotal,
                                 cudaMemcpyHostToDevice, p->stream));
+    // fftlen 2048: fold the bank's rows once for the half-length correlation
+    // (the bank must be complete when the plan is made; jerk_bank_generate
+    // returns once it is)
+    std::vector<long long> fold_src;
+    long long *d_fold_src = nullptr;
+    if (p->fold_twoff >= 0) {
+        for (int s : p->groups[2048]) {
+            const long long nrow = (long long)subs[s].numw * subs[s].numz;
+            for (long long r = 0; r < nrow; r++)
+                fold_src.push_back(p->hsubs[s].kern_off + r * 2048);
+        }
+        p->fold_floats2 = (long long)fold_src.size() * 2048;
+        JERK_CUDA_B(cudaMalloc(&p->d_fold, sizeof(float2) * p->fold_floats2));
+        JERK_CUDA_B(cudaMalloc(&d_fold_src, sizeof(long long) * fold_src.size()));
+        JERK_CUDA_B(cudaMemcpyAsync(d_fold_src, fold_src.data(), sizeof(long long) * fold_src.size(),
+                                    cudaMemcpyHostToDevice, p->stream));
+        JERK_CUDA_B(launch_fold_rows(p->d_bank, d_fold_src, p->d_fold, (int)fold_src.size(),
+                                     p->stream));
+    }
     JERK_CUDA_B(cudaMalloc(&p->d_subs, sizeof(SubDev) * nsubs));
     JERK_CUDA_B(cudaMemcpyAsync(p->d_subs, p->hsubs.data(), sizeof(SubDev) * nsubs,
                                 cudaMemcpyHostToDevice, p->stream));
@@ -1280,6 +1318,7 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
             return bail(rc);
     }
     JERK_CUDA_B(cudaStreamSynchronize(p->stream));
+    cudaFree(d_fold_src);
 #undef JERK_CUDA_B
     *out = p;
     return JERK_OK;
@@ -1344,6 +1383,16 @@ static inline double fft_flops(int n)
     return 5.0 * n * log2((double)n);
 }
 
+// The plan's own correlation launch for one FFT length (the folded form at
+// 2048).
+static cudaError_t launch_corr_of(const jerk_plan *p, const SearchDev &a, int N, const RowGroup &G,
+                                  cudaStream_t st)
+{
+    if (N == 2048 && p->d_fold)
+        return launch_corr_fold(a, G, G.rowstart[G.n], p->d_fold, p->d_tw + p->fold_twoff, st);
+    return launch_corr(a, N, G, G.rowstart[G.n], st);
+}
+
 // The rows of the subharmonics subs (one fftlen), numbered consecutively.
 static RowGroup row_group(const jerk_plan *p, const std::vector<int> &subs)
 {
@@ -1393,7 +1442,7 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
             flops += nrow * a.nb * (fft_flops(N) + 6.0 * N) + nrow * numrs * 3.0;
         }
         const int tok = launch_begin(p, kclass(p, "corr_" + std::to_string(N)), bytes, flops);
-        e = launch_corr(a, N, G, rows, p->stream);
+        e = launch_corr_of(p, a, N, G, p->stream);
         launch_end(p, tok);
         if (e != cudaSuccess)
             return cuda_fail(e, "corr_kernel");
@@ -1756,7 +1805,7 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
                 continue;
             }
             tok = launch_begin(p0, kclass(p0, "wave_corr_" + std::to_string(kv.first)), 0.0, 0.0);
-            e = launch_corr(p->pass.a, kv.first, G, G.rowstart[G.n], st);
+            e = launch_corr_of(p, p->pass.a, kv.first, G, st);
             launch_end(p0, tok);
             if (e != cudaSuccess)
                 return fail_all(e, "corr_kernel");
@@ -1767,11 +1816,17 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
         GroupLaunch C{};
         C.n = (int)kv.second.size();
         double bytes = 0, flops = 0;
+        bool fold = N == 2048;
         for (int j = 0; j < C.n; j++) {
             jerk_plan *p = W[kv.second[j]];
             const SearchDev &a = p->pass.a;
             C.P[j] = a;
             C.G[j] = row_group(p, p->groups.at(N));
+            // at 2048 every plan has folded rows (made with the plan), so the
+            // merged launch computes exactly what the plan's own launch does
+            fold = fold && p->d_fold;
+            C.fold[j] = p->d_fold;
+            C.fold_tw[j] = p->d_fold ? p->d_tw + p->fold_twoff : nullptr;
             for (int g = 0; g < C.G[j].n; g++) {
                 const int s = C.G[j].sub[g];
                 const double nrow = (double)p->subs[s].numw * p->subs[s].numz;
@@ -1783,7 +1838,7 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
             }
         }
         tok = launch_begin(p0, kclass(p0, "wave_corr_" + std::to_string(N)), bytes, flops);
-        e = launch_corr_group(C, N, st);
+        e = fold ? launch_corr_fold_group(C, st) : launch_corr_group(C, N, st);
         launch_end(p0, tok);
         if (e != cudaSuccess)
             return fail_all(e, "corr_group_kernel");
@@ -2109,6 +2164,7 @@ extern "C" long long jerk_plan_device_bytes(const jerk_plan *p)
                        sizeof(float2) * p->prepped_f2 +
                        (sizeof(unsigned long long) + sizeof(float)) * p->max_hits +
                        sizeof(StepDev) * p->hsteps.size() + sizeof(float2) * p->spec_cap +
+                       sizeof(float2) * p->fold_floats2 +
                        (p->own_bank ? sizeof(float2) * jerk_bank_elements(p->subs.data(), p->nsubs)
                                     : 0));
 }
