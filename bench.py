@@ -49,13 +49,14 @@ WORKLOAD = "jerk search, 2^25-sample spectra, -zmax 200 -wmax 300 -numharm 16 -s
 # lanes x 2 flops per FMA x 1965 MHz); the correlation kernels are bound by it.
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
-# DRAM traffic of one corr_kernel<2048> launch at 16 rsteps per batch, from an
-# ncu capture (dram__bytes_read.sum / dram__bytes_write.sum) of
+# DRAM traffic of one fftlen-2048 correlation launch (corr_fold_kernel) at 16
+# rsteps per batch, from an ncu capture (dram__bytes_read.sum /
+# dram__bytes_write.sum) of
 #   python bench.py --rsteps 128 --steps 1 --warmup 1 --no-cpu-baseline --no-ref-gpu
-#                   --e2e-steps 1 --batch 16
-# The read side (kernel rows + data rows) is paid once per launch; the write
-# side (the volumes) grows with the rsteps per batch.
-CORR2048_TRAFFIC = {"read": 492.14464e6, "write": 2244.205e6, "batch": 16}
+#                   --e2e-steps 1 --batch 16 --no-extras
+# The read side (folded kernel rows + data rows) is paid once per launch; the
+# write side (the volumes) grows with the rsteps per batch.
+CORR2048_TRAFFIC = {"read": 492.621312e6, "write": 2241.046e6, "batch": 16}
 
 
 def corr2048_traffic(batch: int) -> float:
@@ -1126,8 +1127,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": traffic,
-                         "traffic_source": "ncu capture at 16 rsteps per batch, write side "
-                                           "scaled by rsteps per batch" if traffic else None,
+                         "traffic_source": "ncu capture of corr_fold_kernel at 16 rsteps per "
+                                           "batch, write side scaled by rsteps per batch"
+                                           if traffic else None,
                          "fp32": {"achieved": fp32_achieved, "peak": FP32_PEAK_TFLOPS,
                                   "unit": "TFLOP/s", "frac": fp32_achieved / FP32_PEAK_TFLOPS,
                                   "peak_source": "nominal (148 SMs x 128 lanes x 2 x 1965 MHz)"},
