@@ -296,6 +296,38 @@ __device__ __forceinline__ void fft_stage_inplace(float2 *buf, const float2 *tw,
     __syncthreads();
 }
 
+// One middle stage from src to dst (separate buffers): no barrier inside;
+// the caller syncs before dst is read and before src is written again.
+template <int N, int SIGN, int T, int Ns, int R>
+__device__ __forceinline__ void fft_stage_oop(const float2 *src, float2 *dst, const float2 *tw,
+                                              int tid)
+{
+    constexpr int NB = N / R;
+    static_assert(NB % T == 0 && IsPow2<NB>::value && NB >= 16 && IsPow2<Ns>::value &&
+                      IsPow2<R>::value, "power-of-two stage, whole butterflies per thread");
+    constexpr int PER = NB / T;
+#pragma unroll
+    for (int p = 0; p < PER; p++) {
+        const int j = tid + p * T;
+        float2 v[R];
+        const int pj = pad(j);
+#pragma unroll
+        for (int r = 0; r < R; r++)
+            v[r] = src[pad_add(pj, r * NB)];
+        const int k = j % Ns;
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++)
+                v[r] = cmul(v[r], twiddle<SIGN>(tw, r * Ns + k));
+        }
+        Dft<R, SIGN>::run(v);
+        const int pd = pad((j / Ns) * Ns * R + k);
+#pragma unroll
+        for (int r = 0; r < R; r++)
+            dst[pad_add(pd, r * Ns)] = v[r];
+    }
+}
+
 // Last stage: Ns * R == N, so the output index of (j, r) is j + r * Ns.
 // No barrier inside; the caller must sync before buf is written again.
 template <int N, int SIGN, int T, int Ns, int R, class Out>

@@ -679,7 +679,7 @@ cudaError_t launch_fold_rows(const float2 *bank, const long long *src, float2 *o
 
 // shared memory of corr_fold_kernel, in float2: two transform buffers, the
 // two twiddle tables, the staged half data row
-constexpr int kFoldBufs = 2 * fft_buf_len<kFoldH>();
+constexpr int kFoldBufs = 4 * fft_buf_len<kFoldH>();
 constexpr int kFoldSmem = kFoldBufs + kFoldTw1 + kFoldTw2 + kFoldH;
 static_assert((kFoldBufs + kFoldTw1 + kFoldTw2) % 2 == 0, "16-byte aligned staging row");
 
@@ -693,8 +693,12 @@ __global__ void __launch_bounds__(128, 4)
     constexpr int H = kFoldH;
     extern __shared__ __align__(16) float2 sm2[];
     __shared__ uint64_t s_bar;
+    // stage 0 writes bufE / bufO, stage 1 reads them and writes outE / outO,
+    // stage 2 reads those: two barriers per rstep
     float2 *bufE = sm2;
     float2 *bufO = sm2 + fft_buf_len<H>();
+    float2 *outE = sm2 + 2 * fft_buf_len<H>();
+    float2 *outO = sm2 + 3 * fft_buf_len<H>();
     float2 *tws = sm2 + kFoldBufs;
     float2 *dsm = tws + kFoldTw1 + kFoldTw2;
     const int tid = threadIdx.x;
@@ -762,15 +766,17 @@ __global__ void __launch_bounds__(128, 4)
             bulk_row_load(dsm, D0 + (long long)(b + 1) * kFoldN, kRowBytes, &s_bar);
         }
         // stage 1: radix 16 (Ns = 8), 64 butterflies per transform
-        fft_stage_inplace<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, tws, tid & 63, true);
+        fft_stage_oop<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, odd_half ? outO : outE, tws,
+                                        tid & 63);
+        __syncthreads();
         // stage 2: radix 8 (Ns = 128), butterfly tid of both, shared twiddles
         {
             float2 we[8], wo[8];
             const int pj = pad(tid);
 #pragma unroll
             for (int r = 0; r < 8; r++) {
-                we[r] = bufE[pad_add(pj, r * 128)];
-                wo[r] = bufO[pad_add(pj, r * 128)];
+                we[r] = outE[pad_add(pj, r * 128)];
+                wo[r] = outO[pad_add(pj, r * 128)];
             }
 #pragma unroll
             for (int r = 1; r < 8; r++) {
@@ -791,7 +797,9 @@ __global__ void __launch_bounds__(128, 4)
                     *reinterpret_cast<float2 *>(outp + kk) = make_float2(pe, po);
             }
         }
-        __syncthreads();
+        // no barrier: the next rstep's stage 0 writes bufE / bufO, last read
+        // in stage 1 before the barrier above, and its stage 1 writes
+        // outE / outO only after the barrier that follows its stage 0
     }
 }
 
@@ -805,8 +813,12 @@ __device__ __forceinline__ void corr_fold_body(const SearchDev &P, const RowGrou
     constexpr int H = kFoldH;
     extern __shared__ __align__(16) float2 sm2[];
     __shared__ uint64_t s_bar;
+    // stage 0 writes bufE / bufO, stage 1 reads them and writes outE / outO,
+    // stage 2 reads those: two barriers per rstep
     float2 *bufE = sm2;
     float2 *bufO = sm2 + fft_buf_len<H>();
+    float2 *outE = sm2 + 2 * fft_buf_len<H>();
+    float2 *outO = sm2 + 3 * fft_buf_len<H>();
     float2 *tws = sm2 + kFoldBufs;
     float2 *dsm = tws + kFoldTw1 + kFoldTw2;
     const int tid = threadIdx.x;
@@ -871,15 +883,17 @@ __device__ __forceinline__ void corr_fold_body(const SearchDev &P, const RowGrou
             bulk_row_load(dsm, D0 + (long long)(b + 1) * kFoldN, kRowBytes, &s_bar);
         }
         // stage 1: radix 16 (Ns = 8), 64 butterflies per transform
-        fft_stage_inplace<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, tws, tid & 63, true);
+        fft_stage_oop<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, odd_half ? outO : outE, tws,
+                                        tid & 63);
+        __syncthreads();
         // stage 2: radix 8 (Ns = 128), butterfly tid of both, shared twiddles
         {
             float2 we[8], wo[8];
             const int pj = pad(tid);
 #pragma unroll
             for (int r = 0; r < 8; r++) {
-                we[r] = bufE[pad_add(pj, r * 128)];
-                wo[r] = bufO[pad_add(pj, r * 128)];
+                we[r] = outE[pad_add(pj, r * 128)];
+                wo[r] = outO[pad_add(pj, r * 128)];
             }
 #pragma unroll
             for (int r = 1; r < 8; r++) {
@@ -900,7 +914,9 @@ __device__ __forceinline__ void corr_fold_body(const SearchDev &P, const RowGrou
                     *reinterpret_cast<float2 *>(outp + kk) = make_float2(pe, po);
             }
         }
-        __syncthreads();
+        // no barrier: the next rstep's stage 0 writes bufE / bufO, last read
+        // in stage 1 before the barrier above, and its stage 1 writes
+        // outE / outO only after the barrier that follows its stage 0
     }
 }
 
