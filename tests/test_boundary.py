@@ -196,3 +196,21 @@ def test_dedisp_plan_rejects_bad_offsets():
     with pytest.raises(jerk.JerkError) as ei:  # 4096 subband rows of 32 samples: too wide
         jerk.dedisp_plan(64, 4096, np.zeros((1, 4096)))
     assert ei.value.code == jerk.JERK_EUNSUPPORTED
+
+
+def test_merge_hits_host_only_edges():
+    """jerk_merge_hits needs no GPU: no hits give an empty list, a key past
+    the last rstep or mismatched lengths are refused."""
+    import numpy as np
+
+    from prestozl_b200 import jerk
+
+    obs, fftlen, _ = jerk.obs_from_params(1 << 19, 1 << 20, 64e-6, 20, 60, 8, 2.0)
+    fund = jerk.subharm_sizes(obs, fftlen)[0]
+    assert len(jerk.merge_hits(obs, fund, np.zeros(0, np.uint64), np.zeros(0, np.float32))) == 0
+    per_rstep = obs.numharmstages * fund["numw"] * fund["numz"] * obs.corr_uselen
+    with pytest.raises(jerk.JerkError):
+        jerk.merge_hits(obs, fund, np.array([per_rstep * 10 ** 6], np.uint64),
+                        np.array([50.0], np.float32))
+    with pytest.raises(jerk.JerkError):
+        jerk.merge_hits(obs, fund, np.array([1, 2], np.uint64), np.array([50.0], np.float32))
