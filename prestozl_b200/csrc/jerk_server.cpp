@@ -141,21 +141,23 @@ static BankKey key_of(const Geometry &g)
 }
 
 // Device bytes a plan for g will hold (volumes, rinds, chunks, hit buffer,
-// steps, spectrum staging).
+// steps, spectrum staging, and its folded copy of the fftlen-2048 rows).
 static long long plan_footprint(const Geometry &g, int batch)
 {
-    long long vol = 0, chunks = 0;
+    long long vol = 0, chunks = 0, folded = 0;
     for (const auto &s : g.subs) {
         const double hf = (double)s.harmnum / s.numharm;
         const long long stride = (((long long)(g.obs.corr_uselen * hf) + 8) + 3) & ~3LL;
         vol += (long long)s.numw * s.numz * stride * 4;
         chunks += (long long)s.fftlen * 8;
+        if (s.fftlen == 2048)
+            folded += (long long)s.numw * s.numz * 2048 * 8;
     }
     const long long rsteps = (long long)((g.obs.highestbin - g.obs.rlo) / (g.obs.corr_uselen / 2)) + 1;
     return vol * batch + chunks * batch +
            2LL * batch * (long long)g.subs.size() * g.obs.corr_uselen +
            (long long)(1 << 22) * 12 + rsteps * (long long)g.subs.size() * 24 +
-           g.obs.numbins * 8 + (64LL << 20);
+           g.obs.numbins * 8 + folded + (64LL << 20);
 }
 
 // Device bytes of a time-series request's buffer: the series (turned into its
