@@ -442,6 +442,113 @@ __device__ __forceinline__ void fft_block(float2 *buf, const float2 *tw, int tid
     fft_block<N, SIGN>(buf, tw, tid, in, out, [] {});
 }
 
+// ---------------------------------------------------------------------------
+// Two transforms at once in the two lanes of sm_100's packed FP32
+// instructions (add / sub / mul / fma .f32x2).  A Cp holds one complex value
+// of each transform: re = (re of lane 0, re of lane 1), im likewise.  Each
+// packed operation rounds every lane as its scalar form does (round to
+// nearest even), so the two transforms are computed exactly as two scalar
+// runs of the same operation sequence would be, with half the instructions.
+struct Cp {
+    float2 re, im;
+};
+
+__device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
+        "mov.b64 pa, {%2, %3};\n\t"
+        "mov.b64 pb, {%4, %5};\n\t"
+        "sub.rn.f32x2 pd, pa, pb;\n\t"
+        "mov.b64 {%0, %1}, pd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ Cp padd(Cp a, Cp b) { return {add2(a.re, b.re), add2(a.im, b.im)}; }
+__device__ __forceinline__ Cp psub(Cp a, Cp b) { return {sub2(a.re, b.re), sub2(a.im, b.im)}; }
+// a + i b and a - i b
+__device__ __forceinline__ Cp padd_i(Cp a, Cp b) { return {sub2(a.re, b.im), add2(a.im, b.re)}; }
+__device__ __forceinline__ Cp psub_i(Cp a, Cp b) { return {add2(a.re, b.im), sub2(a.im, b.re)}; }
+// a (c + i s) for a constant or table root shared by both lanes:
+// (re c - im s, im c + re s), each part one product and one fused add
+__device__ __forceinline__ Cp pmul(Cp a, float c, float s)
+{
+    return {fma2(a.re, bc(c), mul2(a.im, bc(-s))), fma2(a.im, bc(c), mul2(a.re, bc(s)))};
+}
+
+// Inverse (exponent sign +1) DFTs of radix 4, 8 and 16 on lane pairs; the
+// output order is that of Dft<R, +1>.
+__device__ __forceinline__ void pdft4(Cp &v0, Cp &v1, Cp &v2, Cp &v3)
+{
+    const Cp a = padd(v0, v2), b = psub(v0, v2), c = padd(v1, v3), e = psub(v1, v3);
+    v0 = padd(a, c);
+    v2 = psub(a, c);
+    v1 = padd_i(b, e);
+    v3 = psub_i(b, e);
+}
+
+__device__ __forceinline__ void pdft8(Cp *v)
+{
+    pdft4(v[0], v[2], v[4], v[6]);
+    pdft4(v[1], v[3], v[5], v[7]);
+    // now v[0, 2, 4, 6] = E[0..3], v[1, 3, 5, 7] = O[0..3]
+    const float h = 0.70710678118654752440f;
+    const Cp e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    const Cp o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    // W8 = h (1 + i):   W8 O1 = h (t.re, t.im),  t = (o.re - o.im, o.im + o.re)
+    // W8^3 = h (-1 + i): W8^3 O3 = h (-u.re, u.im), u = (o.re + o.im, o.re - o.im)
+    const float2 tr = sub2(o1.re, o1.im), ti = add2(o1.im, o1.re);
+    const float2 ur = add2(o3.re, o3.im), ui = sub2(o3.re, o3.im);
+    v[0] = padd(e0, o0);
+    v[4] = psub(e0, o0);
+    v[1] = {fma2(bc(h), tr, e1.re), fma2(bc(h), ti, e1.im)};
+    v[5] = {fma2(bc(-h), tr, e1.re), fma2(bc(-h), ti, e1.im)};
+    v[2] = padd_i(e2, o2);
+    v[6] = psub_i(e2, o2);
+    v[3] = {fma2(bc(-h), ur, e3.re), fma2(bc(h), ui, e3.im)};
+    v[7] = {fma2(bc(h), ur, e3.re), fma2(bc(-h), ui, e3.im)};
+}
+
+// 16 = 4 x 4 as in Dft<16>: DFT4 over n1 for each n2, W16^(n2 k1), DFT4 over n2
+__device__ __forceinline__ void pdft16(Cp *v)
+{
+    const float c1 = 0.92387953251128675613f;  // cos(pi/8)
+    const float s1 = 0.38268343236508977173f;  // sin(pi/8)
+    const float h = 0.70710678118654752440f;
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++)
+        pdft4(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
+    // element (n2, k1) is now v[n2 + 4 k1]; multiply by W16^(n2 k1)
+    v[1 + 4] = pmul(v[1 + 4], c1, s1);                                          // m = 1
+    v[1 + 8] = {mul2(bc(h), sub2(v[9].re, v[9].im)), mul2(bc(h), add2(v[9].im, v[9].re))};  // 2
+    v[1 + 12] = pmul(v[1 + 12], s1, c1);                                        // m = 3
+    v[2 + 4] = {mul2(bc(h), sub2(v[6].re, v[6].im)), mul2(bc(h), add2(v[6].im, v[6].re))};  // 2
+    v[2 + 8] = {mul2(bc(-1.0f), v[10].im), v[10].re};                           // m = 4
+    v[2 + 12] = {mul2(bc(-h), add2(v[14].re, v[14].im)), mul2(bc(h), sub2(v[14].re, v[14].im))};  // 6
+    v[3 + 4] = pmul(v[3 + 4], s1, c1);                                          // m = 3
+    v[3 + 8] = {mul2(bc(-h), add2(v[11].re, v[11].im)), mul2(bc(h), sub2(v[11].re, v[11].im))};  // 6
+    v[3 + 12] = pmul(v[3 + 12], -c1, -s1);                                      // m = 9
+    // DFT4 over n2 for each k1: inputs v[4 k1 + n2], outputs k1 + 4 k2
+    Cp t[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+        Cp a0 = v[4 * k1], a1 = v[4 * k1 + 1], a2 = v[4 * k1 + 2], a3 = v[4 * k1 + 3];
+        pdft4(a0, a1, a2, a3);
+        t[k1] = a0;
+        t[k1 + 4] = a1;
+        t[k1 + 8] = a2;
+        t[k1 + 12] = a3;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+        v[i] = t[i];
+}
+
 // Host: the per-stage twiddle tables of FftPlan<N>, forward sign, computed
 // in double and rounded to float.
 template <int N>

@@ -612,15 +612,17 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrGroupOcc<N>::value)
 // rows of length 2048 once (fold_rows_kernel, in double, each value rounded
 // once) and the correlation runs two 1024-point transforms that read each
 // data value once for both: the first radix-2 layer of the 2048-point
-// transform (its butterflies and twiddles) is gone, the last stage shares
-// its twiddles between the two transforms, and each thread stores the two
-// powers of an output pair with one 8-byte store.
+// transform (its butterflies and twiddles) is gone, and the two transforms
+// share every twiddle and every data value.
 //
-// The 1024-point plan is [8, 16, 8] for 128 threads: stage 0 (radix 8, 128
-// butterflies) -- thread j does butterfly j of both transforms from the same
-// 8 data values; stage 1 (radix 16, 64 butterflies each) -- threads 0-63 the
-// even transform, 64-127 the odd one; stage 2 (radix 8, 128 butterflies) --
-// thread j butterfly j of both, with shared twiddles.
+// The two transforms run in the two lanes of packed FP32 instructions
+// (Cp, pdft8, pdft16): every butterfly of the even transform has its twin
+// in the odd one at the same position with the same twiddle, so each
+// instruction does both.  The 1024-point plan is [8, 16, 8] for 128
+// threads: stage 0 (radix 8) -- thread j does butterfly j of both from the
+// same 8 data values; stage 1 (radix 16, 64 butterflies) -- warps 0-1,
+// butterfly j of both; stage 2 (radix 8) -- thread j butterfly j of both,
+// and the lane pair of powers (outputs 2 m, 2 m + 1) is one 8-byte store.
 
 static int sm_count();
 
@@ -677,11 +679,167 @@ cudaError_t launch_fold_rows(const float2 *bank, const long long *src, float2 *o
     return cudaGetLastError();
 }
 
-// shared memory of corr_fold_kernel, in float2: two transform buffers, the
-// two twiddle tables, the staged half data row
-constexpr int kFoldBufs = 4 * fft_buf_len<kFoldH>();
-constexpr int kFoldSmem = kFoldBufs + kFoldTw1 + kFoldTw2 + kFoldH;
-static_assert((kFoldBufs + kFoldTw1 + kFoldTw2) % 2 == 0, "16-byte aligned staging row");
+// Shared memory of the folded correlation.  The transform buffers hold one
+// lane pair per point, float4 (re even, re odd, im even, im odd), with one
+// float4 of padding after every 8 (one 128-byte row of banks), so that the
+// 16-byte accesses of each quarter-warp fall in 8 distinct bank groups in
+// every stage:
+//   stage 0 writes 8 t + r            -> padded 9 t + r
+//   stage 1 reads  j + 64 r           -> padded j + j/8 + 72 r
+//           writes 128 (j/8) + j%8 + 8 r -> padded 144 (j/8) + j%8 + 9 r
+//   stage 2 reads  t + 128 r          -> padded t + t/8 + 144 r
+// After the buffers: the two twiddle tables (float2) and the staged half
+// data row.
+__host__ __device__ constexpr int pad4(int i) { return i + (i >> 3); }
+constexpr int kFoldBuf4 = kFoldH + kFoldH / 8;  // float4 per buffer
+constexpr int kFoldSmem = 2 * kFoldBuf4 * 16 + (kFoldTw1 + kFoldTw2 + kFoldH) * 8;  // bytes
+static_assert((2 * kFoldBuf4 * 16 + (kFoldTw1 + kFoldTw2) * 8) % 16 == 0,
+              "16-byte aligned staging row");
+
+__device__ __forceinline__ void st_cp(float4 *p, const Cp &v)
+{
+    *p = make_float4(v.re.x, v.re.y, v.im.x, v.im.y);
+}
+__device__ __forceinline__ Cp ld_cp(const float4 *p)
+{
+    const float4 q = *p;
+    return {make_float2(q.x, q.y), make_float2(q.z, q.w)};
+}
+// v (c + i s) with (c, s) the conjugate of a forward table root w: the
+// inverse transform's twiddle
+__device__ __forceinline__ Cp pmul_conj(const Cp &v, float2 w) { return pmul(v, w.x, -w.y); }
+
+// The rstep loop of one CTA of the folded correlation (both launch forms).
+// kr[r], ki[r]: the lane pairs (re A, re B), (im A, im B) of the row's
+// folded values at k = tid + 128 r.  steps: the row's subharmonic at b = 0
+// (stride nsubs per rstep); out: its volume row at b = 0.
+__device__ __forceinline__ void fold_rsteps(float4 *bufA, float4 *bufB, const float2 *tw1,
+                                            const float2 *tw2, const float2 *dsm, uint64_t *bar,
+                                            const float2 (&kr)[8], const float2 (&ki)[8],
+                                            const float2 *D0, const StepDev *steps, int nsubs,
+                                            float *out, long long plane_size, int offset,
+                                            int b0, int b1, unsigned *status)
+{
+    constexpr unsigned kRowBytes = kFoldH * sizeof(float2);
+    const int tid = threadIdx.x;
+    for (int b = b0; b < b1; b++) {
+        const int numrs = steps[(long long)b * nsubs].numrs;
+        float *outp = out + (long long)b * plane_size;
+        if (!bar_wait(bar, (b - b0) & 1) && status)
+            atomicOr(status, kStatusCopy);
+        // stage 0: radix 8 of both transforms from the same data values
+        {
+            Cp v[8];
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const float2 d = dsm[tid + 128 * r];
+                // d A and d B: (dr ar - di ai, dr ai + di ar) per lane
+                v[r].re = fma2(bc(d.x), kr[r], mul2(bc(-d.y), ki[r]));
+                v[r].im = fma2(bc(d.x), ki[r], mul2(bc(d.y), kr[r]));
+            }
+            pdft8(v);
+            // stage 1's input twiddles, applied here: element 8 t + r of
+            // this stage is input (t / 8) of stage-1 butterfly
+            // 8 (t % 8) + r, whose twiddle is W_128^((t / 8) r)
+            const float2 *w1 = tw1 + (tid >> 3) * 8;
+#pragma unroll
+            for (int r = 1; r < 8; r++)
+                v[r] = pmul_conj(v[r], w1[r]);
+            float4 *p = bufA + 9 * tid;
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+                st_cp(p + r, v[r]);
+        }
+        __syncthreads();
+        // every thread has read the staged row: start the next rstep's copy
+        if (tid == 0 && b + 1 < b1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_row_load(const_cast<float2 *>(dsm), D0 + (long long)(b + 1) * kFoldN, kRowBytes,
+                          bar);
+        }
+        // stage 1: radix 16 (Ns = 8), butterfly j = tid of both transforms,
+        // by warps 0-1
+        if (tid < 64) {
+            const int j = tid, k = j & 7;
+            Cp v[16];
+            const float4 *p = bufA + j + (j >> 3);
+#pragma unroll
+            for (int r = 0; r < 16; r++)
+                v[r] = ld_cp(p + 72 * r);
+            pdft16(v);
+            float4 *q = bufB + 144 * (j >> 3) + k;
+#pragma unroll
+            for (int r = 0; r < 16; r++)
+                st_cp(q + 9 * r, v[r]);
+        }
+        __syncthreads();
+        // stage 2: radix 8 (Ns = 128), butterfly tid of both
+        {
+            Cp v[8];
+            const float4 *p = bufB + tid + (tid >> 3);
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+                v[r] = ld_cp(p + 144 * r);
+#pragma unroll
+            for (int r = 1; r < 8; r++)
+                v[r] = pmul_conj(v[r], tw2[r * 128 + tid]);
+            pdft8(v);
+            // outputs 2 m and 2 m + 1, m = tid + 128 r: the lane pair of
+            // powers is one 8-byte store (offset and numrs are even)
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const int kk = 2 * (tid + 128 * r) - offset;
+                const float2 pw = fma2(v[r].re, v[r].re, mul2(v[r].im, v[r].im));
+                if ((unsigned)kk < (unsigned)numrs)
+                    *reinterpret_cast<float2 *>(outp + kk) = pw;
+            }
+        }
+        // no barrier: the next rstep's stage 0 writes bufA, last read in
+        // stage 1 before the barrier above, and its stage 1 writes bufB only
+        // after the barrier that follows its stage 0
+    }
+}
+
+// Set-up shared by both launch forms: carve shared memory, start the first
+// data-row copy, stage the twiddles, load this thread's folded values, then
+// run the rstep loop.
+__device__ __forceinline__ void fold_cta(const SubDev &sd, const float2 *prepped,
+                                         const StepDev *steps, int nsubs, float *planes,
+                                         int lrow, const float2 *__restrict__ Fr,
+                                         const float2 *__restrict__ ftw, int b0, int b1,
+                                         unsigned *status)
+{
+    extern __shared__ __align__(16) float4 sm4[];
+    __shared__ uint64_t s_bar;
+    float4 *bufA = sm4;
+    float4 *bufB = sm4 + kFoldBuf4;
+    float2 *tws = reinterpret_cast<float2 *>(sm4 + 2 * kFoldBuf4);
+    float2 *dsm = tws + kFoldTw1 + kFoldTw2;
+    const int tid = threadIdx.x;
+    const float2 *D0 = prepped + sd.data_off;
+    constexpr unsigned kRowBytes = kFoldH * sizeof(float2);
+
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0 && b0 < b1)
+        bulk_row_load(dsm, D0 + (long long)b0 * kFoldN, kRowBytes, &s_bar);
+    for (int i = tid; i < kFoldTw1 + kFoldTw2; i += 128)
+        tws[i] = ftw[i];
+    float2 kr[8], ki[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const float2 a = Fr[tid + 128 * r], bb = Fr[kFoldH + tid + 128 * r];
+        kr[r] = make_float2(a.x, bb.x);
+        ki[r] = make_float2(a.y, bb.y);
+    }
+    __syncthreads();
+    fold_rsteps(bufA, bufB, tws, tws + kFoldTw1, dsm, &s_bar, kr, ki, D0, steps, nsubs,
+                planes + sd.plane_off + (long long)lrow * sd.stride, sd.plane_size,
+                sd.halfwidth * 2, b0, b1, status);
+}
 
 // A plan's own launch at fftlen 2048: one CTA per kernel row (blockIdx.x)
 // of the group, rsteps of chunk blockIdx.y of gridDim.y; F: the group's
@@ -690,234 +848,15 @@ __global__ void __launch_bounds__(128, 4)
     corr_fold_kernel(const __grid_constant__ SearchDev P, const __grid_constant__ RowGroup G,
                      const float2 *__restrict__ F, const float2 *__restrict__ ftw)
 {
-    constexpr int H = kFoldH;
-    extern __shared__ __align__(16) float2 sm2[];
-    __shared__ uint64_t s_bar;
-    // stage 0 writes bufE / bufO, stage 1 reads them and writes outE / outO,
-    // stage 2 reads those: two barriers per rstep
-    float2 *bufE = sm2;
-    float2 *bufO = sm2 + fft_buf_len<H>();
-    float2 *outE = sm2 + 2 * fft_buf_len<H>();
-    float2 *outO = sm2 + 3 * fft_buf_len<H>();
-    float2 *tws = sm2 + kFoldBufs;
-    float2 *dsm = tws + kFoldTw1 + kFoldTw2;
-    const int tid = threadIdx.x;
     const int row = blockIdx.x;
     int gi = 0;
     while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
         gi++;
     const int s = G.sub[gi];
-    const int lrow = row - G.rowstart[gi];
-    const SubDev sd = P.subs[s];
-    const float2 *D0 = P.prepped + sd.data_off;
     const int bchunk = (P.nb + (int)gridDim.y - 1) / (int)gridDim.y;
     const int b0 = min(P.nb, (int)blockIdx.y * bchunk), b1 = min(P.nb, b0 + bchunk);
-    constexpr unsigned kRowBytes = H * sizeof(float2);
-
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (tid == 0 && b0 < b1)
-        bulk_row_load(dsm, D0 + (long long)b0 * kFoldN, kRowBytes, &s_bar);
-    for (int i = tid; i < kFoldTw1 + kFoldTw2; i += 128)
-        tws[i] = ftw[i];
-    // this thread's folded kernel values: A and B at k = tid + 128 r
-    float2 ka[8], kb[8];
-    const float2 *Fr = F + (long long)row * kFoldN;
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-        ka[r] = Fr[tid + 128 * r];
-        kb[r] = Fr[H + tid + 128 * r];
-    }
-    __syncthreads();
-
-    const int offset = sd.halfwidth * 2;
-    const bool odd_half = tid >= 64;  // stage 1: warps 2-3 take the odd transform
-    for (int b = b0; b < b1; b++) {
-        const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
-        float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
-                      (long long)lrow * sd.stride;
-        if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
-            atomicOr(P.status, kStatusCopy);
-        // stage 0: radix 8 of both transforms from the same data values
-        {
-            float2 ve[8], vo[8];
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const float2 d = dsm[tid + 128 * r];
-                ve[r] = cmul(d, ka[r]);
-                vo[r] = cmul(d, kb[r]);
-            }
-            Dft<8, +1>::run(ve);
-            Dft<8, +1>::run(vo);
-            const int pd = pad(tid * 8);
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                bufE[pad_add(pd, r)] = ve[r];
-                bufO[pad_add(pd, r)] = vo[r];
-            }
-        }
-        __syncthreads();
-        // every thread has read the staged row: start the next rstep's copy
-        if (tid == 0 && b + 1 < b1) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            bulk_row_load(dsm, D0 + (long long)(b + 1) * kFoldN, kRowBytes, &s_bar);
-        }
-        // stage 1: radix 16 (Ns = 8), 64 butterflies per transform
-        fft_stage_oop<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, odd_half ? outO : outE, tws,
-                                        tid & 63);
-        __syncthreads();
-        // stage 2: radix 8 (Ns = 128), butterfly tid of both, shared twiddles
-        {
-            float2 we[8], wo[8];
-            const int pj = pad(tid);
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                we[r] = outE[pad_add(pj, r * 128)];
-                wo[r] = outO[pad_add(pj, r * 128)];
-            }
-#pragma unroll
-            for (int r = 1; r < 8; r++) {
-                const float2 w = twiddle<+1>(tws + kFoldTw1, r * 128 + tid);
-                we[r] = cmul(we[r], w);
-                wo[r] = cmul(wo[r], w);
-            }
-            Dft<8, +1>::run(we);
-            Dft<8, +1>::run(wo);
-            // outputs 2 m and 2 m + 1, m = tid + 128 r: one pair of powers per
-            // 8-byte store (offset and numrs are even)
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const int kk = 2 * (tid + 128 * r) - offset;
-                const float pe = fmaf(we[r].x, we[r].x, we[r].y * we[r].y);
-                const float po = fmaf(wo[r].x, wo[r].x, wo[r].y * wo[r].y);
-                if ((unsigned)kk < (unsigned)numrs)
-                    *reinterpret_cast<float2 *>(outp + kk) = make_float2(pe, po);
-            }
-        }
-        // no barrier: the next rstep's stage 0 writes bufE / bufO, last read
-        // in stage 1 before the barrier above, and its stage 1 writes
-        // outE / outO only after the barrier that follows its stage 0
-    }
-}
-
-// One CTA of a wave at fftlen 2048 (the folded form): the same loop as
-// corr_fold_kernel, reaching its plan's arguments by reference.
-__device__ __forceinline__ void corr_fold_body(const SearchDev &P, const RowGroup &G,
-                                               const float2 *__restrict__ F,
-                                               const float2 *__restrict__ ftw, const int row,
-                                               const int b0, const int b1)
-{
-    constexpr int H = kFoldH;
-    extern __shared__ __align__(16) float2 sm2[];
-    __shared__ uint64_t s_bar;
-    // stage 0 writes bufE / bufO, stage 1 reads them and writes outE / outO,
-    // stage 2 reads those: two barriers per rstep
-    float2 *bufE = sm2;
-    float2 *bufO = sm2 + fft_buf_len<H>();
-    float2 *outE = sm2 + 2 * fft_buf_len<H>();
-    float2 *outO = sm2 + 3 * fft_buf_len<H>();
-    float2 *tws = sm2 + kFoldBufs;
-    float2 *dsm = tws + kFoldTw1 + kFoldTw2;
-    const int tid = threadIdx.x;
-    int gi = 0;
-    while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
-        gi++;
-    const int s = G.sub[gi];
-    const int lrow = row - G.rowstart[gi];
-    const SubDev sd = P.subs[s];
-    const float2 *D0 = P.prepped + sd.data_off;
-    constexpr unsigned kRowBytes = H * sizeof(float2);
-
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (tid == 0 && b0 < b1)
-        bulk_row_load(dsm, D0 + (long long)b0 * kFoldN, kRowBytes, &s_bar);
-    for (int i = tid; i < kFoldTw1 + kFoldTw2; i += 128)
-        tws[i] = ftw[i];
-    // this thread's folded kernel values: A and B at k = tid + 128 r
-    float2 ka[8], kb[8];
-    const float2 *Fr = F + (long long)row * kFoldN;
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-        ka[r] = Fr[tid + 128 * r];
-        kb[r] = Fr[H + tid + 128 * r];
-    }
-    __syncthreads();
-
-    const int offset = sd.halfwidth * 2;
-    const bool odd_half = tid >= 64;  // stage 1: warps 2-3 take the odd transform
-    for (int b = b0; b < b1; b++) {
-        const int numrs = P.steps[(P.first_rstep + b) * P.nsubs + s].numrs;
-        float *outp = P.planes + sd.plane_off + (long long)b * sd.plane_size +
-                      (long long)lrow * sd.stride;
-        if (!bar_wait(&s_bar, (b - b0) & 1) && P.status)
-            atomicOr(P.status, kStatusCopy);
-        // stage 0: radix 8 of both transforms from the same data values
-        {
-            float2 ve[8], vo[8];
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const float2 d = dsm[tid + 128 * r];
-                ve[r] = cmul(d, ka[r]);
-                vo[r] = cmul(d, kb[r]);
-            }
-            Dft<8, +1>::run(ve);
-            Dft<8, +1>::run(vo);
-            const int pd = pad(tid * 8);
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                bufE[pad_add(pd, r)] = ve[r];
-                bufO[pad_add(pd, r)] = vo[r];
-            }
-        }
-        __syncthreads();
-        // every thread has read the staged row: start the next rstep's copy
-        if (tid == 0 && b + 1 < b1) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            bulk_row_load(dsm, D0 + (long long)(b + 1) * kFoldN, kRowBytes, &s_bar);
-        }
-        // stage 1: radix 16 (Ns = 8), 64 butterflies per transform
-        fft_stage_oop<H, +1, 64, 8, 16>(odd_half ? bufO : bufE, odd_half ? outO : outE, tws,
-                                        tid & 63);
-        __syncthreads();
-        // stage 2: radix 8 (Ns = 128), butterfly tid of both, shared twiddles
-        {
-            float2 we[8], wo[8];
-            const int pj = pad(tid);
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                we[r] = outE[pad_add(pj, r * 128)];
-                wo[r] = outO[pad_add(pj, r * 128)];
-            }
-#pragma unroll
-            for (int r = 1; r < 8; r++) {
-                const float2 w = twiddle<+1>(tws + kFoldTw1, r * 128 + tid);
-                we[r] = cmul(we[r], w);
-                wo[r] = cmul(wo[r], w);
-            }
-            Dft<8, +1>::run(we);
-            Dft<8, +1>::run(wo);
-            // outputs 2 m and 2 m + 1, m = tid + 128 r: one pair of powers per
-            // 8-byte store (offset and numrs are even)
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const int kk = 2 * (tid + 128 * r) - offset;
-                const float pe = fmaf(we[r].x, we[r].x, we[r].y * we[r].y);
-                const float po = fmaf(wo[r].x, wo[r].x, wo[r].y * wo[r].y);
-                if ((unsigned)kk < (unsigned)numrs)
-                    *reinterpret_cast<float2 *>(outp + kk) = make_float2(pe, po);
-            }
-        }
-        // no barrier: the next rstep's stage 0 writes bufE / bufO, last read
-        // in stage 1 before the barrier above, and its stage 1 writes
-        // outE / outO only after the barrier that follows its stage 0
-    }
+    fold_cta(P.subs[s], P.prepped, P.steps + P.first_rstep * P.nsubs + s, P.nsubs, P.planes,
+             row - G.rowstart[gi], F + (long long)row * kFoldN, ftw, b0, b1, P.status);
 }
 
 __global__ void __launch_bounds__(128, 4) corr_fold_group_kernel(const __grid_constant__ GroupLaunch M)
@@ -927,7 +866,16 @@ __global__ void __launch_bounds__(128, 4) corr_fold_group_kernel(const __grid_co
     const int ny = M.ny[i];
     int b0, b1;
     rstep_chunk(M.P[i].nb, ny, local % ny, &b0, &b1);
-    corr_fold_body(M.P[i], M.G[i], M.fold[i], M.fold_tw[i], local / ny, b0, b1);
+    const SearchDev &P = M.P[i];
+    const RowGroup &G = M.G[i];
+    const int row = local / ny;
+    int gi = 0;
+    while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
+        gi++;
+    const int s = G.sub[gi];
+    fold_cta(P.subs[s], P.prepped, P.steps + P.first_rstep * P.nsubs + s, P.nsubs, P.planes,
+             row - G.rowstart[gi], M.fold[i] + (long long)row * kFoldN, M.fold_tw[i], b0, b1,
+             P.status);
 }
 
 // A wave's plans at fftlen 2048, in the folded form (M.fold, M.fold_tw set).
@@ -935,7 +883,7 @@ cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st)
 {
     if (M.n < 1 || M.n > kMaxGroupPlans)
         return cudaErrorInvalidValue;
-    const size_t smem = sizeof(float2) * kFoldSmem;
+    const size_t smem = kFoldSmem;
     cudaError_t e = cudaFuncSetAttribute(corr_fold_group_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
@@ -967,7 +915,7 @@ cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st)
 cudaError_t launch_corr_fold(const SearchDev &P, const RowGroup &G, int rows, const float2 *F,
                              const float2 *ftw, cudaStream_t st)
 {
-    const size_t smem = sizeof(float2) * kFoldSmem;
+    const size_t smem = kFoldSmem;
     cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess)

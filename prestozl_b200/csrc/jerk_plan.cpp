@@ -1225,6 +1225,7 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
             append_twiddles(o.second, tw);
     }
     if (p->groups.count(2048)) {
+        twtotal += twtotal & 1;  // the fold tables start with 16-byte entries
         p->fold_twoff = twtotal;
         tw.resize(twtotal + fold_twiddle_size());
         fold_twiddle_table(tw.data() + twtotal);
@@ -1427,7 +1428,6 @@ static int run_volumes(jerk_plan *p, SearchDev &a)
     cudaError_t e = cudaSuccess;
     for (auto &kv : p->groups) {
         const RowGroup G = row_group(p, kv.second);
-        const int rows = G.rowstart[G.n];
         // algorithmic traffic: each kernel row read once per batch, each
         // prepared chunk read once, every good power written once
         const int N = kv.first;
