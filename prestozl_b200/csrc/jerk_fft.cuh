@@ -481,7 +481,7 @@ __device__ __forceinline__ Cp pmul(Cp a, float c, float s)
     return {fma2(a.re, bc(c), mul2(a.im, bc(-s))), fma2(a.im, bc(c), mul2(a.re, bc(s)))};
 }
 
-// Inverse (exponent sign +1) DFTs of radix 4, 8 and 16 on lane pairs; the
+// Inverse (exponent sign +1) DFTs of radix 4 and 8 on lane pairs; the
 // output order is that of Dft<R, +1>.
 __device__ __forceinline__ void pdft4(Cp &v0, Cp &v1, Cp &v2, Cp &v3)
 {
@@ -512,41 +512,6 @@ __device__ __forceinline__ void pdft8(Cp *v)
     v[6] = psub_i(e2, o2);
     v[3] = {fma2(bc(-h), ur, e3.re), fma2(bc(h), ui, e3.im)};
     v[7] = {fma2(bc(h), ur, e3.re), fma2(bc(-h), ui, e3.im)};
-}
-
-// 16 = 4 x 4 as in Dft<16>: DFT4 over n1 for each n2, W16^(n2 k1), DFT4 over n2
-__device__ __forceinline__ void pdft16(Cp *v)
-{
-    const float c1 = 0.92387953251128675613f;  // cos(pi/8)
-    const float s1 = 0.38268343236508977173f;  // sin(pi/8)
-    const float h = 0.70710678118654752440f;
-#pragma unroll
-    for (int n2 = 0; n2 < 4; n2++)
-        pdft4(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
-    // element (n2, k1) is now v[n2 + 4 k1]; multiply by W16^(n2 k1)
-    v[1 + 4] = pmul(v[1 + 4], c1, s1);                                          // m = 1
-    v[1 + 8] = {mul2(bc(h), sub2(v[9].re, v[9].im)), mul2(bc(h), add2(v[9].im, v[9].re))};  // 2
-    v[1 + 12] = pmul(v[1 + 12], s1, c1);                                        // m = 3
-    v[2 + 4] = {mul2(bc(h), sub2(v[6].re, v[6].im)), mul2(bc(h), add2(v[6].im, v[6].re))};  // 2
-    v[2 + 8] = {mul2(bc(-1.0f), v[10].im), v[10].re};                           // m = 4
-    v[2 + 12] = {mul2(bc(-h), add2(v[14].re, v[14].im)), mul2(bc(h), sub2(v[14].re, v[14].im))};  // 6
-    v[3 + 4] = pmul(v[3 + 4], s1, c1);                                          // m = 3
-    v[3 + 8] = {mul2(bc(-h), add2(v[11].re, v[11].im)), mul2(bc(h), sub2(v[11].re, v[11].im))};  // 6
-    v[3 + 12] = pmul(v[3 + 12], -c1, -s1);                                      // m = 9
-    // DFT4 over n2 for each k1: inputs v[4 k1 + n2], outputs k1 + 4 k2
-    Cp t[16];
-#pragma unroll
-    for (int k1 = 0; k1 < 4; k1++) {
-        Cp a0 = v[4 * k1], a1 = v[4 * k1 + 1], a2 = v[4 * k1 + 2], a3 = v[4 * k1 + 3];
-        pdft4(a0, a1, a2, a3);
-        t[k1] = a0;
-        t[k1 + 4] = a1;
-        t[k1 + 8] = a2;
-        t[k1 + 12] = a3;
-    }
-#pragma unroll
-    for (int i = 0; i < 16; i++)
-        v[i] = t[i];
 }
 
 // Host: the per-stage twiddle tables of FftPlan<N>, forward sign, computed

@@ -615,14 +615,18 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrGroupOcc<N>::value)
 // transform (its butterflies and twiddles) is gone, and the two transforms
 // share every twiddle and every data value.
 //
-// The two transforms run in the two lanes of packed FP32 instructions
-// (Cp, pdft8, pdft16): every butterfly of the even transform has its twin
-// in the odd one at the same position with the same twiddle, so each
-// instruction does both.  The 1024-point plan is [8, 16, 8] for 128
-// threads: stage 0 (radix 8) -- thread j does butterfly j of both from the
-// same 8 data values; stage 1 (radix 16, 64 butterflies) -- warps 0-1,
-// butterfly j of both; stage 2 (radix 8) -- thread j butterfly j of both,
-// and the lane pair of powers (outputs 2 m, 2 m + 1) is one 8-byte store.
+// The 1024-point plan is [8, 16, 8] for 128 threads.  Stages 0 and 2 run
+// the two transforms in the two lanes of packed FP32 instructions (Cp,
+// pdft8): every butterfly of the even transform has its twin in the odd one
+// at the same position with the same twiddle and data value, so each
+// instruction does both.  Stage 0 (radix 8): thread j does butterfly j of
+// both from the same 8 data values, and applies stage 1's input twiddles.
+// Stage 1 (radix 16, 64 butterflies per transform): one transform per
+// thread in scalar FP32, warps 0-1 the even one and 2-3 the odd one, so all
+// four warps work (a scalar instruction holds the FP32 pipe for one cycle,
+// a packed one for two: the pipe time is the same either way).  Stage 2
+// (radix 8): thread j does butterfly j of both, and the lane pair of powers
+// (outputs 2 m, 2 m + 1) is one 8-byte store.
 
 static int sm_count();
 
@@ -679,32 +683,17 @@ cudaError_t launch_fold_rows(const float2 *bank, const long long *src, float2 *o
     return cudaGetLastError();
 }
 
-// Shared memory of the folded correlation.  The transform buffers hold one
-// lane pair per point, float4 (re even, re odd, im even, im odd), with one
-// float4 of padding after every 8 (one 128-byte row of banks), so that the
-// 16-byte accesses of each quarter-warp fall in 8 distinct bank groups in
-// every stage:
-//   stage 0 writes 8 t + r            -> padded 9 t + r
-//   stage 1 reads  j + 64 r           -> padded j + j/8 + 72 r
-//           writes 128 (j/8) + j%8 + 8 r -> padded 144 (j/8) + j%8 + 9 r
-//   stage 2 reads  t + 128 r          -> padded t + t/8 + 144 r
-// After the buffers: the two twiddle tables (float2) and the staged half
-// data row.
-__host__ __device__ constexpr int pad4(int i) { return i + (i >> 3); }
-constexpr int kFoldBuf4 = kFoldH + kFoldH / 8;  // float4 per buffer
-constexpr int kFoldSmem = 2 * kFoldBuf4 * 16 + (kFoldTw1 + kFoldTw2 + kFoldH) * 8;  // bytes
-static_assert((2 * kFoldBuf4 * 16 + (kFoldTw1 + kFoldTw2) * 8) % 16 == 0,
-              "16-byte aligned staging row");
+// Shared memory of the folded correlation: four transform buffers (stage 0
+// writes even / odd, stage 1 reads them and writes the other two, stage 2
+// reads those), each a padded float2 plane (pad(), conflict-free for all
+// three stages' access patterns); stage 0's twiddle table; the staged half
+// data row.  Stage 2's roots are read through L1 (8 KB, shared by the CTAs
+// of an SM), which leaves room for 5 CTAs per SM.
+constexpr int kFoldPlane = fft_buf_len<kFoldH>();  // float2 per transform buffer
+constexpr int kFoldSmem = (4 * kFoldPlane + kFoldTw1 + kFoldH) * 8;  // bytes
+constexpr int kFoldOcc = 5;  // CTAs per SM (registers and shared memory both allow 5)
+static_assert((4 * kFoldPlane + kFoldTw1) % 2 == 0, "16-byte aligned staging row");
 
-__device__ __forceinline__ void st_cp(float4 *p, const Cp &v)
-{
-    *p = make_float4(v.re.x, v.re.y, v.im.x, v.im.y);
-}
-__device__ __forceinline__ Cp ld_cp(const float4 *p)
-{
-    const float4 q = *p;
-    return {make_float2(q.x, q.y), make_float2(q.z, q.w)};
-}
 // v (c + i s) with (c, s) the conjugate of a forward table root w: the
 // inverse transform's twiddle
 __device__ __forceinline__ Cp pmul_conj(const Cp &v, float2 w) { return pmul(v, w.x, -w.y); }
@@ -713,7 +702,8 @@ __device__ __forceinline__ Cp pmul_conj(const Cp &v, float2 w) { return pmul(v, 
 // kr[r], ki[r]: the lane pairs (re A, re B), (im A, im B) of the row's
 // folded values at k = tid + 128 r.  steps: the row's subharmonic at b = 0
 // (stride nsubs per rstep); out: its volume row at b = 0.
-__device__ __forceinline__ void fold_rsteps(float4 *bufA, float4 *bufB, const float2 *tw1,
+__device__ __forceinline__ void fold_rsteps(float2 *bufE, float2 *bufO, float2 *outE,
+                                            float2 *outO, const float2 *tw1,
                                             const float2 *tw2, const float2 *dsm, uint64_t *bar,
                                             const float2 (&kr)[8], const float2 (&ki)[8],
                                             const float2 *D0, const StepDev *steps, int nsubs,
@@ -745,10 +735,12 @@ __device__ __forceinline__ void fold_rsteps(float4 *bufA, float4 *bufB, const fl
 #pragma unroll
             for (int r = 1; r < 8; r++)
                 v[r] = pmul_conj(v[r], w1[r]);
-            float4 *p = bufA + 9 * tid;
+            const int pd = pad(tid * 8);
 #pragma unroll
-            for (int r = 0; r < 8; r++)
-                st_cp(p + r, v[r]);
+            for (int r = 0; r < 8; r++) {
+                bufE[pad_add(pd, r)] = make_float2(v[r].re.x, v[r].im.x);
+                bufO[pad_add(pd, r)] = make_float2(v[r].re.y, v[r].im.y);
+            }
         }
         __syncthreads();
         // every thread has read the staged row: start the next rstep's copy
@@ -757,32 +749,39 @@ __device__ __forceinline__ void fold_rsteps(float4 *bufA, float4 *bufB, const fl
             bulk_row_load(const_cast<float2 *>(dsm), D0 + (long long)(b + 1) * kFoldN, kRowBytes,
                           bar);
         }
-        // stage 1: radix 16 (Ns = 8), butterfly j = tid of both transforms,
-        // by warps 0-1
-        if (tid < 64) {
-            const int j = tid, k = j & 7;
-            Cp v[16];
-            const float4 *p = bufA + j + (j >> 3);
+        // stage 1: radix 16 (Ns = 8), one transform per thread (scalar):
+        // warps 0-1 butterfly j = tid of the even transform, warps 2-3 of the
+        // odd one; its input twiddles were applied by stage 0
+        {
+            const bool odd = tid >= 64;
+            const int j = tid & 63;
+            const float2 *src = odd ? bufO : bufE;
+            float2 *dst = odd ? outO : outE;
+            float2 x[16];
+            const int pj = pad(j);
 #pragma unroll
             for (int r = 0; r < 16; r++)
-                v[r] = ld_cp(p + 72 * r);
-            pdft16(v);
-            float4 *q = bufB + 144 * (j >> 3) + k;
+                x[r] = src[pad_add(pj, r * 64)];
+            Dft<16, +1>::run(x);
+            const int pq = pad((j >> 3) * 128 + (j & 7));
 #pragma unroll
             for (int r = 0; r < 16; r++)
-                st_cp(q + 9 * r, v[r]);
+                dst[pad_add(pq, r * 8)] = x[r];
         }
         __syncthreads();
         // stage 2: radix 8 (Ns = 128), butterfly tid of both
         {
             Cp v[8];
-            const float4 *p = bufB + tid + (tid >> 3);
+            const int pj = pad(tid);
 #pragma unroll
-            for (int r = 0; r < 8; r++)
-                v[r] = ld_cp(p + 144 * r);
+            for (int r = 0; r < 8; r++) {
+                const float2 e = outE[pad_add(pj, r * 128)], o = outO[pad_add(pj, r * 128)];
+                v[r].re = make_float2(e.x, o.x);
+                v[r].im = make_float2(e.y, o.y);
+            }
 #pragma unroll
             for (int r = 1; r < 8; r++)
-                v[r] = pmul_conj(v[r], tw2[r * 128 + tid]);
+                v[r] = pmul_conj(v[r], __ldg(tw2 + r * 128 + tid));
             pdft8(v);
             // outputs 2 m and 2 m + 1, m = tid + 128 r: the lane pair of
             // powers is one 8-byte store (offset and numrs are even)
@@ -794,9 +793,9 @@ __device__ __forceinline__ void fold_rsteps(float4 *bufA, float4 *bufB, const fl
                     *reinterpret_cast<float2 *>(outp + kk) = pw;
             }
         }
-        // no barrier: the next rstep's stage 0 writes bufA, last read in
-        // stage 1 before the barrier above, and its stage 1 writes bufB only
-        // after the barrier that follows its stage 0
+        // no barrier: the next rstep's stage 0 writes bufE / bufO, last read
+        // in stage 1 before the barrier above, and its stage 1 writes outE /
+        // outO only after the barrier that follows its stage 0
     }
 }
 
@@ -809,12 +808,10 @@ __device__ __forceinline__ void fold_cta(const SubDev &sd, const float2 *prepped
                                          const float2 *__restrict__ ftw, int b0, int b1,
                                          unsigned *status)
 {
-    extern __shared__ __align__(16) float4 sm4[];
+    extern __shared__ __align__(16) float2 smf[];
     __shared__ uint64_t s_bar;
-    float4 *bufA = sm4;
-    float4 *bufB = sm4 + kFoldBuf4;
-    float2 *tws = reinterpret_cast<float2 *>(sm4 + 2 * kFoldBuf4);
-    float2 *dsm = tws + kFoldTw1 + kFoldTw2;
+    float2 *tws = smf + 4 * kFoldPlane;
+    float2 *dsm = tws + kFoldTw1;
     const int tid = threadIdx.x;
     const float2 *D0 = prepped + sd.data_off;
     constexpr unsigned kRowBytes = kFoldH * sizeof(float2);
@@ -826,7 +823,7 @@ __device__ __forceinline__ void fold_cta(const SubDev &sd, const float2 *prepped
     __syncthreads();
     if (tid == 0 && b0 < b1)
         bulk_row_load(dsm, D0 + (long long)b0 * kFoldN, kRowBytes, &s_bar);
-    for (int i = tid; i < kFoldTw1 + kFoldTw2; i += 128)
+    for (int i = tid; i < kFoldTw1; i += 128)
         tws[i] = ftw[i];
     float2 kr[8], ki[8];
 #pragma unroll
@@ -836,7 +833,8 @@ __device__ __forceinline__ void fold_cta(const SubDev &sd, const float2 *prepped
         ki[r] = make_float2(a.y, bb.y);
     }
     __syncthreads();
-    fold_rsteps(bufA, bufB, tws, tws + kFoldTw1, dsm, &s_bar, kr, ki, D0, steps, nsubs,
+    fold_rsteps(smf, smf + kFoldPlane, smf + 2 * kFoldPlane, smf + 3 * kFoldPlane, tws,
+                ftw + kFoldTw1, dsm, &s_bar, kr, ki, D0, steps, nsubs,
                 planes + sd.plane_off + (long long)lrow * sd.stride, sd.plane_size,
                 sd.halfwidth * 2, b0, b1, status);
 }
@@ -844,7 +842,7 @@ __device__ __forceinline__ void fold_cta(const SubDev &sd, const float2 *prepped
 // A plan's own launch at fftlen 2048: one CTA per kernel row (blockIdx.x)
 // of the group, rsteps of chunk blockIdx.y of gridDim.y; F: the group's
 // folded rows in launch order; ftw: the two twiddle tables.
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, kFoldOcc)
     corr_fold_kernel(const __grid_constant__ SearchDev P, const __grid_constant__ RowGroup G,
                      const float2 *__restrict__ F, const float2 *__restrict__ ftw)
 {
@@ -859,7 +857,7 @@ __global__ void __launch_bounds__(128, 4)
              row - G.rowstart[gi], F + (long long)row * kFoldN, ftw, b0, b1, P.status);
 }
 
-__global__ void __launch_bounds__(128, 4) corr_fold_group_kernel(const __grid_constant__ GroupLaunch M)
+__global__ void __launch_bounds__(128, kFoldOcc) corr_fold_group_kernel(const __grid_constant__ GroupLaunch M)
 {
     const int i = group_plan(M, blockIdx.x);
     const int local = blockIdx.x - M.cta0[i];
@@ -892,7 +890,7 @@ cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st)
                                  (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess)
         return e;
-    const int wave = sm_count() * 4;
+    const int wave = sm_count() * kFoldOcc;
     long long total = 0;
     for (int i = 0; i < M.n; i++)
         total += M.G[i].rowstart[M.G[i].n];
@@ -923,7 +921,7 @@ cudaError_t launch_corr_fold(const SearchDev &P, const RowGroup &G, int rows, co
                                  (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess)
         return e;
-    const int wave = sm_count() * 4;
+    const int wave = sm_count() * kFoldOcc;
     const int split = rows >= 2 * wave ? 1 : std::max(1, std::min(P.nb, (2 * wave + rows - 1) / rows));
     corr_fold_kernel<<<dim3(rows, split), 128, smem, st>>>(P, G, F, ftw);
     return cudaGetLastError();
@@ -1640,7 +1638,7 @@ static cudaError_t launch_corr_group_n(GroupLaunch &M, cudaStream_t st)
 int corr_wave_ctas(int fftlen)
 {
     switch (fftlen) {
-#define JERK_CW(NN) case NN: return sm_count() * CorrOcc<NN>::value;
+#define JERK_CW(NN) case NN: return sm_count() * (NN == kFoldN ? kFoldOcc : CorrOcc<NN>::value);
     JERK_CW(128) JERK_CW(192) JERK_CW(256) JERK_CW(384) JERK_CW(512) JERK_CW(768)
     JERK_CW(1024) JERK_CW(1280) JERK_CW(2048) JERK_CW(4096) JERK_CW(5120) JERK_CW(7680)
     JERK_CW(10240) JERK_CW(15360)
