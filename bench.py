@@ -56,7 +56,7 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 #                   --e2e-steps 1 --batch 16 --no-extras
 # The read side (folded kernel rows + data rows) is paid once per launch; the
 # write side (the volumes) grows with the rsteps per batch.
-CORR2048_TRAFFIC = {"read": 491.242752e6, "write": 2241.772e6, "batch": 16}
+CORR2048_TRAFFIC = {"read": 491.168256e6, "write": 2241.328e6, "batch": 16}
 
 
 def corr2048_traffic(batch: int) -> float:
