@@ -481,7 +481,7 @@ __device__ __forceinline__ Cp pmul(Cp a, float c, float s)
     return {fma2(a.re, bc(c), mul2(a.im, bc(-s))), fma2(a.im, bc(c), mul2(a.re, bc(s)))};
 }
 
-// Inverse (exponent sign +1) DFTs of radix 4 and 8 on lane pairs; the
+// Inverse (exponent sign +1) DFTs of radix 4, 8 and 5 on lane pairs; the
 // output order is that of Dft<R, +1>.
 __device__ __forceinline__ void pdft4(Cp &v0, Cp &v1, Cp &v2, Cp &v3)
 {
@@ -512,6 +512,34 @@ __device__ __forceinline__ void pdft8(Cp *v)
     v[6] = psub_i(e2, o2);
     v[3] = {fma2(bc(-h), ur, e3.re), fma2(bc(h), ui, e3.im)};
     v[7] = {fma2(bc(h), ur, e3.re), fma2(bc(-h), ui, e3.im)};
+}
+
+// Radix 5, as in Dft<5, +1>: with a1 = v1 + v4, b1 = v1 - v4, a2 = v2 + v3,
+// b2 = v2 - v3 (c1, c2 = cos 2pi/5, cos 4pi/5; s1, s2 = sin 2pi/5, sin 4pi/5)
+//   v0 = v0 + a1 + a2
+//   v1, v4 = v0 + c1 a1 + c2 a2 +/- i (s1 b1 + s2 b2)
+//   v2, v3 = v0 + c2 a1 + c1 a2 +/- i (s2 b1 - s1 b2)
+__device__ __forceinline__ void pdft5(Cp *v)
+{
+    const float c1 = 0.30901699437494742410f;   // cos(2 pi/5)
+    const float c2 = -0.80901699437494742410f;  // cos(4 pi/5)
+    const float s1 = 0.95105651629515357212f;   // sin(2 pi/5)
+    const float s2 = 0.58778525229247312917f;   // sin(4 pi/5)
+    const Cp a1 = padd(v[1], v[4]), b1 = psub(v[1], v[4]);
+    const Cp a2 = padd(v[2], v[3]), b2 = psub(v[2], v[3]);
+    const Cp x0 = v[0];
+    const Cp p1 = {fma2(bc(c2), a2.re, fma2(bc(c1), a1.re, x0.re)),
+                   fma2(bc(c2), a2.im, fma2(bc(c1), a1.im, x0.im))};
+    const Cp p2 = {fma2(bc(c1), a2.re, fma2(bc(c2), a1.re, x0.re)),
+                   fma2(bc(c1), a2.im, fma2(bc(c2), a1.im, x0.im))};
+    const Cp t1 = {fma2(bc(s2), b2.re, mul2(bc(s1), b1.re)), fma2(bc(s2), b2.im, mul2(bc(s1), b1.im))};
+    const Cp t2 = {fma2(bc(-s1), b2.re, mul2(bc(s2), b1.re)),
+                   fma2(bc(-s1), b2.im, mul2(bc(s2), b1.im))};
+    v[0] = {add2(add2(x0.re, a1.re), a2.re), add2(add2(x0.im, a1.im), a2.im)};
+    v[1] = padd_i(p1, t1);
+    v[4] = psub_i(p1, t1);
+    v[2] = padd_i(p2, t2);
+    v[3] = psub_i(p2, t2);
 }
 
 // Host: the per-stage twiddle tables of FftPlan<N>, forward sign, computed

@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrGroupOcc<N>::value)
 }
 
 // ---------------------------------------------------------------------------
-// 2b. Correlation at fftlen 2048 on folded kernel rows.
+// 2b. Correlation at fftlen 2048 and 1280 on folded kernel rows.
 //
 // The prepared chunk D repeats with period N/2 (it is the transform of data
 // spread to even interbins), so the inverse transform of D conj(K) splits
@@ -609,108 +609,145 @@ __global__ void __launch_bounds__(FftPlan<N>::T, CorrGroupOcc<N>::value)
 //   y[2m]     = IFFT_{N/2}(D A)[m],  A[k] = conj K[k] + conj K[k + N/2]
 //   y[2m + 1] = IFFT_{N/2}(D B)[m],  B[k] = (conj K[k] - conj K[k + N/2]) e^{+2 pi i k/N}
 // for k < N/2.  A and B depend only on the kernel row, so a plan folds its
-// rows of length 2048 once (fold_rows_kernel, in double, each value rounded
-// once) and the correlation runs two 1024-point transforms that read each
-// data value once for both: the first radix-2 layer of the 2048-point
+// rows of a folded length once (fold_rows_kernel, in double, each value
+// rounded once) and the correlation runs two half-length transforms that read
+// each data value once for both: the first radix-2 layer of the full
 // transform (its butterflies and twiddles) is gone, and the two transforms
 // share every twiddle and every data value.
 //
-// The 1024-point plan is [8, 16, 8] for 128 threads.  Stages 0 and 2 run
-// the two transforms in the two lanes of packed FP32 instructions (Cp,
-// pdft8): every butterfly of the even transform has its twin in the odd one
-// at the same position with the same twiddle and data value, so each
-// instruction does both.  Stage 0 (radix 8): thread j does butterfly j of
-// both from the same 8 data values, and applies stage 1's input twiddles.
-// Stage 1 (radix 16, 64 butterflies per transform): one transform per
-// thread in scalar FP32, warps 0-1 the even one and 2-3 the odd one, so all
-// four warps work (a scalar instruction holds the FP32 pipe for one cycle,
-// a packed one for two: the pipe time is the same either way).  Stage 2
-// (radix 8): thread j does butterfly j of both, and the lane pair of powers
-// (outputs 2 m, 2 m + 1) is one 8-byte store.
+// The half-length plan is [8, 16, R2] for T = N/16 threads (H = N/2 = 128
+// R2: 1024 = [8, 16, 8] on 128 threads, 640 = [8, 16, 5] on 80).  Stages 0
+// and 2 run the two transforms in the two lanes of packed FP32 instructions
+// (Cp, pdft8, pdft5): every butterfly of the even transform has its twin in
+// the odd one at the same position with the same twiddle and data value, so
+// each instruction does both.  Stage 0 (radix 8, T butterflies): thread j
+// does butterfly j of both from the same 8 data values, and applies stage 1's
+// input twiddles.  Stage 1 (radix 16, T/2 butterflies per transform): one
+// transform per thread in scalar FP32, the first half of the threads the even
+// one and the second half the odd one, so every warp works (a scalar
+// instruction holds the FP32 pipe for one cycle, a packed one for two: the
+// pipe time is the same either way).  Stage 2 (radix R2, 128 butterflies,
+// Ns = 128): butterfly j of both, and the lane pair of powers (outputs 2 m,
+// 2 m + 1) is one 8-byte store.
 
 static int sm_count();
 
-constexpr int kFoldN = 2048;
-constexpr int kFoldH = kFoldN / 2;
-constexpr int kFoldTw1 = 8 * 16;     // stage 1: W_128^(r k) at [r 8 + k]
-constexpr int kFoldTw2 = 128 * 8;    // stage 2: W_1024^(r k) at [r 128 + k]
+template <int N>
+struct FoldPlan;
+// CTAs per SM: 5 at 2048 (93 registers, 44 KB of shared memory); 6 at 1280
+template <>
+struct FoldPlan<2048> {
+    static constexpr int R2 = 8, Occ = 5;
+};
+template <>
+struct FoldPlan<1280> {
+    static constexpr int R2 = 5, Occ = 6;
+};
+template <int N>
+struct Fold : FoldPlan<N> {
+    static constexpr int H = N / 2;
+    static constexpr int T = H / 8;                   // threads, stage-0 butterflies
+    static constexpr int Plane = fft_buf_len<H>();     // float2 per transform buffer
+    static constexpr int Tw2 = 128 * FoldPlan<N>::R2;  // stage 2: W_H^(r k) at [r 128 + k]
+    // shared memory: four transform buffers, stage 0's table, the data row
+    static constexpr int Smem = (4 * Plane + 128 + H) * 8;
+    static_assert(H == 128 * FoldPlan<N>::R2 && T % 16 == 0, "[8, 16, R2] on N/16 threads");
+    static_assert((4 * Plane + 128) % 2 == 0, "16-byte aligned staging row");
+};
+constexpr int kFoldTw1 = 8 * 16;  // stage 1's roots W_128^(r k) at [r 8 + k] (both lengths)
 
-int fold_twiddle_size() { return kFoldTw1 + kFoldTw2; }
+bool fold_length(int N) { return N == 2048 || N == 1280; }
+int fold_occ(int N) { return N == 2048 ? Fold<2048>::Occ : N == 1280 ? Fold<1280>::Occ : 0; }
 
-// Host: the two tables, forward sign, in double rounded to float.
-void fold_twiddle_table(float2 *out)
+int fold_twiddle_size(int N)
+{
+    return N == 2048 ? kFoldTw1 + Fold<2048>::Tw2 : N == 1280 ? kFoldTw1 + Fold<1280>::Tw2 : 0;
+}
+
+// Host: the two tables of a folded length, forward sign, in double rounded
+// to float.
+void fold_twiddle_table(int N, float2 *out)
 {
     const double tau = 2.0 * 3.14159265358979323846264338327950288;
+    const int H = N / 2, R2 = H / 128;
     for (int r = 0; r < 16; r++)
         for (int k = 0; k < 8; k++) {
             const double a = -tau * (double)(r * k) / 128.0;
             out[r * 8 + k] = make_float2((float)cos(a), (float)sin(a));
         }
-    for (int r = 0; r < 8; r++)
+    for (int r = 0; r < R2; r++)
         for (int k = 0; k < 128; k++) {
-            const double a = -tau * (double)(r * k) / 1024.0;
+            const double a = -tau * (double)(r * k) / (double)H;
             out[kFoldTw1 + r * 128 + k] = make_float2((float)cos(a), (float)sin(a));
         }
 }
 
 // Folded rows: row i of the launch's groups (consecutive over its
 // subharmonics) from bank row src[i]; out[i] = A (first half), B (second).
+template <int N>
 __global__ void fold_rows_kernel(const float2 *__restrict__ bank, const long long *src,
                                  float2 *__restrict__ out, int nrows)
 {
+    constexpr int H = N / 2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long row = t / kFoldH;
-    const int k = (int)(t % kFoldH);
+    const long long row = t / H;
+    const int k = (int)(t % H);
     if (row >= nrows)
         return;
     const float2 *K = bank + src[row];
-    const float2 k0 = K[k], k1 = K[k + kFoldH];
+    const float2 k0 = K[k], k1 = K[k + H];
     // conj K[k] +/- conj K[k + N/2], in double
     const double ar = (double)k0.x + (double)k1.x, ai = -(double)k0.y - (double)k1.y;
     const double dr = (double)k0.x - (double)k1.x, di = -(double)k0.y + (double)k1.y;
     double sn, cs;
-    sincospi((double)k / (double)kFoldH, &sn, &cs);  // e^{+2 pi i k / N}
-    float2 *o = out + row * kFoldN;
+    sincospi((double)k / (double)H, &sn, &cs);  // e^{+2 pi i k / N}
+    float2 *o = out + row * N;
     o[k] = make_float2((float)ar, (float)ai);
-    o[k + kFoldH] = make_float2((float)(dr * cs - di * sn), (float)(dr * sn + di * cs));
+    o[k + H] = make_float2((float)(dr * cs - di * sn), (float)(dr * sn + di * cs));
 }
 
-cudaError_t launch_fold_rows(const float2 *bank, const long long *src, float2 *out, int nrows,
-                             cudaStream_t st)
+cudaError_t launch_fold_rows(int N, const float2 *bank, const long long *src, float2 *out,
+                             int nrows, cudaStream_t st)
 {
-    const long long n = (long long)nrows * kFoldH;
-    fold_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(bank, src, out, nrows);
+    const long long n = (long long)nrows * (N / 2);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (N == 2048)
+        fold_rows_kernel<2048><<<blocks, 256, 0, st>>>(bank, src, out, nrows);
+    else if (N == 1280)
+        fold_rows_kernel<1280><<<blocks, 256, 0, st>>>(bank, src, out, nrows);
+    else
+        return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
-
-// Shared memory of the folded correlation: four transform buffers (stage 0
-// writes even / odd, stage 1 reads them and writes the other two, stage 2
-// reads those), each a padded float2 plane (pad(), conflict-free for all
-// three stages' access patterns); stage 0's twiddle table; the staged half
-// data row.  Stage 2's roots are read through L1 (8 KB, shared by the CTAs
-// of an SM), which leaves room for 5 CTAs per SM.
-constexpr int kFoldPlane = fft_buf_len<kFoldH>();  // float2 per transform buffer
-constexpr int kFoldSmem = (4 * kFoldPlane + kFoldTw1 + kFoldH) * 8;  // bytes
-constexpr int kFoldOcc = 5;  // CTAs per SM (registers and shared memory both allow 5)
-static_assert((4 * kFoldPlane + kFoldTw1) % 2 == 0, "16-byte aligned staging row");
 
 // v (c + i s) with (c, s) the conjugate of a forward table root w: the
 // inverse transform's twiddle
 __device__ __forceinline__ Cp pmul_conj(const Cp &v, float2 w) { return pmul(v, w.x, -w.y); }
 
 // The rstep loop of one CTA of the folded correlation (both launch forms).
+// Shared memory holds four transform buffers (stage 0 writes even / odd,
+// stage 1 reads them and writes the other two, stage 2 reads those), each a
+// padded float2 plane (pad(), conflict-free for all three stages' access
+// patterns), stage 0's table and the staged half data row; stage 2's roots
+// are read through L1 (shared by the CTAs of an SM).
 // kr[r], ki[r]: the lane pairs (re A, re B), (im A, im B) of the row's
-// folded values at k = tid + 128 r.  steps: the row's subharmonic at b = 0
-// (stride nsubs per rstep); out: its volume row at b = 0.
+// folded values at k = tid + T r.  steps: the row's subharmonic at b = 0
+// (stride nsubs per rstep); out: its volume row at b = 0; norm: the
+// subharmonic's 1/fftlen^2, applied to the powers where N is not a power
+// of two (prep_kernel scales power-of-two chunks by 1/fftlen instead).
+template <int N>
 __device__ __forceinline__ void fold_rsteps(float2 *bufE, float2 *bufO, float2 *outE,
                                             float2 *outO, const float2 *tw1,
                                             const float2 *tw2, const float2 *dsm, uint64_t *bar,
                                             const float2 (&kr)[8], const float2 (&ki)[8],
                                             const float2 *D0, const StepDev *steps, int nsubs,
                                             float *out, long long plane_size, int offset,
-                                            int b0, int b1, unsigned *status)
+                                            float norm, int b0, int b1, unsigned *status)
 {
-    constexpr unsigned kRowBytes = kFoldH * sizeof(float2);
+    using F = Fold<N>;
+    constexpr int T = F::T, H = F::H, R2 = F::R2;
+    constexpr int NB1 = T / 2;  // stage-1 butterflies per transform
+    constexpr unsigned kRowBytes = H * sizeof(float2);
     const int tid = threadIdx.x;
     for (int b = b0; b < b1; b++) {
         const int numrs = steps[(long long)b * nsubs].numrs;
@@ -722,16 +759,16 @@ __device__ __forceinline__ void fold_rsteps(float2 *bufE, float2 *bufO, float2 *
             Cp v[8];
 #pragma unroll
             for (int r = 0; r < 8; r++) {
-                const float2 d = dsm[tid + 128 * r];
+                const float2 d = dsm[tid + T * r];
                 // d A and d B: (dr ar - di ai, dr ai + di ar) per lane
                 v[r].re = fma2(bc(d.x), kr[r], mul2(bc(-d.y), ki[r]));
                 v[r].im = fma2(bc(d.x), ki[r], mul2(bc(d.y), kr[r]));
             }
             pdft8(v);
             // stage 1's input twiddles, applied here: element 8 t + r of
-            // this stage is input (t / 8) of stage-1 butterfly
-            // 8 (t % 8) + r, whose twiddle is W_128^((t / 8) r)
-            const float2 *w1 = tw1 + (tid >> 3) * 8;
+            // this stage is input t / (T/16) of stage-1 butterfly
+            // (8 t + r) mod (T/2), whose twiddle is W_128^((t / (T/16)) r)
+            const float2 *w1 = tw1 + (tid / (T / 16)) * 8;
 #pragma unroll
             for (int r = 1; r < 8; r++)
                 v[r] = pmul_conj(v[r], w1[r]);
@@ -746,22 +783,27 @@ __device__ __forceinline__ void fold_rsteps(float2 *bufE, float2 *bufO, float2 *
         // every thread has read the staged row: start the next rstep's copy
         if (tid == 0 && b + 1 < b1) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            bulk_row_load(const_cast<float2 *>(dsm), D0 + (long long)(b + 1) * kFoldN, kRowBytes,
-                          bar);
+            bulk_row_load(const_cast<float2 *>(dsm), D0 + (long long)(b + 1) * N, kRowBytes, bar);
         }
-        // stage 1: radix 16 (Ns = 8), one transform per thread (scalar):
-        // warps 0-1 butterfly j = tid of the even transform, warps 2-3 of the
-        // odd one; its input twiddles were applied by stage 0
+        // stage 1: radix 16 (Ns = 8), one transform per thread (scalar): the
+        // first T/2 threads butterfly j = tid of the even transform, the rest
+        // of the odd one; its input twiddles were applied by stage 0
         {
-            const bool odd = tid >= 64;
-            const int j = tid & 63;
+            const bool odd = tid >= NB1;
+            const int j = odd ? tid - NB1 : tid;
             const float2 *src = odd ? bufO : bufE;
             float2 *dst = odd ? outO : outE;
             float2 x[16];
-            const int pj = pad(j);
+            if constexpr (IsPow2<NB1>::value) {
+                const int pj = pad(j);
 #pragma unroll
-            for (int r = 0; r < 16; r++)
-                x[r] = src[pad_add(pj, r * 64)];
+                for (int r = 0; r < 16; r++)
+                    x[r] = src[pad_add(pj, r * NB1)];
+            } else {
+#pragma unroll
+                for (int r = 0; r < 16; r++)
+                    x[r] = src[pad(j + r * NB1)];
+            }
             Dft<16, +1>::run(x);
             const int pq = pad((j >> 3) * 128 + (j & 7));
 #pragma unroll
@@ -769,28 +811,38 @@ __device__ __forceinline__ void fold_rsteps(float2 *bufE, float2 *bufO, float2 *
                 dst[pad_add(pq, r * 8)] = x[r];
         }
         __syncthreads();
-        // stage 2: radix 8 (Ns = 128), butterfly tid of both
-        {
-            Cp v[8];
-            const int pj = pad(tid);
+        // stage 2: radix R2 (Ns = 128), butterflies j = tid, tid + T, ... < 128
+        // of both
 #pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const float2 e = outE[pad_add(pj, r * 128)], o = outO[pad_add(pj, r * 128)];
-                v[r].re = make_float2(e.x, o.x);
-                v[r].im = make_float2(e.y, o.y);
-            }
+        for (int jb = 0; jb < 128; jb += T) {
+            const int j = jb + tid;
+            if (128 % T == 0 || j < 128) {
+                Cp v[R2];
+                const int pj = pad(j);
 #pragma unroll
-            for (int r = 1; r < 8; r++)
-                v[r] = pmul_conj(v[r], __ldg(tw2 + r * 128 + tid));
-            pdft8(v);
-            // outputs 2 m and 2 m + 1, m = tid + 128 r: the lane pair of
-            // powers is one 8-byte store (offset and numrs are even)
+                for (int r = 0; r < R2; r++) {
+                    const float2 e = outE[pad_add(pj, r * 128)], o = outO[pad_add(pj, r * 128)];
+                    v[r].re = make_float2(e.x, o.x);
+                    v[r].im = make_float2(e.y, o.y);
+                }
 #pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const int kk = 2 * (tid + 128 * r) - offset;
-                const float2 pw = fma2(v[r].re, v[r].re, mul2(v[r].im, v[r].im));
-                if ((unsigned)kk < (unsigned)numrs)
-                    *reinterpret_cast<float2 *>(outp + kk) = pw;
+                for (int r = 1; r < R2; r++)
+                    v[r] = pmul_conj(v[r], __ldg(tw2 + r * 128 + j));
+                if constexpr (R2 == 8)
+                    pdft8(v);
+                else
+                    pdft5(v);
+                // outputs 2 m and 2 m + 1, m = j + 128 r: the lane pair of
+                // powers is one 8-byte store (offset and numrs are even)
+#pragma unroll
+                for (int r = 0; r < R2; r++) {
+                    const int kk = 2 * (j + 128 * r) - offset;
+                    float2 pw = fma2(v[r].re, v[r].re, mul2(v[r].im, v[r].im));
+                    if constexpr (!IsPow2<N>::value)
+                        pw = mul2(pw, bc(norm));
+                    if ((unsigned)kk < (unsigned)numrs)
+                        *reinterpret_cast<float2 *>(outp + kk) = pw;
+                }
             }
         }
         // no barrier: the next rstep's stage 0 writes bufE / bufO, last read
@@ -802,19 +854,22 @@ __device__ __forceinline__ void fold_rsteps(float2 *bufE, float2 *bufO, float2 *
 // Set-up shared by both launch forms: carve shared memory, start the first
 // data-row copy, stage the twiddles, load this thread's folded values, then
 // run the rstep loop.
+template <int N>
 __device__ __forceinline__ void fold_cta(const SubDev &sd, const float2 *prepped,
                                          const StepDev *steps, int nsubs, float *planes,
                                          int lrow, const float2 *__restrict__ Fr,
                                          const float2 *__restrict__ ftw, int b0, int b1,
                                          unsigned *status)
 {
+    using F = Fold<N>;
+    constexpr int T = F::T, H = F::H;
     extern __shared__ __align__(16) float2 smf[];
     __shared__ uint64_t s_bar;
-    float2 *tws = smf + 4 * kFoldPlane;
+    float2 *tws = smf + 4 * F::Plane;
     float2 *dsm = tws + kFoldTw1;
     const int tid = threadIdx.x;
     const float2 *D0 = prepped + sd.data_off;
-    constexpr unsigned kRowBytes = kFoldH * sizeof(float2);
+    constexpr unsigned kRowBytes = H * sizeof(float2);
 
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&s_bar)) : "memory");
@@ -822,27 +877,28 @@ __device__ __forceinline__ void fold_cta(const SubDev &sd, const float2 *prepped
     }
     __syncthreads();
     if (tid == 0 && b0 < b1)
-        bulk_row_load(dsm, D0 + (long long)b0 * kFoldN, kRowBytes, &s_bar);
-    for (int i = tid; i < kFoldTw1; i += 128)
+        bulk_row_load(dsm, D0 + (long long)b0 * N, kRowBytes, &s_bar);
+    for (int i = tid; i < kFoldTw1; i += T)
         tws[i] = ftw[i];
     float2 kr[8], ki[8];
 #pragma unroll
     for (int r = 0; r < 8; r++) {
-        const float2 a = Fr[tid + 128 * r], bb = Fr[kFoldH + tid + 128 * r];
+        const float2 a = Fr[tid + T * r], bb = Fr[H + tid + T * r];
         kr[r] = make_float2(a.x, bb.x);
         ki[r] = make_float2(a.y, bb.y);
     }
     __syncthreads();
-    fold_rsteps(smf, smf + kFoldPlane, smf + 2 * kFoldPlane, smf + 3 * kFoldPlane, tws,
-                ftw + kFoldTw1, dsm, &s_bar, kr, ki, D0, steps, nsubs,
-                planes + sd.plane_off + (long long)lrow * sd.stride, sd.plane_size,
-                sd.halfwidth * 2, b0, b1, status);
+    fold_rsteps<N>(smf, smf + F::Plane, smf + 2 * F::Plane, smf + 3 * F::Plane, tws,
+                   ftw + kFoldTw1, dsm, &s_bar, kr, ki, D0, steps, nsubs,
+                   planes + sd.plane_off + (long long)lrow * sd.stride, sd.plane_size,
+                   sd.halfwidth * 2, sd.pownorm, b0, b1, status);
 }
 
-// A plan's own launch at fftlen 2048: one CTA per kernel row (blockIdx.x)
-// of the group, rsteps of chunk blockIdx.y of gridDim.y; F: the group's
-// folded rows in launch order; ftw: the two twiddle tables.
-__global__ void __launch_bounds__(128, kFoldOcc)
+// A plan's own launch at a folded length: one CTA per kernel row
+// (blockIdx.x) of the group, rsteps of chunk blockIdx.y of gridDim.y; F: the
+// group's folded rows in launch order; ftw: the two twiddle tables.
+template <int N>
+__global__ void __launch_bounds__(Fold<N>::T, Fold<N>::Occ)
     corr_fold_kernel(const __grid_constant__ SearchDev P, const __grid_constant__ RowGroup G,
                      const float2 *__restrict__ F, const float2 *__restrict__ ftw)
 {
@@ -853,11 +909,13 @@ __global__ void __launch_bounds__(128, kFoldOcc)
     const int s = G.sub[gi];
     const int bchunk = (P.nb + (int)gridDim.y - 1) / (int)gridDim.y;
     const int b0 = min(P.nb, (int)blockIdx.y * bchunk), b1 = min(P.nb, b0 + bchunk);
-    fold_cta(P.subs[s], P.prepped, P.steps + P.first_rstep * P.nsubs + s, P.nsubs, P.planes,
-             row - G.rowstart[gi], F + (long long)row * kFoldN, ftw, b0, b1, P.status);
+    fold_cta<N>(P.subs[s], P.prepped, P.steps + P.first_rstep * P.nsubs + s, P.nsubs, P.planes,
+                row - G.rowstart[gi], F + (long long)row * N, ftw, b0, b1, P.status);
 }
 
-__global__ void __launch_bounds__(128, kFoldOcc) corr_fold_group_kernel(const __grid_constant__ GroupLaunch M)
+template <int N>
+__global__ void __launch_bounds__(Fold<N>::T, Fold<N>::Occ)
+    corr_fold_group_kernel(const __grid_constant__ GroupLaunch M)
 {
     const int i = group_plan(M, blockIdx.x);
     const int local = blockIdx.x - M.cta0[i];
@@ -871,26 +929,32 @@ __global__ void __launch_bounds__(128, kFoldOcc) corr_fold_group_kernel(const __
     while (gi + 1 < G.n && row >= G.rowstart[gi + 1])
         gi++;
     const int s = G.sub[gi];
-    fold_cta(P.subs[s], P.prepped, P.steps + P.first_rstep * P.nsubs + s, P.nsubs, P.planes,
-             row - G.rowstart[gi], M.fold[i] + (long long)row * kFoldN, M.fold_tw[i], b0, b1,
-             P.status);
+    fold_cta<N>(P.subs[s], P.prepped, P.steps + P.first_rstep * P.nsubs + s, P.nsubs, P.planes,
+                row - G.rowstart[gi], M.fold[i] + (long long)row * N, M.fold_tw[i], b0, b1,
+                P.status);
 }
 
-// A wave's plans at fftlen 2048, in the folded form (M.fold, M.fold_tw set).
-cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st)
+template <class K>
+static cudaError_t fold_attrs(K kernel, int smem)
 {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    return e;
+}
+
+// A wave's plans at a folded length (M.fold, M.fold_tw set).
+template <int N>
+static cudaError_t launch_corr_fold_group_n(GroupLaunch M, cudaStream_t st)
+{
+    using F = Fold<N>;
     if (M.n < 1 || M.n > kMaxGroupPlans)
         return cudaErrorInvalidValue;
-    const size_t smem = kFoldSmem;
-    cudaError_t e = cudaFuncSetAttribute(corr_fold_group_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(corr_fold_group_kernel,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
+    cudaError_t e = fold_attrs(corr_fold_group_kernel<N>, F::Smem);
     if (e != cudaSuccess)
         return e;
-    const int wave = sm_count() * kFoldOcc;
+    const int wave = sm_count() * F::Occ;
     long long total = 0;
     for (int i = 0; i < M.n; i++)
         total += M.G[i].rowstart[M.G[i].n];
@@ -906,25 +970,37 @@ cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st)
     if (x >= (1ll << 31))
         return cudaErrorInvalidValue;
     M.cta0[M.n] = (int)x;
-    corr_fold_group_kernel<<<(unsigned)x, 128, smem, st>>>(M);
+    corr_fold_group_kernel<N><<<(unsigned)x, F::T, F::Smem, st>>>(M);
     return cudaGetLastError();
 }
 
-cudaError_t launch_corr_fold(const SearchDev &P, const RowGroup &G, int rows, const float2 *F,
-                             const float2 *ftw, cudaStream_t st)
+cudaError_t launch_corr_fold_group(int N, GroupLaunch M, cudaStream_t st)
 {
-    const size_t smem = kFoldSmem;
-    cudaError_t e = cudaFuncSetAttribute(corr_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(corr_fold_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
+    return N == 2048 ? launch_corr_fold_group_n<2048>(M, st)
+           : N == 1280 ? launch_corr_fold_group_n<1280>(M, st)
+                       : cudaErrorInvalidValue;
+}
+
+template <int N>
+static cudaError_t launch_corr_fold_n(const SearchDev &P, const RowGroup &G, int rows,
+                                      const float2 *Fr, const float2 *ftw, cudaStream_t st)
+{
+    using F = Fold<N>;
+    cudaError_t e = fold_attrs(corr_fold_kernel<N>, F::Smem);
     if (e != cudaSuccess)
         return e;
-    const int wave = sm_count() * kFoldOcc;
+    const int wave = sm_count() * F::Occ;
     const int split = rows >= 2 * wave ? 1 : std::max(1, std::min(P.nb, (2 * wave + rows - 1) / rows));
-    corr_fold_kernel<<<dim3(rows, split), 128, smem, st>>>(P, G, F, ftw);
+    corr_fold_kernel<N><<<dim3(rows, split), F::T, F::Smem, st>>>(P, G, Fr, ftw);
     return cudaGetLastError();
+}
+
+cudaError_t launch_corr_fold(int N, const SearchDev &P, const RowGroup &G, int rows,
+                             const float2 *F, const float2 *ftw, cudaStream_t st)
+{
+    return N == 2048 ? launch_corr_fold_n<2048>(P, G, rows, F, ftw, st)
+           : N == 1280 ? launch_corr_fold_n<1280>(P, G, rows, F, ftw, st)
+                       : cudaErrorInvalidValue;
 }
 
 // ---------------------------------------------------------------------------
@@ -1638,7 +1714,7 @@ static cudaError_t launch_corr_group_n(GroupLaunch &M, cudaStream_t st)
 int corr_wave_ctas(int fftlen)
 {
     switch (fftlen) {
-#define JERK_CW(NN) case NN: return sm_count() * (NN == kFoldN ? kFoldOcc : CorrOcc<NN>::value);
+#define JERK_CW(NN) case NN: return sm_count() * (fold_length(NN) ? fold_occ(NN) : CorrOcc<NN>::value);
     JERK_CW(128) JERK_CW(192) JERK_CW(256) JERK_CW(384) JERK_CW(512) JERK_CW(768)
     JERK_CW(1024) JERK_CW(1280) JERK_CW(2048) JERK_CW(4096) JERK_CW(5120) JERK_CW(7680)
     JERK_CW(10240) JERK_CW(15360)

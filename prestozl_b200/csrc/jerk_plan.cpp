@@ -40,13 +40,25 @@ cudaError_t launch_corr_group(GroupLaunch M, int fftlen, cudaStream_t st);
 cudaError_t launch_harmsum_group(GroupLaunch M, int nstages, cudaStream_t st);
 cudaError_t launch_wait_probe(unsigned int *status, cudaStream_t st);
 int corr_wave_ctas(int fftlen);
-int fold_twiddle_size();
-void fold_twiddle_table(float2 *out);
-cudaError_t launch_fold_rows(const float2 *bank, const long long *src, float2 *out, int nrows,
-                             cudaStream_t st);
-cudaError_t launch_corr_fold(const SearchDev &P, const RowGroup &G, int rows, const float2 *F,
-                             const float2 *ftw, cudaStream_t st);
-cudaError_t launch_corr_fold_group(GroupLaunch M, cudaStream_t st);
+bool fold_length(int N);
+int fold_twiddle_size(int N);
+void fold_twiddle_table(int N, float2 *out);
+cudaError_t launch_fold_rows(int N, const float2 *bank, const long long *src, float2 *out,
+                             int nrows, cudaStream_t st);
+cudaError_t launch_corr_fold(int N, const SearchDev &P, const RowGroup &G, int rows,
+                             const float2 *F, const float2 *ftw, cudaStream_t st);
+cudaError_t launch_corr_fold_group(int N, GroupLaunch M, cudaStream_t st);
+
+// The FFT lengths whose correlation runs on folded kernel rows, and a
+// length's slot in a plan's per-length fold arrays (-1: not folded).
+constexpr int kFoldLens[2] = {2048, 1280};
+static int fold_slot(int N)
+{
+    for (int i = 0; i < 2; i++)
+        if (kFoldLens[i] == N)
+            return i;
+    return -1;
+}
 int harmsum_wave_ctas(int nstages);
 int fft_twiddle_size(int N);
 void fft_twiddle_table(int N, float2 *out);
@@ -744,11 +756,11 @@ struct jerk_plan {
     float2 *d_bank = nullptr;
     bool own_bank = false;
     float2 *d_tw = nullptr;
-    // fftlen 2048: the rows folded for the half-length correlation, and the
-    // offset of its twiddle tables in d_tw
-    float2 *d_fold = nullptr;
-    long long fold_floats2 = 0;
-    int fold_twoff = -1;
+    // per folded length (kFoldLens): the rows folded for the half-length
+    // correlation, and the offset of its twiddle tables in d_tw
+    float2 *d_fold[2] = {nullptr, nullptr};
+    long long fold_floats2[2] = {0, 0};
+    int fold_twoff[2] = {-1, -1};
     SubDev *d_subs = nullptr;
     StepDev *d_steps = nullptr;
     uint16_t *d_zinds = nullptr;
@@ -907,7 +919,8 @@ static void plan_free_device(jerk_plan *p)
     if (p->own_bank)
         cudaFree(p->d_bank);
     cudaFree(p->d_tw);
-    cudaFree(p->d_fold);
+    cudaFree(p->d_fold[0]);
+    cudaFree(p->d_fold[1]);
     cudaFree(p->d_subs);
     cudaFree(p->d_steps);
     cudaFree(p->d_zinds);
@@ -1224,12 +1237,15 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
         for (auto &o : byoff)
             append_twiddles(o.second, tw);
     }
-    if (p->groups.count(2048)) {
-        twtotal += twtotal & 1;  // the fold tables start with 16-byte entries
-        p->fold_twoff = twtotal;
-        tw.resize(twtotal + fold_twiddle_size());
-        fold_twiddle_table(tw.data() + twtotal);
-        twtotal += fold_twiddle_size();
+    for (int f = 0; f < 2; f++) {
+        const int N = kFoldLens[f];
+        if (!p->groups.count(N))
+            continue;
+        twtotal += twtotal & 1;  // 16-byte aligned tables
+        p->fold_twoff[f] = twtotal;
+        tw.resize(twtotal + fold_twiddle_size(N));
+        fold_twiddle_table(N, tw.data() + twtotal);
+        twtotal += fold_twiddle_size(N);
     }
 
 #define JERK_CUDA_B(call)                                \
@@ -1257,24 +1273,37 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
     JERK_CUDA_B(cudaMalloc(&p->d_tw, sizeof(float2) * twtotal));
     JERK_CUDA_B(cudaMemcpyAsync(p->d_tw, tw.data(), sizeof(float2) * twtotal,
                                 cudaMemcpyHostToDevice, p->stream));
-    // fftlen 2048: fold the bank's rows once for the half-length correlation
-    // (the bank must be complete when the plan is made; jerk_bank_generate
-    // returns once it is)
-    std::vector<long long> fold_src;
-    long long *d_fold_src = nullptr;
-    if (p->fold_twoff >= 0) {
-        for (int s : p->groups[2048]) {
+    // folded lengths: fold the bank's rows once for the half-length
+    // correlation (the bank must be complete when the plan is made;
+    // jerk_bank_generate returns once it is)
+    std::vector<long long> fold_src[2];
+    // device copies of the source-row tables, freed when this function
+    // returns on any path (cudaFree waits for the fold kernels reading them)
+    struct FoldSrc {
+        long long *d[2] = {nullptr, nullptr};
+        ~FoldSrc()
+        {
+            cudaFree(d[0]);
+            cudaFree(d[1]);
+        }
+    } d_fold_src;
+    for (int f = 0; f < 2; f++) {
+        const int N = kFoldLens[f];
+        if (p->fold_twoff[f] < 0)
+            continue;
+        for (int s : p->groups[N]) {
             const long long nrow = (long long)subs[s].numw * subs[s].numz;
             for (long long r = 0; r < nrow; r++)
-                fold_src.push_back(p->hsubs[s].kern_off + r * 2048);
+                fold_src[f].push_back(p->hsubs[s].kern_off + r * N);
         }
-        p->fold_floats2 = (long long)fold_src.size() * 2048;
-        JERK_CUDA_B(cudaMalloc(&p->d_fold, sizeof(float2) * p->fold_floats2));
-        JERK_CUDA_B(cudaMalloc(&d_fold_src, sizeof(long long) * fold_src.size()));
-        JERK_CUDA_B(cudaMemcpyAsync(d_fold_src, fold_src.data(), sizeof(long long) * fold_src.size(),
-                                    cudaMemcpyHostToDevice, p->stream));
-        JERK_CUDA_B(launch_fold_rows(p->d_bank, d_fold_src, p->d_fold, (int)fold_src.size(),
-                                     p->stream));
+        p->fold_floats2[f] = (long long)fold_src[f].size() * N;
+        JERK_CUDA_B(cudaMalloc(&p->d_fold[f], sizeof(float2) * p->fold_floats2[f]));
+        JERK_CUDA_B(cudaMalloc(&d_fold_src.d[f], sizeof(long long) * fold_src[f].size()));
+        JERK_CUDA_B(cudaMemcpyAsync(d_fold_src.d[f], fold_src[f].data(),
+                                    sizeof(long long) * fold_src[f].size(), cudaMemcpyHostToDevice,
+                                    p->stream));
+        JERK_CUDA_B(launch_fold_rows(N, p->d_bank, d_fold_src.d[f], p->d_fold[f],
+                                     (int)fold_src[f].size(), p->stream));
     }
     JERK_CUDA_B(cudaMalloc(&p->d_subs, sizeof(SubDev) * nsubs));
     JERK_CUDA_B(cudaMemcpyAsync(p->d_subs, p->hsubs.data(), sizeof(SubDev) * nsubs,
@@ -1319,7 +1348,6 @@ extern "C" int jerk_plan_create(jerk_plan **out, const jerk_obs *obs, const jerk
             return bail(rc);
     }
     JERK_CUDA_B(cudaStreamSynchronize(p->stream));
-    cudaFree(d_fold_src);
 #undef JERK_CUDA_B
     *out = p;
     return JERK_OK;
@@ -1385,12 +1413,14 @@ static inline double fft_flops(int n)
 }
 
 // The plan's own correlation launch for one FFT length (the folded form at
-// 2048).
+// the folded lengths).
 static cudaError_t launch_corr_of(const jerk_plan *p, const SearchDev &a, int N, const RowGroup &G,
                                   cudaStream_t st)
 {
-    if (N == 2048 && p->d_fold)
-        return launch_corr_fold(a, G, G.rowstart[G.n], p->d_fold, p->d_tw + p->fold_twoff, st);
+    const int f = fold_slot(N);
+    if (f >= 0 && p->d_fold[f])
+        return launch_corr_fold(N, a, G, G.rowstart[G.n], p->d_fold[f], p->d_tw + p->fold_twoff[f],
+                                st);
     return launch_corr(a, N, G, G.rowstart[G.n], st);
 }
 
@@ -1816,17 +1846,19 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
         GroupLaunch C{};
         C.n = (int)kv.second.size();
         double bytes = 0, flops = 0;
-        bool fold = N == 2048;
+        const int f = fold_slot(N);
+        bool fold = f >= 0;
         for (int j = 0; j < C.n; j++) {
             jerk_plan *p = W[kv.second[j]];
             const SearchDev &a = p->pass.a;
             C.P[j] = a;
             C.G[j] = row_group(p, p->groups.at(N));
-            // at 2048 every plan has folded rows (made with the plan), so the
-            // merged launch computes exactly what the plan's own launch does
-            fold = fold && p->d_fold;
-            C.fold[j] = p->d_fold;
-            C.fold_tw[j] = p->d_fold ? p->d_tw + p->fold_twoff : nullptr;
+            // at a folded length every plan has folded rows (made with the
+            // plan), so the merged launch computes exactly what the plan's
+            // own launch does
+            fold = fold && p->d_fold[f];
+            C.fold[j] = f >= 0 ? p->d_fold[f] : nullptr;
+            C.fold_tw[j] = f >= 0 && p->d_fold[f] ? p->d_tw + p->fold_twoff[f] : nullptr;
             for (int g = 0; g < C.G[j].n; g++) {
                 const int s = C.G[j].sub[g];
                 const double nrow = (double)p->subs[s].numw * p->subs[s].numz;
@@ -1838,7 +1870,7 @@ static int enqueue_wave(const std::vector<jerk_plan *> &W)
             }
         }
         tok = launch_begin(p0, kclass(p0, "wave_corr_" + std::to_string(N)), bytes, flops);
-        e = fold ? launch_corr_fold_group(C, st) : launch_corr_group(C, N, st);
+        e = fold ? launch_corr_fold_group(N, C, st) : launch_corr_group(C, N, st);
         launch_end(p0, tok);
         if (e != cudaSuccess)
             return fail_all(e, "corr_group_kernel");
@@ -2164,7 +2196,7 @@ extern "C" long long jerk_plan_device_bytes(const jerk_plan *p)
                        sizeof(float2) * p->prepped_f2 +
                        (sizeof(unsigned long long) + sizeof(float)) * p->max_hits +
                        sizeof(StepDev) * p->hsteps.size() + sizeof(float2) * p->spec_cap +
-                       sizeof(float2) * p->fold_floats2 +
+                       sizeof(float2) * (p->fold_floats2[0] + p->fold_floats2[1]) +
                        (p->own_bank ? sizeof(float2) * jerk_bank_elements(p->subs.data(), p->nsubs)
                                     : 0));
 }

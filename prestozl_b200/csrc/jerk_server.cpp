@@ -141,7 +141,8 @@ static BankKey key_of(const Geometry &g)
 }
 
 // Device bytes a plan for g will hold (volumes, rinds, chunks, hit buffer,
-// steps, spectrum staging, and its folded copy of the fftlen-2048 rows).
+// steps, spectrum staging, and its folded copy of the fftlen-2048 and -1280
+// rows).
 static long long plan_footprint(const Geometry &g, int batch)
 {
     long long vol = 0, chunks = 0, folded = 0;
@@ -150,8 +151,8 @@ static long long plan_footprint(const Geometry &g, int batch)
         const long long stride = (((long long)(g.obs.corr_uselen * hf) + 8) + 3) & ~3LL;
         vol += (long long)s.numw * s.numz * stride * 4;
         chunks += (long long)s.fftlen * 8;
-        if (s.fftlen == 2048)
-            folded += (long long)s.numw * s.numz * 2048 * 8;
+        if (s.fftlen == 2048 || s.fftlen == 1280)
+            folded += (long long)s.numw * s.numz * s.fftlen * 8;
     }
     const long long rsteps = (long long)((g.obs.highestbin - g.obs.rlo) / (g.obs.corr_uselen / 2)) + 1;
     return vol * batch + chunks * batch +
