@@ -112,7 +112,8 @@ typedef struct jerk_config {
     void *stream;             /* cudaStream_t to run on; NULL = a private stream */
     const void *device_bank;  /* optional resident bank (jerk_bank_generate); it
                                  must be complete when the plan is created (the
-                                 plan folds its fftlen-2048 rows from it then) */
+                                 plan folds its fftlen-2048 and -1280 rows from it
+                                 then) */
     int harm_mode;            /* harmonic-sum kernel (a tuning knob; results do
                                  not depend on it): 1 = gather (global loads),
                                  2 = gather + TMA prefetch of the next tile into
