@@ -36,10 +36,24 @@ fftwf_plan fftwf_plan_dft_1d(int n, fftwf_complex *in, fftwf_complex *out,
     return p;
 }
 
+/* Per-thread double-precision scratch, grown as needed and kept for the
+ * thread's life: no allocation per execute, and plans stay safe to execute
+ * from several threads at once, as FFTW's new-array execute is. */
+static __thread double *g_scratch;
+static __thread size_t g_scratch_len;
+
 void fftwf_execute_dft(const fftwf_plan p, fftwf_complex *in, fftwf_complex *out)
 {
     const int n = p->n;
-    double *a = (double *)malloc(sizeof(double) * 4 * (size_t)n);
+    const size_t need = 4 * (size_t)n;
+    if (g_scratch_len < need) {
+        double *grown = (double *)realloc(g_scratch, sizeof(double) * need);
+        if (!grown)
+            abort();
+        g_scratch = grown;
+        g_scratch_len = need;
+    }
+    double *a = g_scratch;
     double *b = a + 2 * (size_t)n;
     const float *fin = (const float *)in;
     float *fout = (float *)out;
@@ -49,7 +63,6 @@ void fftwf_execute_dft(const fftwf_plan p, fftwf_complex *in, fftwf_complex *out
     mixfft_exec(p->fft, a, b);
     for (long k = 0; k < 2L * n; k++)
         fout[k] = (float)b[k];
-    free(a);
 }
 
 void fftwf_execute(const fftwf_plan p) { fftwf_execute_dft(p, p->in, p->out); }
